@@ -1,0 +1,358 @@
+"""Benchmark of the generate_grid_sdf / generate_sdf hot path on B200.
+
+Workload (one "step"): generate_grid_sdf with SignMethod::Raycast on a 256^3
+grid over the bounding box (padded 10 %) of the displaced star icosphere,
+subdivision 6 (40,962 vertices, 81,920 triangles) — the medium plain-method
+configuration.  `value` is cells/s with the mesh resident in HBM; `e2e` is the
+same metric through the host-pointer C ABI (mesh H2D and result D2H inside the
+timed region).  The 1M-point queries of the same configuration (Bvh+Raycast,
+Rtree) and the brute force on 65,536 points are reported beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun every rank runs an independent replica (the path has no
+exchange step), timed on the device, max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+GRID_N = 256
+N_POINTS = 1_000_000
+N_BRUTE = 65_536
+SEED = 0
+
+
+def workload():
+    from mesh_to_sdf_b200 import synth
+
+    v, idx = synth.star(6, seed=SEED)
+    lo, hi = synth.padded_bbox(v, 0.1)
+    return v, idx, lo, hi
+
+
+def grid_for(lo, hi, n=(GRID_N, GRID_N, GRID_N)):
+    import mesh_to_sdf_b200 as m2s
+
+    return m2s.Grid.from_bounding_box(lo, hi, list(n))
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_setup():
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        torch.cuda.set_device(local)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    import torch
+
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+
+
+# --------------------------------------------------------------------------- CPU baseline
+def cpu_slab(grid):
+    """A bounded sample of the same grid: the 32 middle z-layers (1/8 of the cells), same cells."""
+    import mesh_to_sdf_b200 as m2s
+
+    nz = 32
+    z0 = GRID_N // 2 - nz // 2
+    first = grid.first_cell.copy()
+    first[2] = np.float32(grid.first_cell[2] + np.float32(z0) * grid.cell_size[2])
+    return m2s.Grid.new(first, grid.cell_size, [GRID_N, GRID_N, nz])
+
+
+def run_cpu_grid(v, idx, g, threads):
+    import oracle
+
+    t = time.perf_counter()
+    oracle.generate_grid_sdf(v, idx, g.first_cell, g.cell_size, g.cell_count, "raycast", n_threads=threads)
+    return time.perf_counter() - t
+
+
+def reference_arm(args, world, rank):
+    """The reference's CPU path (its C++ restatement; cargo is not on this image), all host cores."""
+    if rank != 0:
+        return
+    v, idx, lo, hi = workload()
+    grid = grid_for(lo, hi)
+    slab = cpu_slab(grid)
+    cores = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        run_cpu_grid(v, idx, slab, cores)
+    ts = [run_cpu_grid(v, idx, slab, cores) for _ in range(args.steps)]
+    sec = float(np.mean(ts))
+    value = slab.get_total_cell_count() / sec
+    line = {"impl": "reference", "metric": "SDF cells/s (generate_grid_sdf, Raycast)", "value": value,
+            "unit": "cells/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded star icosphere s6)",
+            "config": {"workload": "star_s6_grid256_raycast", "sample": "256x256x32 middle slab of the 256^3 grid"},
+            "cpu_baseline": {"value": value, "unit": "cells/s", "cores": cores, "kind": "port",
+                             "sample": "256x256x32 middle z-slab (2.1M cells) of the 256^3 grid, per step"},
+            "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------- GPU arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-points", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        reference_arm(args, world, rank)
+        if world > 1:
+            torch_destroy()
+        return
+
+    import torch
+
+    import mesh_to_sdf_b200 as m2s
+    from mesh_to_sdf_b200 import synth
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    v, idx, lo, hi = workload()
+    grid = grid_for(lo, hi)
+    N = grid.get_total_cell_count()
+    T = len(idx) // 3
+    A, S = m2s.AccelerationMethod, m2s.SignMethod
+    mesh = m2s.build_sdf_acceleration(v, m2s.Topology.TriangleList(idx), A.none(S.Raycast))
+    out = torch.empty(N, dtype=torch.float32, device=dev)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def step():
+        mesh.grid_device(grid, S.Raycast, out, status, stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    assert int(status.item()) == 0, f"device status {int(status.item())}"
+
+    # ---- timed region: K steps, L2 flushed between steps (untimed), device events per step
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier(world)
+    with ClockSampler(local) as clk:
+        t_wall = time.perf_counter()
+        for i in range(args.steps):
+            flush.fill_(i & 0xFF)
+            ev[i][0].record()
+            step()
+            ev[i][1].record()
+        torch.cuda.synchronize()
+        t_wall = time.perf_counter() - t_wall
+    barrier(world)
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = max_over_ranks(float(np.sum(step_ms)), world)
+    launches = m2s.last_grid_stats()["kernel_launches"] * args.steps
+    ms_per_step = total_ms / args.steps
+    value = world * N * args.steps / (total_ms / 1e3)
+    assert int(status.item()) == 0
+
+    # ---- roofline of the dominant phase: propagation (k_relax rounds), profiled on the same stream
+    m2s.set_profiling(True)
+    flush.fill_(1)
+    step()
+    torch.cuda.synchronize()
+    m2s.set_profiling(False)
+    phases = m2s.last_grid_phase_ms()
+    stats = m2s.last_grid_stats()
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    # Algorithmic bytes of a relax round: per relaxed state its entry (8 B) and
+    # triangle record (48 B); per neighbour evaluation the neighbour's snapshot
+    # key read (8 B) and its working key (8 B).
+    relax_bytes = stats["states_relaxed"] * 56 + stats["neighbour_evals"] * 16
+    prop_s = phases["propagation"] / 1e3
+    achieved = relax_bytes / prop_s / 1e9 if prop_s > 0 else 0.0
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved / hbm_peak, "traffic": None,
+                "kernel": "k_relax (propagation rounds)", "peak_source": "measured" if peaks else "fallback",
+                "phase_ms": phases, "stats": stats}
+
+    # ---- e2e: the host-pointer C ABI with pinned buffers, H2D + D2H inside the timed region
+    vh = torch.from_numpy(np.ascontiguousarray(v)).pin_memory().numpy()
+    ih = torch.from_numpy(np.ascontiguousarray(idx.view(np.int32))).pin_memory().numpy().view(np.uint32)
+    oh = torch.empty(N, dtype=torch.float32).pin_memory().numpy()
+    import ctypes
+
+    L = m2s._lib.lib()
+    first = np.ascontiguousarray(grid.first_cell)
+    size = np.ascontiguousarray(grid.cell_size)
+    count = np.array(grid.cell_count, np.uint64)
+    nout = ctypes.c_uint64(0)
+
+    def e2e_step():
+        st = L.m2s_generate_grid_sdf(vh.ctypes.data, len(vh), ih.ctypes.data, len(ih), 32, 0, first.ctypes.data,
+                                     size.ctypes.data, count.ctypes.data, 0, oh.ctypes.data, ctypes.byref(nout), None)
+        assert st == 0, st
+
+    for _ in range(2):
+        e2e_step()
+    barrier(world)
+    e2e_times = []
+    for i in range(args.steps):
+        flush.fill_(i & 0xFF)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_step()
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_s = max_over_ranks(float(np.sum(e2e_times)), world)
+    e2e = {"value": world * N * args.steps / e2e_s, "unit": "cells/s", "h2d_bytes_per_step": int(vh.nbytes + ih.nbytes),
+           "d2h_bytes_per_step": int(oh.nbytes)}
+    assert np.array_equal(oh.view(np.uint32), out.cpu().numpy().view(np.uint32)), "e2e result differs from device path"
+
+    # ---- point queries of the same configuration
+    points = {}
+    if not args.no_points:
+        q = torch.from_numpy(synth.mixed_points(v, idx, N_POINTS, seed=SEED)).to(dev)
+        qo = torch.empty(N_POINTS, dtype=torch.float32, device=dev)
+        for name, am, n in (("bvh_raycast", A.bvh(S.Raycast), N_POINTS), ("rtree", A.rtree(), N_POINTS),
+                            ("rtree_bvh", A.rtree_bvh(), N_POINTS), ("none_raycast", A.none(S.Raycast), N_BRUTE),
+                            ("none_normal", A.none(S.Normal), N_BRUTE)):
+            acc = m2s.build_sdf_acceleration(v, m2s.Topology.TriangleList(idx), am)
+            qq = q[:n].contiguous()
+            for _ in range(2):
+                acc.query_device(qq, qo, status, stream)
+            torch.cuda.synchronize()
+            reps = 3
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            flush.fill_(2)
+            e0.record()
+            for _ in range(reps):
+                acc.query_device(qq, qo, status, stream)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            points[name] = {"points": n, "ms": ms, "pts_per_s": n / (ms / 1e3)}
+            if name.startswith("none"):
+                points[name]["pairs_per_s"] = n * T / (ms / 1e3)
+            acc.close()
+        assert int(status.item()) == 0
+
+    # ---- CPU baseline (rank 0, N = 1 only): the oracle port on a bounded sample
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        slab = cpu_slab(grid)
+        cores = os.cpu_count() or 1
+        sec = run_cpu_grid(v, idx, slab, cores)
+        cpu = {"value": slab.get_total_cell_count() / sec, "unit": "cells/s", "cores": cores, "kind": "port",
+               "sample": "256x256x32 middle z-slab (2.1M cells) of the 256^3 grid, C++ restatement, all host threads"}
+
+    if rank == 0:
+        line = {"metric": "SDF cells/s (generate_grid_sdf, Raycast)", "value": value, "unit": "cells/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded star icosphere s6, 81,920 triangles)",
+                "config": {"workload": "star_s6_grid256_raycast", "grid": [GRID_N] * 3, "triangles": T,
+                           "sign": "Raycast", "parallelism": f"replicas x{world}",
+                           "l2": "flushed between steps (256 MiB write, untimed)"},
+                "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": int(launches),
+                "clocks": clk.summary(), "points": points, "wall_s_timed": t_wall}
+        print(json.dumps(line), flush=True)
+    mesh.close()
+    if world > 1:
+        torch_destroy()
+
+
+def torch_destroy():
+    import torch
+
+    if torch.distributed.is_initialized():
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

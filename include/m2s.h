@@ -1,0 +1,152 @@
+/* mesh_to_sdf_b200 — C ABI of the B200 (sm_100a) signed-distance library.
+ *
+ * This is the drop-in boundary for the Rust crate `mesh_to_sdf`: every entry
+ * point below replaces one public function of that crate (citations are
+ * `mesh_to_sdf/src/<file>:<line>`), with the crate's arguments flattened to
+ * plain pointers and sizes.  A Rust shim maps `Topology`, `SignMethod`,
+ * `AccelerationMethod`, `Grid` and `Point` (flattened to float[3]) onto these
+ * calls and turns non-zero status codes back into the crate's panics.
+ *
+ * Conventions
+ *  - vertices / query points: float[3 * n], x y z interleaved (a `[f32; 3]`
+ *    slice, or any `Point` copied out through x()/y()/z()).
+ *  - indices: NULL with index_bits = M2S_INDEX_NONE (the crate's `None`), or
+ *    uint16_t* / uint32_t* with index_bits = 16 / 32.
+ *  - outputs are caller-allocated; *out_len receives the number of results,
+ *    which is 0 exactly when the crate returns an empty Vec.
+ *  - `stream` is a cudaStream_t (NULL = the legacy default stream).  Host-
+ *    pointer entry points block until their results are in host memory.
+ *    `_device` entry points take device pointers, enqueue on `stream` and
+ *    return without synchronising; their status arrives in `d_status`.
+ *  - every call runs on the calling thread's current CUDA device.
+ *  - there is no CPU path: without a usable sm_100 device every compute entry
+ *    point returns M2S_ERR_NO_DEVICE.
+ */
+#ifndef M2S_H
+#define M2S_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The crate panics where these are non-zero. */
+enum m2s_status {
+  M2S_OK = 0,
+  M2S_ERR_INVALID_ARGUMENT = 1,
+  M2S_ERR_NONFINITE_QUERY = 2, /* lib.rs:374-376 assert!(point.is_finite()) */
+  M2S_ERR_INDEX_COUNT = 3,     /* lib.rs:203, lib.rs:207 list length % 3 != 0 */
+  M2S_ERR_INDEX_RANGE = 4,     /* slice indexing panic (test at lib.rs:557-566) */
+  M2S_ERR_NAN_DISTANCE = 5,    /* lib.rs:330 expect("NaN distance") */
+  M2S_ERR_EMPTY_MESH = 6,      /* rtree.rs:317 nearest.unwrap() on an empty tree */
+  M2S_ERR_CUDA = 7,
+  M2S_ERR_OUT_OF_MEMORY = 8,
+  M2S_ERR_LIMIT = 9, /* a bounded device loop (stack, worklist, rounds) hit its limit */
+  M2S_ERR_NO_DEVICE = 10
+};
+
+enum { M2S_TOPOLOGY_TRIANGLE_LIST = 0, M2S_TOPOLOGY_TRIANGLE_STRIP = 1 }; /* lib.rs:156-171 */
+enum { M2S_INDEX_NONE = 0, M2S_INDEX_U16 = 16, M2S_INDEX_U32 = 32 };
+enum { M2S_SIGN_RAYCAST = 0, M2S_SIGN_NORMAL = 1 }; /* lib.rs:252-263 */
+enum {                                              /* lib.rs:272-286 */
+       M2S_ACCEL_NONE = 0,
+       M2S_ACCEL_BVH = 1,
+       M2S_ACCEL_RTREE = 2,
+       M2S_ACCEL_RTREE_BVH = 3
+};
+
+/* Resident acceleration structure: `SdfAccelerationMesh` (lib.rs:303-312).
+ * Owns device copies of the mesh and its LBVH; immutable after build and safe
+ * to query from several streams at once. */
+typedef struct m2s_mesh m2s_mesh;
+
+/* generate_sdf (lib.rs:364-391).  `sign` is ignored for RTREE (always the
+ * normal sign, rtree.rs:306-326) and RTREE_BVH (always the 3-ray vote,
+ * rtree_bvh.rs:143-201).  out: n_queries floats. */
+int m2s_generate_sdf(const float* vertices, uint64_t n_vertices, const void* indices,
+                     uint64_t n_indices, int index_bits, int topology, const float* query_points,
+                     uint64_t n_queries, int accel, int sign, float* out, uint64_t* out_len,
+                     void* stream);
+
+/* generate_grid_sdf (generate/grid.rs:265-378).  The grid is `Grid::new(first_cell,
+ * cell_size, cell_count)` (grid.rs:43-49); out holds the cell_count product of
+ * floats in the crate's order, index = z + y*nz + x*ny*nz (grid.rs:122-124). */
+int m2s_generate_grid_sdf(const float* vertices, uint64_t n_vertices, const void* indices,
+                          uint64_t n_indices, int index_bits, int topology,
+                          const float first_cell[3], const float cell_size[3],
+                          const uint64_t cell_count[3], int sign, float* out, uint64_t* out_len,
+                          void* stream);
+
+/* build_sdf_acceleration (lib.rs:410-433).  *out_mesh is NULL (and M2S_OK is
+ * returned) exactly where the crate returns None: RTREE_BVH on an empty mesh
+ * (rtree_bvh.rs:124-126). */
+int m2s_build_sdf_acceleration(const float* vertices, uint64_t n_vertices, const void* indices,
+                               uint64_t n_indices, int index_bits, int topology, int accel,
+                               int sign, m2s_mesh** out_mesh, void* stream);
+
+/* query_sdf (lib.rs:463-485).  Non-finite query points are rejected with
+ * M2S_ERR_NONFINITE_QUERY (the crate does not check them here). */
+int m2s_query_sdf(const m2s_mesh* mesh, const float* query_points, uint64_t n_queries,
+                  float* out, uint64_t* out_len, void* stream);
+
+/* query_vector_to_closest_point_rtree_bvh (rtree_bvh.rs:217-276, exported at
+ * lib.rs:150).  The mesh must have been built with M2S_ACCEL_RTREE_BVH.
+ * out_vectors: 3 floats per query (closest point - query); out_inside: 1 byte
+ * per query (1 = inside by the 3-ray vote). */
+int m2s_query_vector_to_closest_point(const m2s_mesh* mesh, const float* query_points,
+                                      uint64_t n_queries, float* out_vectors,
+                                      uint8_t* out_inside, uint64_t* out_len, void* stream);
+
+/* Releases a handle from m2s_build_sdf_acceleration (NULL is a no-op). */
+void m2s_mesh_free(m2s_mesh* mesh);
+
+/* Triangle count and acceleration method of a handle. */
+uint64_t m2s_mesh_triangle_count(const m2s_mesh* mesh);
+int m2s_mesh_accel(const m2s_mesh* mesh);
+
+/* ---- device-resident variants (HBM in, HBM out, asynchronous) ----------- */
+
+/* query_sdf over device arrays.  d_status: device uint32 that receives the
+ * OR of status bits (1 << code) raised by the kernels; may be NULL. */
+int m2s_query_sdf_device(const m2s_mesh* mesh, const float* d_query_points, uint64_t n_queries,
+                         float* d_out, uint32_t* d_status, void* stream);
+
+/* generate_grid_sdf against a resident mesh (built with any method; the grid
+ * path uses its triangles and LBVH).  d_out: device floats. */
+int m2s_grid_sdf_device(const m2s_mesh* mesh, const float first_cell[3],
+                        const float cell_size[3], const uint64_t cell_count[3], int sign,
+                        float* d_out, uint32_t* d_status, void* stream);
+
+/* ---- utilities ----------------------------------------------------------- */
+
+/* Stable LSD radix sort of (uint32 key, uint32 value) pairs on the device, the
+ * sort behind the LBVH build; exposed so tests can compare it bit for bit with
+ * a CPU stable sort.  Arrays are device pointers; results overwrite them. */
+int m2s_radix_sort_pairs_device(uint32_t* d_keys, uint32_t* d_values, uint64_t n, int key_bits,
+                                void* stream);
+
+/* Diagnostics of the last grid call on this thread: [seed updates, rounds,
+ * states relaxed, neighbour evaluations, ray hits, overflow recoveries,
+ * kernel launches, relax rounds launched]. */
+int m2s_last_grid_stats(uint64_t out[8]);
+
+/* When enabled (per thread), grid calls time their phases with CUDA events on
+ * their stream — the points the crate logs at generate/grid.rs:303-307,
+ * 342-346 and 369-373 — readable with m2s_last_grid_phase_ms as
+ * [seeding, propagation, rays, finalize] in milliseconds. */
+void m2s_set_profiling(int enable);
+int m2s_last_grid_phase_ms(float out[4]);
+
+const char* m2s_status_string(int status);
+/* Detail of the last failure on the calling thread ("" if none). */
+const char* m2s_last_error(void);
+/* 1 if a CUDA device of compute capability 10.x is usable, else 0. */
+int m2s_device_available(void);
+int m2s_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* M2S_H */

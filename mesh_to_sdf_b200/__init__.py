@@ -1,0 +1,389 @@
+"""mesh_to_sdf_b200 — signed distance fields from triangle meshes on NVIDIA B200.
+
+A drop-in for the two entry points of the Rust crate ``mesh_to_sdf``
+(``generate_sdf`` and ``generate_grid_sdf``) plus its resident-mesh API
+(``build_sdf_acceleration`` / ``query_sdf``), computed by hand-written CUDA
+kernels for sm_100a behind the C ABI of ``include/m2s.h``.  Names, arguments
+and error behaviour follow the crate (file:line citations are to
+``mesh_to_sdf/src/``); where the crate panics, this module raises
+:class:`M2SError` carrying the C status code.
+
+There is no CPU implementation here: every compute call runs on the GPU and
+fails loudly when ``libm2s.so`` or an sm_100 device is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+from dataclasses import dataclass
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+
+__all__ = [
+    "SignMethod", "AccelerationMethod", "Topology", "Grid", "SnapResult", "SdfAccelerationMesh", "M2SError",
+    "generate_sdf", "generate_grid_sdf", "build_sdf_acceleration", "query_sdf",
+    "query_vector_to_closest_point_rtree_bvh", "ALL_SDF_ACCELERATION_METHODS", "device_available",
+]
+
+F32 = np.float32
+
+STATUS = {
+    0: "OK", 1: "INVALID_ARGUMENT", 2: "NONFINITE_QUERY", 3: "INDEX_COUNT", 4: "INDEX_RANGE",
+    5: "NAN_DISTANCE", 6: "EMPTY_MESH", 7: "CUDA", 8: "OUT_OF_MEMORY", 9: "LIMIT", 10: "NO_DEVICE",
+}
+
+
+class M2SError(RuntimeError):
+    """A non-zero status from the C ABI (the crate panics in these cases)."""
+
+    def __init__(self, status: int, what: str):
+        L = _lib.lib()
+        detail = (L.m2s_last_error() or b"").decode(errors="replace")
+        msg = (L.m2s_status_string(status) or b"").decode()
+        super().__init__(f"{what}: {STATUS.get(status, status)} ({msg}){' — ' + detail if detail else ''}")
+        self.status = status
+
+
+def _check(st: int, what: str):
+    if st != 0:
+        raise M2SError(st, what)
+
+
+class SignMethod(enum.IntEnum):
+    """lib.rs:252-263."""
+    Raycast = 0
+    Normal = 1
+
+
+@dataclass(frozen=True)
+class AccelerationMethod:
+    """lib.rs:272-286: None(sign), Bvh(sign), Rtree, RtreeBvh (the default)."""
+    kind: int
+    sign: SignMethod = SignMethod.Raycast
+
+    NONE = 0
+    BVH = 1
+    RTREE = 2
+    RTREE_BVH = 3
+
+    @classmethod
+    def none(cls, sign: SignMethod = SignMethod.Raycast):
+        return cls(cls.NONE, SignMethod(sign))
+
+    @classmethod
+    def bvh(cls, sign: SignMethod = SignMethod.Raycast):
+        return cls(cls.BVH, SignMethod(sign))
+
+    @classmethod
+    def rtree(cls):
+        return cls(cls.RTREE, SignMethod.Normal)
+
+    @classmethod
+    def rtree_bvh(cls):
+        return cls(cls.RTREE_BVH, SignMethod.Raycast)
+
+    @classmethod
+    def default(cls):
+        return cls.rtree_bvh()
+
+    def __repr__(self):
+        name = {0: "None", 1: "Bvh", 2: "Rtree", 3: "RtreeBvh"}[self.kind]
+        return f"AccelerationMethod.{name}({self.sign.name})" if self.kind in (0, 1) else f"AccelerationMethod.{name}"
+
+
+# lib.rs:289-296
+ALL_SDF_ACCELERATION_METHODS = (
+    AccelerationMethod.none(SignMethod.Raycast), AccelerationMethod.none(SignMethod.Normal),
+    AccelerationMethod.bvh(SignMethod.Raycast), AccelerationMethod.bvh(SignMethod.Normal),
+    AccelerationMethod.rtree(), AccelerationMethod.rtree_bvh(),
+)
+
+
+@dataclass(frozen=True)
+class Topology:
+    """lib.rs:156-171: TriangleList(Option<&[I]>) / TriangleStrip(Option<&[I]>), I = u16 or u32."""
+    strip: bool
+    indices: Optional[np.ndarray] = None
+
+    @classmethod
+    def TriangleList(cls, indices=None):
+        return cls(False, None if indices is None else np.asarray(indices))
+
+    @classmethod
+    def TriangleStrip(cls, indices=None):
+        return cls(True, None if indices is None else np.asarray(indices))
+
+    def _ffi(self):
+        """(pointer-owner array or None, n_indices, index_bits, topology code)."""
+        if self.indices is None:
+            return None, 0, 0, int(self.strip)
+        idx = self.indices
+        if idx.dtype == np.uint16:
+            arr, bits = np.ascontiguousarray(idx.reshape(-1)), 16
+        else:
+            if idx.size and (idx.min() < 0 or idx.max() > 0xFFFFFFFF):
+                raise ValueError("indices must fit in u32")
+            arr, bits = np.ascontiguousarray(idx.reshape(-1).astype(np.uint32)), 32
+        return arr, len(arr), bits, int(self.strip)
+
+
+@dataclass(frozen=True)
+class SnapResult:
+    """grid.rs:10-17."""
+    inside: bool
+    cell: tuple
+
+    @classmethod
+    def Inside(cls, cell):
+        return cls(True, tuple(int(c) for c in cell))
+
+    @classmethod
+    def Outside(cls, cell):
+        return cls(False, tuple(int(c) for c in cell))
+
+
+class Grid:
+    """grid.rs:30-173.  All arithmetic is float32, in the crate's operation order."""
+
+    def __init__(self, first_cell, cell_size, cell_count):
+        self.first_cell = np.asarray(first_cell, F32).reshape(3).copy()
+        self.cell_size = np.asarray(cell_size, F32).reshape(3).copy()
+        self.cell_count = tuple(int(c) for c in cell_count)
+        if any(c < 0 for c in self.cell_count):
+            raise ValueError("cell counts must be non-negative")
+
+    @classmethod
+    def new(cls, first_cell, cell_size, cell_count):
+        return cls(first_cell, cell_size, cell_count)
+
+    @classmethod
+    def from_bounding_box(cls, bbox_min, bbox_max, cell_count):
+        # grid.rs:59-74
+        mn = np.asarray(bbox_min, F32).reshape(3)
+        mx = np.asarray(bbox_max, F32).reshape(3)
+        fc = np.array([F32(c) for c in cell_count], F32)
+        size = ((mx - mn).astype(F32) / fc).astype(F32)
+        first = (mn + (size * F32(0.5)).astype(F32)).astype(F32)
+        return cls(first, size, cell_count)
+
+    def get_first_cell(self):
+        return self.first_cell.copy()
+
+    def get_last_cell(self):
+        # grid.rs:82-88
+        n = np.array(self.cell_count, F32)
+        return (self.first_cell + (n * self.cell_size).astype(F32)).astype(F32)
+
+    def get_cell_size(self):
+        return self.cell_size.copy()
+
+    def get_cell_count(self):
+        return list(self.cell_count)
+
+    def get_total_cell_count(self):
+        return self.cell_count[0] * self.cell_count[1] * self.cell_count[2]
+
+    def get_bounding_box(self):
+        # grid.rs:110-119
+        mn = (self.first_cell - (self.cell_size * F32(0.5)).astype(F32)).astype(F32)
+        n = np.array(self.cell_count, F32)
+        mx = (mn + (n * self.cell_size).astype(F32)).astype(F32)
+        return mn, mx
+
+    def get_cell_idx(self, cell):
+        # grid.rs:122-124 (z fastest)
+        return int(cell[2]) + int(cell[1]) * self.cell_count[2] + int(cell[0]) * self.cell_count[1] * self.cell_count[2]
+
+    def get_cell_integer_coordinates(self, idx):
+        # grid.rs:127-132
+        nz, ny = self.cell_count[2], self.cell_count[1]
+        return [idx // (ny * nz), (idx // nz) % ny, idx % nz]
+
+    def get_cell_center(self, cell):
+        # grid.rs:135-141
+        c = np.array([F32(int(x)) for x in cell], F32)
+        return (self.first_cell + (c * self.cell_size).astype(F32)).astype(F32)
+
+    def cell_centers(self):
+        """All cell centres, (n, 3) float32, in output order."""
+        nx, ny, nz = self.cell_count
+        ix, iy, iz = np.meshgrid(np.arange(nx, dtype=F32), np.arange(ny, dtype=F32), np.arange(nz, dtype=F32),
+                                 indexing="ij")
+        c = np.stack([ix, iy, iz], -1).reshape(-1, 3)
+        return (self.first_cell + (c * self.cell_size).astype(F32)).astype(F32)
+
+    def snap_point_to_grid(self, point):
+        # grid.rs:145-170
+        p = np.asarray(point, F32).reshape(3)
+        rel = ((p - self.get_bounding_box()[0]).astype(F32) / self.cell_size).astype(F32)
+        out, inside = [], True
+        for d in range(3):
+            f = float(np.floor(rel[d]))
+            c = 0 if np.isnan(f) else int(max(min(f, 9.2e18), -9.2e18))
+            cl = min(max(c, 0), self.cell_count[d] - 1)
+            inside &= cl == c
+            out.append(cl)
+        return SnapResult.Inside(out) if inside else SnapResult.Outside(out)
+
+    def __repr__(self):
+        return f"Grid(first_cell={self.first_cell.tolist()}, cell_size={self.cell_size.tolist()}, " \
+               f"cell_count={list(self.cell_count)})"
+
+
+def _points(x, what="points"):
+    a = np.ascontiguousarray(np.asarray(x, dtype=F32).reshape(-1, 3))
+    return a
+
+
+def _vp(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+def device_available() -> bool:
+    return bool(_lib.lib().m2s_device_available())
+
+
+def generate_sdf(vertices, indices: Topology, query_points, acceleration_method: AccelerationMethod = None):
+    """lib.rs:364-391: signed distance of every query point (positive outside)."""
+    am = acceleration_method or AccelerationMethod.default()
+    v = _points(vertices)
+    q = _points(query_points)
+    idx, ni, bits, topo = indices._ffi()
+    out = np.empty(len(q), F32)
+    n = ctypes.c_uint64(0)
+    st = _lib.lib().m2s_generate_sdf(_vp(v), len(v), _vp(idx), ni, bits, topo, _vp(q), len(q), am.kind,
+                                     int(am.sign), _vp(out), ctypes.byref(n), None)
+    _check(st, "generate_sdf")
+    return out[: n.value]
+
+
+def generate_grid_sdf(vertices, indices: Topology, grid: Grid, sign_method: SignMethod = SignMethod.Raycast):
+    """generate/grid.rs:265-378: signed distances of every cell centre, z fastest."""
+    v = _points(vertices)
+    idx, ni, bits, topo = indices._ffi()
+    first = np.ascontiguousarray(grid.first_cell, F32)
+    size = np.ascontiguousarray(grid.cell_size, F32)
+    count = np.ascontiguousarray(np.array(grid.cell_count, np.uint64))
+    out = np.empty(grid.get_total_cell_count(), F32)
+    n = ctypes.c_uint64(0)
+    st = _lib.lib().m2s_generate_grid_sdf(_vp(v), len(v), _vp(idx), ni, bits, topo, _vp(first), _vp(size),
+                                          _vp(count), int(sign_method), _vp(out), ctypes.byref(n), None)
+    _check(st, "generate_grid_sdf")
+    return out[: n.value]
+
+
+GRID_STATS = ("seed_updates", "rounds", "states_relaxed", "neighbour_evals", "ray_hits", "overflow_recoveries",
+              "kernel_launches", "rounds_launched")
+
+
+def last_grid_stats():
+    """Counters of the last grid call on this thread (names in GRID_STATS)."""
+    a = np.zeros(8, np.uint64)
+    _lib.lib().m2s_last_grid_stats(_vp(a))
+    return dict(zip(GRID_STATS, (int(x) for x in a)))
+
+
+def set_profiling(enable: bool):
+    """Time grid phases with CUDA events (per thread); see last_grid_phase_ms()."""
+    _lib.lib().m2s_set_profiling(1 if enable else 0)
+
+
+def last_grid_phase_ms():
+    """{seeding, propagation, rays, finalize} device milliseconds of the last profiled grid call."""
+    a = np.zeros(4, np.float32)
+    _lib.lib().m2s_last_grid_phase_ms(_vp(a))
+    return dict(zip(("seeding", "propagation", "rays", "finalize"), (float(x) for x in a)))
+
+
+class SdfAccelerationMesh:
+    """lib.rs:303-312: a mesh and its LBVH resident in HBM (owns an m2s_mesh*)."""
+
+    def __init__(self, handle, method: AccelerationMethod):
+        self._h = ctypes.c_void_p(handle)
+        self.method = method
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def triangle_count(self):
+        return int(_lib.lib().m2s_mesh_triangle_count(self._h))
+
+    def close(self):
+        if self._h and self._h.value:
+            _lib.lib().m2s_mesh_free(self._h)
+            self._h = ctypes.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- device-resident variants (torch tensors on cuda) -----------------
+    def query_device(self, q, out, status=None, stream=None):
+        """query_sdf on device tensors: q (n,3) float32, out (n,) float32; asynchronous."""
+        st = _lib.lib().m2s_query_sdf_device(self._h, ctypes.c_void_p(q.data_ptr()), q.shape[0],
+                                             ctypes.c_void_p(out.data_ptr()),
+                                             None if status is None else ctypes.c_void_p(status.data_ptr()),
+                                             None if stream is None else ctypes.c_void_p(stream))
+        _check(st, "query_sdf_device")
+
+    def grid_device(self, grid: Grid, sign_method: SignMethod, out, status=None, stream=None):
+        """generate_grid_sdf into a device tensor `out` of grid.get_total_cell_count() float32."""
+        first = np.ascontiguousarray(grid.first_cell, F32)
+        size = np.ascontiguousarray(grid.cell_size, F32)
+        count = np.ascontiguousarray(np.array(grid.cell_count, np.uint64))
+        st = _lib.lib().m2s_grid_sdf_device(self._h, _vp(first), _vp(size), _vp(count), int(sign_method),
+                                            ctypes.c_void_p(out.data_ptr()),
+                                            None if status is None else ctypes.c_void_p(status.data_ptr()),
+                                            None if stream is None else ctypes.c_void_p(stream))
+        _check(st, "grid_sdf_device")
+
+
+def build_sdf_acceleration(vertices, indices: Topology, acceleration_method: AccelerationMethod = None):
+    """lib.rs:410-433; returns None where the crate does (RtreeBvh on an empty mesh)."""
+    am = acceleration_method or AccelerationMethod.default()
+    v = _points(vertices)
+    idx, ni, bits, topo = indices._ffi()
+    h = ctypes.c_void_p(None)
+    st = _lib.lib().m2s_build_sdf_acceleration(_vp(v), len(v), _vp(idx), ni, bits, topo, am.kind, int(am.sign),
+                                               ctypes.byref(h), None)
+    _check(st, "build_sdf_acceleration")
+    if not h.value:
+        return None
+    return SdfAccelerationMesh(h.value, am)
+
+
+def query_sdf(acceleration: SdfAccelerationMesh, query_points):
+    """lib.rs:463-485."""
+    q = _points(query_points)
+    out = np.empty(len(q), F32)
+    n = ctypes.c_uint64(0)
+    st = _lib.lib().m2s_query_sdf(acceleration.handle, _vp(q), len(q), _vp(out), ctypes.byref(n), None)
+    _check(st, "query_sdf")
+    return out[: n.value]
+
+
+def query_vector_to_closest_point_rtree_bvh(acceleration: SdfAccelerationMesh, query_points):
+    """rtree_bvh.rs:217-276: (closest point - query, inside) per query."""
+    q = _points(query_points)
+    vec = np.empty((len(q), 3), F32)
+    inside = np.empty(len(q), np.uint8)
+    n = ctypes.c_uint64(0)
+    st = _lib.lib().m2s_query_vector_to_closest_point(acceleration.handle, _vp(q), len(q), _vp(vec), _vp(inside),
+                                                      ctypes.byref(n), None)
+    _check(st, "query_vector_to_closest_point_rtree_bvh")
+    return vec[: n.value], inside[: n.value].astype(bool)
+
+
+def radix_sort_pairs_device(keys, values, key_bits=32, stream=None):
+    """Stable LSD radix sort of device uint32 (int32 tensors reinterpreted) key/value pairs, in place."""
+    st = _lib.lib().m2s_radix_sort_pairs_device(ctypes.c_void_p(keys.data_ptr()), ctypes.c_void_p(values.data_ptr()),
+                                                keys.numel(), int(key_bits),
+                                                None if stream is None else ctypes.c_void_p(stream))
+    _check(st, "radix_sort_pairs_device")

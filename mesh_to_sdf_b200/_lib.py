@@ -1,0 +1,63 @@
+"""ctypes binding of libm2s.so (the C ABI of include/m2s.h)."""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libm2s.so")
+_lock = threading.Lock()
+_lib = None
+
+P = ctypes.c_void_p
+U64 = ctypes.c_uint64
+I = ctypes.c_int
+
+# name -> (restype, argtypes); every function declared in include/m2s.h
+SIGNATURES = {
+    "m2s_generate_sdf": (I, [P, U64, P, U64, I, I, P, U64, I, I, P, P, P]),
+    "m2s_generate_grid_sdf": (I, [P, U64, P, U64, I, I, P, P, P, I, P, P, P]),
+    "m2s_build_sdf_acceleration": (I, [P, U64, P, U64, I, I, I, I, P, P]),
+    "m2s_query_sdf": (I, [P, P, U64, P, P, P]),
+    "m2s_query_vector_to_closest_point": (I, [P, P, U64, P, P, P, P]),
+    "m2s_mesh_free": (None, [P]),
+    "m2s_mesh_triangle_count": (U64, [P]),
+    "m2s_mesh_accel": (I, [P]),
+    "m2s_query_sdf_device": (I, [P, P, U64, P, P, P]),
+    "m2s_grid_sdf_device": (I, [P, P, P, P, I, P, P, P]),
+    "m2s_radix_sort_pairs_device": (I, [P, P, U64, I, P]),
+    "m2s_last_grid_stats": (I, [P]),
+    "m2s_set_profiling": (None, [I]),
+    "m2s_last_grid_phase_ms": (I, [P]),
+    "m2s_status_string": (ctypes.c_char_p, [I]),
+    "m2s_last_error": (ctypes.c_char_p, []),
+    "m2s_device_available": (I, []),
+    "m2s_version": (I, []),
+}
+
+
+class LibraryMissing(RuntimeError):
+    pass
+
+
+def lib():
+    """Loads libm2s.so (building it if the sources are newer).  Raises if it cannot be built."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            from . import build as _build
+
+            if not _build.up_to_date():
+                try:
+                    _build.build()
+                except Exception as e:  # no nvcc: the prebuilt library must exist
+                    if not os.path.exists(LIB_PATH):
+                        raise LibraryMissing(f"libm2s.so is missing and cannot be built: {e}") from e
+            L = ctypes.CDLL(LIB_PATH)
+            for name, (res, args) in SIGNATURES.items():
+                f = getattr(L, name)
+                f.restype = res
+                f.argtypes = args
+            _lib = L
+    return _lib

@@ -1,0 +1,180 @@
+// Device geometry for mesh_to_sdf_b200 (sm_100a).
+//
+// The arithmetic follows the Rust crate `mesh_to_sdf` operation by operation:
+// Rust never fuses a*b+c, so every add / sub / mul / div / sqrt here goes
+// through a round-to-nearest intrinsic (__fadd_rn and friends), which the
+// compiler may not contract into an FMA whatever -fmad says.  With the same
+// inputs the results are therefore bit-identical to the reference's f32 code.
+#pragma once
+
+#include <cstdint>
+
+namespace m2s {
+
+__device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fs(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fd(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ float fsqrt(float a) { return __fsqrt_rn(a); }
+
+struct P3 {
+  float x, y, z;
+};
+
+__device__ __forceinline__ P3 p3(float4 v) { return {v.x, v.y, v.z}; }
+__device__ __forceinline__ P3 vsub(P3 a, P3 b) { return {fs(a.x, b.x), fs(a.y, b.y), fs(a.z, b.z)}; }
+__device__ __forceinline__ P3 vadd(P3 a, P3 b) { return {fa(a.x, b.x), fa(a.y, b.y), fa(a.z, b.z)}; }
+__device__ __forceinline__ P3 vmul(P3 a, float s) { return {fm(a.x, s), fm(a.y, s), fm(a.z, s)}; }
+// point.rs:100-102 — (x*x' + y*y') + z*z'
+__device__ __forceinline__ float vdot(P3 a, P3 b) { return fa(fa(fm(a.x, b.x), fm(a.y, b.y)), fm(a.z, b.z)); }
+// point.rs:105-111
+__device__ __forceinline__ P3 vcross(P3 a, P3 b) {
+  return {fs(fm(a.y, b.z), fm(a.z, b.y)), fs(fm(a.z, b.x), fm(a.x, b.z)), fs(fm(a.x, b.y), fm(a.y, b.x))};
+}
+__device__ __forceinline__ float vget(P3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
+
+// Rust f32::clamp: a NaN stays NaN.
+__device__ __forceinline__ float rs_clamp01(float v) {
+  if (v < 0.0f) v = 0.0f;
+  if (v > 1.0f) v = 1.0f;
+  return v;
+}
+
+// Degenerate-triangle cases of geo.rs:73-88, decided once per triangle and kept
+// in the record: 0 = proper triangle, 1 = a point (all equal), 2 = segment a..c
+// (a == b), 3 = segment a..b (b == c or a == c).
+enum : int { TRI_PROPER = 0, TRI_POINT = 1, TRI_SEG_AC = 2, TRI_SEG_AB = 3 };
+
+__host__ __device__ __forceinline__ int degenerate_kind(float ax, float ay, float az, float bx, float by,
+                                                        float bz, float cx, float cy, float cz) {
+  bool ab = ax == bx && ay == by && az == bz;
+  bool bc = bx == cx && by == cy && bz == cz;
+  bool ac = ax == cx && ay == cy && az == cz;
+  if (ab && bc && ac) return TRI_POINT;
+  if (ab) return TRI_SEG_AC;
+  if (bc || ac) return TRI_SEG_AB;
+  return TRI_PROPER;
+}
+
+// geo.rs:141-151
+__device__ __forceinline__ P3 closest_point_segment(P3 p, P3 a, P3 b) {
+  P3 ab = vsub(b, a);
+  float m = vdot(ab, ab);
+  P3 ap = vsub(p, a);
+  float s = rs_clamp01(fd(vdot(ab, ap), m));
+  return vadd(a, vmul(ab, s));
+}
+
+// geo.rs:70-138 (Embree Voronoi regions) for a proper triangle.
+__device__ __forceinline__ P3 closest_point_proper(P3 p, P3 a, P3 b, P3 c) {
+  P3 ab = vsub(b, a);
+  P3 ac = vsub(c, a);
+  P3 ap = vsub(p, a);
+  float d1 = vdot(ab, ap);
+  float d2 = vdot(ac, ap);
+  if (d1 <= 0.0f && d2 <= 0.0f) return a;
+  P3 bp = vsub(p, b);
+  float d3 = vdot(ab, bp);
+  float d4 = vdot(ac, bp);
+  if (d3 >= 0.0f && d4 <= d3) return b;
+  P3 cp = vsub(p, c);
+  float d5 = vdot(ab, cp);
+  float d6 = vdot(ac, cp);
+  if (d6 >= 0.0f && d5 <= d6) return c;
+  float vc = fs(fm(d1, d4), fm(d3, d2));
+  if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) return vadd(a, vmul(ab, fd(d1, fs(d1, d3))));
+  float vb = fs(fm(d5, d2), fm(d1, d6));
+  if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) return vadd(a, vmul(ac, fd(d2, fs(d2, d6))));
+  float va = fs(fm(d3, d6), fm(d5, d4));
+  float d43 = fs(d4, d3), d56 = fs(d5, d6);
+  if (va <= 0.0f && d43 >= 0.0f && d56 >= 0.0f) return vadd(b, vmul(vsub(c, b), fd(d43, fa(d43, d56))));
+  float denom = fd(1.0f, fa(fa(va, vb), vc));
+  float v = fm(vb, denom);
+  float w = fm(vc, denom);
+  return vadd(vadd(a, vmul(ab, v)), vmul(ac, w));
+}
+
+// geo.rs:70-138 including the degenerate fallbacks (kind from degenerate_kind).
+__device__ __forceinline__ P3 closest_point_triangle(P3 p, P3 a, P3 b, P3 c, int kind) {
+  if (kind == TRI_PROPER) return closest_point_proper(p, a, b, c);
+  if (kind == TRI_POINT) return a;
+  if (kind == TRI_SEG_AC) return closest_point_segment(p, a, c);
+  return closest_point_segment(p, a, b);
+}
+
+// geo.rs:33-37
+__device__ __forceinline__ float point_triangle_distance2(P3 p, P3 a, P3 b, P3 c, int kind) {
+  P3 d = vsub(p, closest_point_triangle(p, a, b, c, kind));
+  return vdot(d, d);
+}
+
+// geo.rs:43-56: positive when (p - closest) . (ab x ac) > 0, else -distance.
+__device__ __forceinline__ float point_triangle_signed_distance(P3 p, P3 a, P3 b, P3 c, int kind) {
+  P3 cp = closest_point_triangle(p, a, b, c, kind);
+  P3 dir = vsub(p, cp);
+  P3 n = vcross(vsub(b, a), vsub(c, a));
+  float d = fsqrt(vdot(dir, dir));
+  return vdot(dir, n) > 0.0f ? d : -d;
+}
+
+// geo.rs:165-216 for a +axis ray; (y, z) of the projection rotate with the axis
+// as in the reference (X: y,z; Y: z,x; Z: x,y).  Returns true with *t on a hit.
+template <int AXIS>
+__device__ __forceinline__ bool ray_hit_aligned(P3 o, P3 t0, P3 t1, P3 t2, float* t_out) {
+  constexpr int IX = AXIS, IY = (AXIS + 1) % 3, IZ = (AXIS + 2) % 3;
+  P3 e01 = vsub(t1, t0), e12 = vsub(t2, t1), e20 = vsub(t0, t2);
+  P3 p0 = vsub(o, t0), p1 = vsub(o, t1), p2 = vsub(o, t2);
+  float w0 = fs(fm(vget(p1, IZ), vget(e12, IY)), fm(vget(p1, IY), vget(e12, IZ)));
+  float w1 = fs(fm(vget(p2, IZ), vget(e20, IY)), fm(vget(p2, IY), vget(e20, IZ)));
+  float w2 = fs(fm(vget(p0, IZ), vget(e01, IY)), fm(vget(p0, IY), vget(e01, IZ)));
+  if ((w0 < 0.0f && w1 < 0.0f && w2 < 0.0f) || (w0 > 0.0f && w1 > 0.0f && w2 > 0.0f)) {
+    float num = fa(fa(fm(w0, vget(p0, IX)), fm(w2, vget(p2, IX))), fm(w1, vget(p1, IX)));
+    float t = fd(-num, fa(fa(w0, w1), w2));
+    if (t > 0.0f) {
+      *t_out = t;
+      return true;
+    }
+  }
+  return false;
+}
+
+__device__ __forceinline__ bool ray_hit_axis(int axis, P3 o, P3 t0, P3 t1, P3 t2, float* t) {
+  if (axis == 0) return ray_hit_aligned<0>(o, t0, t1, t2, t);
+  if (axis == 1) return ray_hit_aligned<1>(o, t0, t1, t2, t);
+  return ray_hit_aligned<2>(o, t0, t1, t2, t);
+}
+
+// float-cmp 0.9 approx_eq!(f32, a, b, ulps = 2, epsilon = 1e-6): equal, or
+// |a - b| <= epsilon, or the i32 bit patterns (wrapping difference, saturating
+// abs) within 2.
+__device__ __forceinline__ bool approx_eq_band(float a, float b) {
+  if (a == b) return true;
+  if (fabsf(fs(a, b)) <= 1e-6f) return true;
+  int32_t diff = (int32_t)((uint32_t)__float_as_int(a) - (uint32_t)__float_as_int(b));
+  int32_t ad = diff == INT32_MIN ? INT32_MAX : (diff < 0 ? -diff : diff);
+  return ad <= 2;
+}
+
+// lib.rs:315-332: -1 Less, 0 Equal, 1 Greater; *nan set where the crate panics.
+__device__ __forceinline__ int compare_distances(float a, float b, bool* nan) {
+  float A = fabsf(a), B = fabsf(b);
+  if (approx_eq_band(A, B)) {
+    bool an = signbit(a), bn = signbit(b);
+    if (an && !bn) return 1;
+    if (!an && bn) return -1;
+  }
+  if (A < B) return -1;
+  if (A > B) return 1;
+  if (A == B) return 0;
+  *nan = true;
+  return 0;
+}
+
+// geo.rs:4-22: AABB grown by 1e-4 on every side (f32 min/max then -/+ 1e-4).
+__device__ __forceinline__ void padded_box(P3 a, P3 b, P3 c, P3* lo, P3* hi) {
+  const float e = 0.0001f;
+  *lo = {fs(fminf(a.x, fminf(b.x, c.x)), e), fs(fminf(a.y, fminf(b.y, c.y)), e), fs(fminf(a.z, fminf(b.z, c.z)), e)};
+  *hi = {fa(fmaxf(a.x, fmaxf(b.x, c.x)), e), fa(fmaxf(a.y, fmaxf(b.y, c.y)), e), fa(fmaxf(a.z, fmaxf(b.z, c.z)), e)};
+}
+
+}  // namespace m2s

@@ -1,0 +1,606 @@
+// generate_grid_sdf on the device (generate/grid.rs:265-684).
+//
+// 1. Seeding (generate_preheap, grid.rs:383-457): one warp per triangle walks
+//    the cells of its padded, snapped and widened box and keeps, per cell, the
+//    best (distance, triangle) under compare_distances.  Cells hold a packed
+//    64-bit key: high word = f32 bits of the distance, low word = triangle.
+// 2. Propagation (generate_heap + propagate_heap, grid.rs:464-558): the
+//    reference pops states from per-thread heaps in distance order and lets
+//    every accepted state — stale or not — evaluate its triangle on the 27
+//    cells of its 3x3x3 block.  Here the heap becomes delta-stepping: states
+//    are binned by distance (bucket width half a cell) and each round relaxes
+//    the lowest non-empty bucket, one warp per state and one lane per
+//    neighbour.  A proposal is accepted against the cell's value at the start
+//    of the round (a snapshot), and every accepted (cell, triangle) pair is
+//    propagated, as the reference propagates stale states.  Cells store the
+//    best proposal.  For unsigned (Raycast) distances the result does not
+//    depend on the order of atomics.
+// 3. Sign (compute_raycasts, grid.rs:568-684): every triangle is tested, with
+//    the reference's aligned ray test, against the rays that start at the cell
+//    centres of the three low faces and lie in its padded box.  A hit at t
+//    toggles bit k = min(floor(t / size), n - 1) of that ray's column; a
+//    suffix XOR turns toggles into per-cell crossing parities, and a cell is
+//    inside when at least two of its three parities are odd (grid.rs:622-639).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+
+#include "m2s_internal.cuh"
+
+namespace m2s {
+namespace {
+
+constexpr uint32_t NO_TRI = 0xFFFFFFFFu;
+constexpr unsigned long long KEY_EMPTY = (0x7F7FFFFFull << 32) | 0xFFFFFFFFull;  // (f32::MAX, none)
+constexpr int kRing = 16;            // pending distance buckets
+constexpr int kRoundsPerCheck = 16;  // rounds launched between host polls
+constexpr uint32_t kMaxRounds = 1u << 20;
+
+struct GridK {
+  float f[3], s[3];
+  int n[3];
+  unsigned long long ncell;
+  float inv_delta;  // 1 / bucket width
+};
+
+struct PropState {
+  unsigned long long b;  // current bucket
+  uint32_t slot[kRing];  // list holding bucket b + k
+  uint32_t cur;          // list relaxed this round
+  uint32_t count[kRing + 1];
+  uint32_t touched;
+  uint32_t done;
+  uint32_t overflow;
+  uint32_t round;
+  unsigned long long entries, evals, seeds, ray_hits;
+  unsigned long long min_bucket;
+  uint32_t recoveries;
+};
+
+__device__ __forceinline__ P3 center(const GridK& g, int x, int y, int z) {
+  // grid.rs:135-141: first + (i as f32) * size
+  return {fa(g.f[0], fm(__int2float_rn(x), g.s[0])), fa(g.f[1], fm(__int2float_rn(y), g.s[1])),
+          fa(g.f[2], fm(__int2float_rn(z), g.s[2]))};
+}
+__device__ __forceinline__ unsigned long long cell_index(const GridK& g, int x, int y, int z) {
+  return (unsigned long long)z + (unsigned long long)y * g.n[2] + (unsigned long long)x * g.n[1] * g.n[2];
+}
+
+// Rust `f as isize` (saturating, NaN -> 0).
+__device__ __forceinline__ long long sat_i64(float f) {
+  if (isnan(f)) return 0;
+  if (f >= 9.2233720368547758e18f) return LLONG_MAX;
+  if (f <= -9.2233720368547758e18f) return LLONG_MIN;
+  return (long long)f;
+}
+__device__ __forceinline__ unsigned long long sat_u64(float f) {
+  if (isnan(f) || f <= 0.0f) return 0;
+  if (f >= 1.8446744073709552e19f) return ULLONG_MAX;
+  return (unsigned long long)f;
+}
+
+// Grid::snap_point_to_grid (grid.rs:145-170), the cell only.
+__device__ __forceinline__ void snap(const GridK& g, P3 p, int cell[3]) {
+  float pc[3] = {p.x, p.y, p.z};
+  for (int d = 0; d < 3; ++d) {
+    float bbmin = fs(g.f[d], fm(g.s[d], 0.5f));  // get_bounding_box().0, grid.rs:111
+    long long c = sat_i64(floorf(fd(fs(pc[d], bbmin), g.s[d])));
+    long long hi = (long long)g.n[d] - 1;
+    cell[d] = (int)(c < 0 ? 0 : (c > hi ? hi : c));
+  }
+}
+
+template <int SIGN>
+__device__ __forceinline__ float cell_distance(P3 pos, P3 a, P3 b, P3 c, int kind) {
+  if (SIGN == M2S_SIGN_RAYCAST) return fsqrt(point_triangle_distance2(pos, a, b, c, kind));
+  return point_triangle_signed_distance(pos, a, b, c, kind);
+}
+
+__device__ __forceinline__ unsigned long long pack(float d, uint32_t tri) {
+  return ((unsigned long long)__float_as_uint(d) << 32) | tri;
+}
+__device__ __forceinline__ float key_dist(unsigned long long k) { return __uint_as_float((uint32_t)(k >> 32)); }
+__device__ __forceinline__ uint32_t key_tri(unsigned long long k) { return (uint32_t)k; }
+
+// Does `cand` beat `cur`?  Raycast: plain order of non-negative distances,
+// ties to the lower triangle.  Normal: compare_distances (lib.rs:315-332),
+// exact ties to the lower triangle.
+template <int SIGN>
+__device__ __forceinline__ bool beats(unsigned long long cand, unsigned long long cur, bool* nan) {
+  if (SIGN == M2S_SIGN_RAYCAST) return cand < cur;
+  float d = key_dist(cand), o = key_dist(cur);
+  int c = compare_distances(d, o, nan);
+  return c == -1 || (c == 0 && (uint32_t)(cand >> 32) == (uint32_t)(cur >> 32) && key_tri(cand) < key_tri(cur));
+}
+
+template <int SIGN>
+__device__ __forceinline__ bool update_min(unsigned long long* slot, unsigned long long cand, bool* nan) {
+  if (SIGN == M2S_SIGN_RAYCAST) return atomicMin(slot, cand) > cand;
+  unsigned long long old = *(volatile unsigned long long*)slot;
+  while (beats<SIGN>(cand, old, nan)) {
+    unsigned long long prev = atomicCAS(slot, old, cand);
+    if (prev == old) return true;
+    old = prev;
+  }
+  return false;
+}
+
+__global__ void k_fill_u64(unsigned long long* p, unsigned long long n, unsigned long long v) {
+  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (unsigned long long)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
+// ---- 1. seeding -------------------------------------------------------------
+template <int SIGN>
+__global__ void k_seed(GridK g, const TriRec* __restrict__ tris, uint32_t T, unsigned long long* keys,
+                       uint32_t* status, PropState* st) {
+  const uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (t >= T) return;
+  TriRec r = tris[t];
+  P3 a = p3(r.a), b = p3(r.b), c = p3(r.c);
+  int kind = __float_as_int(r.a.w);
+  P3 lo, hi;
+  padded_box(a, b, c, &lo, &hi);  // grid.rs:400
+  int mn[3], mx[3];
+  snap(g, lo, mn);
+  snap(g, hi, mx);
+  // grid.rs:410-426: widen by one cell where the box pokes past a centre.
+  P3 mnf = center(g, mn[0], mn[1], mn[2]);
+  P3 mxf = center(g, mx[0], mx[1], mx[2]);
+  for (int d = 0; d < 3; ++d) {
+    if (mn[d] > 0 && vget(mnf, d) > vget(lo, d)) mn[d] -= 1;
+    if (mx[d] < g.n[d] - 1 && vget(mxf, d) < vget(hi, d)) mx[d] += 1;
+  }
+  long long ex = mx[0] - mn[0] + 1, ey = mx[1] - mn[1] + 1, ez = mx[2] - mn[2] + 1;
+  if (ex <= 0 || ey <= 0 || ez <= 0) return;
+  long long total = ex * ey * ez;
+  bool nan = false;
+  uint32_t updates = 0;
+  for (long long k = lane; k < total; k += 32) {
+    int z = mn[2] + (int)(k % ez);
+    int y = mn[1] + (int)((k / ez) % ey);
+    int x = mn[0] + (int)(k / (ez * ey));
+    float d = cell_distance<SIGN>(center(g, x, y, z), a, b, c, kind);
+    if (isnan(d)) nan = true;
+    if (update_min<SIGN>(&keys[cell_index(g, x, y, z)], pack(d, t), &nan)) ++updates;
+  }
+  if (nan) atomicOr(status, bit(M2S_ERR_NAN_DISTANCE));
+  for (int o = 16; o; o >>= 1) updates += __shfl_xor_sync(0xFFFFFFFFu, updates, o);
+  if (lane == 0 && updates) atomicAdd(&st->seeds, (unsigned long long)updates);
+}
+
+__device__ __forceinline__ unsigned long long bucket_of(const GridK& g, float d) {
+  return sat_u64(floorf(fabsf(d) * g.inv_delta));
+}
+
+// Lowest bucket among flagged cells (seeded cells, or dirty cells on recovery).
+__global__ void k_min_bucket(GridK g, const unsigned long long* keys, const uint8_t* dirty, PropState* st) {
+  unsigned long long best = ULLONG_MAX;
+  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < g.ncell;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    unsigned long long k = keys[i];
+    bool flagged = dirty ? dirty[i] != 0 : k != KEY_EMPTY;
+    if (flagged && key_tri(k) != NO_TRI) best = min(best, bucket_of(g, key_dist(k)));
+  }
+  for (int o = 16; o; o >>= 1) best = min(best, __shfl_xor_sync(0xFFFFFFFFu, best, o));
+  if ((threadIdx.x & 31) == 0 && best != ULLONG_MAX) atomicMin(&st->min_bucket, best);
+}
+
+__global__ void k_state_init(PropState* st) {
+  // Lists 0..kRing-1 hold buckets b..b+kRing-1, list kRing is the relax list.
+  st->b = st->min_bucket == ULLONG_MAX ? 0 : st->min_bucket;
+  for (int k = 0; k < kRing; ++k) st->slot[k] = k;
+  st->cur = kRing;
+  for (int k = 0; k <= kRing; ++k) st->count[k] = 0;
+  st->touched = 0;
+  st->done = 0;
+  st->overflow = 0;
+}
+
+__device__ __forceinline__ void push_entry(const GridK& g, PropState* st, uint2* lists, uint32_t cap, uint8_t* dirty,
+                                           unsigned long long cell, uint32_t tri, float d) {
+  unsigned long long nb = bucket_of(g, d);
+  unsigned long long b = st->b;
+  unsigned long long rel = nb > b ? nb - b : 0;
+  uint32_t slot = st->slot[rel >= kRing ? kRing - 1 : rel];
+  uint32_t pos = atomicAdd(&st->count[slot], 1u);
+  if (pos < cap) {
+    lists[(unsigned long long)slot * cap + pos] = make_uint2((uint32_t)cell, tri);
+  } else {
+    dirty[cell] = 1;
+    atomicOr(&st->overflow, 1u);
+  }
+}
+
+__global__ void k_collect(GridK g, const unsigned long long* keys, uint8_t* dirty, bool from_dirty, PropState* st,
+                          uint2* lists, uint32_t cap) {
+  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < g.ncell;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    unsigned long long k = keys[i];
+    bool flagged = from_dirty ? dirty[i] != 0 : k != KEY_EMPTY;
+    if (!flagged) continue;
+    if (from_dirty) dirty[i] = 0;
+    if (key_tri(k) == NO_TRI) continue;
+    push_entry(g, st, lists, cap, dirty, i, key_tri(k), key_dist(k));
+  }
+}
+
+// Picks the next list to relax: the lowest non-empty bucket.
+__global__ void k_advance(PropState* st, uint32_t cap) {
+  if (st->done) return;
+  st->count[st->cur] = 0;
+  st->touched = 0;
+  for (int it = 0; it <= kRing; ++it) {
+    uint32_t s0 = st->slot[0];
+    if (st->count[s0] > 0) {
+      if (st->count[s0] > cap) st->count[s0] = cap;  // overflowed entries live on as dirty cells
+      st->slot[0] = st->cur;
+      st->cur = s0;
+      st->round += 1;
+      return;
+    }
+    st->b += 1;
+    for (int k = 0; k + 1 < kRing; ++k) st->slot[k] = st->slot[k + 1];
+    st->slot[kRing - 1] = s0;
+  }
+  st->done = 1;
+}
+
+// ---- 2. relaxation round -----------------------------------------------------
+template <int SIGN>
+__global__ void __launch_bounds__(256) k_relax(GridK g, const TriRec* __restrict__ tris,
+                                               const unsigned long long* __restrict__ snap_keys,
+                                               unsigned long long* work_keys, unsigned long long* tags, uint2* lists,
+                                               uint32_t cap, uint32_t* touched_list, uint8_t* dirty, PropState* st,
+                                               uint32_t* status) {
+  if (st->done) return;
+  const uint32_t n = st->count[st->cur];
+  const uint2* list = lists + (unsigned long long)st->cur * cap;
+  const uint32_t round = st->round;
+  const int lane = threadIdx.x & 31;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  // iproduct!(-1..=1, -1..=1, -1..=1) order (grid.rs:512): x outermost.
+  const int dx = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dz = lane % 3 - 1;
+  bool nan = false;
+  uint32_t evals = 0;
+  for (uint32_t e = warp; e < n; e += nwarps) {
+    const uint2 ent = list[e];
+    const unsigned long long cell = ent.x;
+    const uint32_t tri = ent.y;
+    const int z = (int)(cell % g.n[2]);
+    const int y = (int)((cell / g.n[2]) % g.n[1]);
+    const int x = (int)(cell / ((unsigned long long)g.n[1] * g.n[2]));
+    const int X = x + dx, Y = y + dy, Z = z + dz;
+    if (lane >= 27 || X < 0 || Y < 0 || Z < 0 || X >= g.n[0] || Y >= g.n[1] || Z >= g.n[2]) continue;
+    const TriRec r = tris[tri];
+    const float d = cell_distance<SIGN>(center(g, X, Y, Z), p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
+    ++evals;
+    if (isnan(d)) nan = true;
+    const unsigned long long j = cell_index(g, X, Y, Z);
+    const unsigned long long cand = pack(d, tri);
+    if (!beats<SIGN>(cand, snap_keys[j], &nan)) continue;
+    update_min<SIGN>(&work_keys[j], cand, &nan);
+    const unsigned long long tag = ((unsigned long long)round << 32) | tri;
+    if (atomicExch(&tags[j], tag) == tag) continue;  // this (cell, triangle) is already queued this round
+    uint32_t tp = atomicAdd(&st->touched, 1u);
+    if (tp < cap) touched_list[tp] = (uint32_t)j;
+    push_entry(g, st, lists, cap, dirty, j, tri, d);
+  }
+  if (nan) atomicOr(status, bit(M2S_ERR_NAN_DISTANCE));
+  for (int o = 16; o; o >>= 1) evals += __shfl_xor_sync(0xFFFFFFFFu, evals, o);
+  if (lane == 0 && evals) {
+    atomicAdd(&st->evals, (unsigned long long)evals);
+  }
+  if (threadIdx.x == 0 && blockIdx.x == 0) atomicAdd(&st->entries, (unsigned long long)n);
+}
+
+// Publishes this round's accepted values to the snapshot.
+__global__ void k_sync(GridK g, const unsigned long long* work_keys, unsigned long long* snap_keys,
+                       const uint32_t* touched_list, uint32_t cap, const PropState* st) {
+  if (st->done) return;
+  uint32_t n = st->touched;
+  if (n > cap) {
+    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < g.ncell;
+         i += (unsigned long long)gridDim.x * blockDim.x)
+      snap_keys[i] = work_keys[i];
+    return;
+  }
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t j = touched_list[i];
+    snap_keys[j] = work_keys[j];
+  }
+}
+
+// ---- 3. rays -------------------------------------------------------------------
+struct RayK {
+  uint32_t* bits[3];  // per axis: column-major toggles, words[col * W + w]
+  uint32_t words[3];  // W per axis
+};
+
+__device__ __forceinline__ unsigned long long column_of(const GridK& g, int axis, int x, int y, int z) {
+  if (axis == 0) return (unsigned long long)y * g.n[2] + z;
+  if (axis == 1) return (unsigned long long)x * g.n[2] + z;
+  return (unsigned long long)x * g.n[1] + y;
+}
+
+// Range of lattice indices along `d` whose ray origin can lie in [lo, hi];
+// one extra index on each side keeps it conservative.
+__device__ __forceinline__ void lattice_range(const GridK& g, int d, float lo, float hi, int* a, int* b) {
+  float u1 = (lo - g.f[d]) / g.s[d], u2 = (hi - g.f[d]) / g.s[d];
+  float umin = fminf(u1, u2), umax = fmaxf(u1, u2);
+  if (!(isfinite(umin) && isfinite(umax))) {
+    *a = 0;
+    *b = g.n[d] - 1;
+    return;
+  }
+  float fa_ = floorf(umin) - 1.0f, fb_ = ceilf(umax) + 1.0f;
+  *a = fa_ <= 0.0f ? 0 : (fa_ >= (float)(g.n[d] - 1) ? g.n[d] - 1 : (int)fa_);
+  *b = fb_ <= 0.0f ? 0 : (fb_ >= (float)(g.n[d] - 1) ? g.n[d] - 1 : (int)fb_);
+  if (fb_ < 0.0f || fa_ > (float)(g.n[d] - 1)) *b = *a - 1;  // no lattice point in range
+}
+
+template <int AXIS>
+__global__ void k_rays(GridK g, const TriRec* __restrict__ tris, uint32_t T, RayK rk, PropState* st) {
+  constexpr int IY = (AXIS + 1) % 3, IZ = (AXIS + 2) % 3;
+  const uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (t >= T) return;
+  TriRec r = tris[t];
+  P3 a = p3(r.a), b = p3(r.b), c = p3(r.c);
+  P3 lo, hi;
+  padded_box(a, b, c, &lo, &hi);
+  int j0, j1, k0, k1;
+  lattice_range(g, IY, vget(lo, IY), vget(hi, IY), &j0, &j1);
+  lattice_range(g, IZ, vget(lo, IZ), vget(hi, IZ), &k0, &k1);
+  if (j1 < j0 || k1 < k0) return;
+  const int nj = j1 - j0 + 1, nk = k1 - k0 + 1;
+  const long long total = (long long)nj * nk;
+  uint32_t* bitsA = rk.bits[AXIS];
+  const uint32_t W = rk.words[AXIS];
+  uint32_t hits = 0;
+  for (long long q = lane; q < total; q += 32) {
+    int c3[3];
+    c3[AXIS] = 0;
+    c3[IY] = j0 + (int)(q / nk);
+    c3[IZ] = k0 + (int)(q % nk);
+    P3 o = center(g, c3[0], c3[1], c3[2]);  // ray origin: a low-face cell centre (grid.rs:580)
+    float tt;
+    if (!ray_hit_aligned<AXIS>(o, a, b, c, &tt)) continue;
+    ++hits;
+    // grid.rs:604-607
+    unsigned long long kk = sat_u64(floorf(fd(tt, g.s[AXIS])));
+    unsigned long long last = (unsigned long long)g.n[AXIS] - 1;
+    uint32_t k = (uint32_t)(kk < last ? kk : last);
+    unsigned long long col = column_of(g, AXIS, c3[0], c3[1], c3[2]);
+    atomicXor(&bitsA[col * W + (k >> 5)], 1u << (k & 31));
+  }
+  for (int o = 16; o; o >>= 1) hits += __shfl_xor_sync(0xFFFFFFFFu, hits, o);
+  if (lane == 0 && hits) atomicAdd(&st->ray_hits, (unsigned long long)hits);
+}
+
+// Toggle bits -> suffix parity: bit i becomes the XOR of toggles i..n-1, i.e.
+// the parity of the hits whose cell range 0..=k covers cell i.
+__global__ void k_suffix(uint32_t* bits, unsigned long long ncols, uint32_t W) {
+  for (unsigned long long col = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; col < ncols;
+       col += (unsigned long long)gridDim.x * blockDim.x) {
+    uint32_t carry = 0;
+    uint32_t* w = bits + col * W;
+    for (int i = (int)W - 1; i >= 0; --i) {
+      uint32_t s = w[i];
+      s ^= s >> 1;
+      s ^= s >> 2;
+      s ^= s >> 4;
+      s ^= s >> 8;
+      s ^= s >> 16;
+      if (carry) s = ~s;
+      carry = s & 1u;
+      w[i] = s;
+    }
+  }
+}
+
+template <int SIGN>
+__global__ void k_finalize(GridK g, const unsigned long long* __restrict__ keys, RayK rk, float* __restrict__ out) {
+  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < g.ncell;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    float d = key_dist(keys[i]);
+    if (SIGN == M2S_SIGN_RAYCAST) {
+      int z = (int)(i % g.n[2]);
+      int y = (int)((i / g.n[2]) % g.n[1]);
+      int x = (int)(i / ((unsigned long long)g.n[1] * g.n[2]));
+      uint32_t px = (rk.bits[0][column_of(g, 0, x, y, z) * rk.words[0] + (x >> 5)] >> (x & 31)) & 1u;
+      uint32_t py = (rk.bits[1][column_of(g, 1, x, y, z) * rk.words[1] + (y >> 5)] >> (y & 31)) & 1u;
+      uint32_t pz = (rk.bits[2][column_of(g, 2, x, y, z) * rk.words[2] + (z >> 5)] >> (z & 31)) & 1u;
+      if (px + py + pz >= 2) d = -d;
+    }
+    out[i] = d;
+  }
+}
+
+unsigned blocks_for(unsigned long long n, int threads, unsigned cap = 148u * 16u) {
+  unsigned long long b = (n + threads - 1) / threads;
+  return (unsigned)std::max<unsigned long long>(1, std::min<unsigned long long>(b, cap));
+}
+
+}  // namespace
+
+int grid_sdf(const MeshView& m, const GridDesc& gd, int sign, float* d_out, uint32_t* d_status, cudaStream_t s,
+             uint64_t stats[kGridStats], float phase_ms[4]) {
+  const unsigned long long N = gd.cells();
+  if (N == 0) return M2S_OK;
+  for (int d = 0; d < 3; ++d)
+    if (gd.n[d] > 0x7FFFFFFFull) return M2S_ERR_INVALID_ARGUMENT;
+  if (N > 0xFFFFFFFFull) return M2S_ERR_INVALID_ARGUMENT;  // cells are addressed with 32-bit entries
+  GridK g;
+  for (int d = 0; d < 3; ++d) {
+    g.f[d] = gd.first[d];
+    g.s[d] = gd.size[d];
+    g.n[d] = (int)gd.n[d];
+  }
+  g.ncell = N;
+  float minsize = std::min(std::fabs(g.s[0]), std::min(std::fabs(g.s[1]), std::fabs(g.s[2])));
+  float delta = 0.5f * minsize;
+  g.inv_delta = (delta > 0.0f && std::isfinite(delta)) ? 1.0f / delta : 1.0f;
+
+  const uint32_t T = m.n_tris;
+  uint64_t launches = 0;
+  // Phase events (seeding, propagation, rays, finalize) when asked for.
+  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  if (phase_ms)
+    for (auto& e : ev) M2S_CUDA(cudaEventCreate(&e));
+  struct EvFree {
+    cudaEvent_t* e;
+    ~EvFree() {
+      for (int i = 0; i < 5; ++i)
+        if (e[i]) cudaEventDestroy(e[i]);
+    }
+  } evf{ev};
+  auto mark = [&](int i) {
+    if (phase_ms) cudaEventRecord(ev[i], s);
+  };
+  mark(0);
+  DevBuf<unsigned long long> snap_keys, work_keys, tags;
+  DevBuf<PropState> state;
+  int st;
+  if ((st = snap_keys.alloc(N, s)) || (st = state.alloc(1, s))) return st;
+  M2S_CUDA(cudaMemsetAsync(state.p, 0, sizeof(PropState), s));
+  k_fill_u64<<<blocks_for(N, 256), 256, 0, s>>>(snap_keys.p, N, KEY_EMPTY);
+  M2S_CUDA(cudaGetLastError());
+  ++launches;
+
+  if (T > 0) {
+    // ---- seeding
+    unsigned sb = (unsigned)((T * 32ull + 255) / 256);
+    if (sign == M2S_SIGN_RAYCAST)
+      k_seed<M2S_SIGN_RAYCAST><<<sb, 256, 0, s>>>(g, m.tris, T, snap_keys.p, d_status, state.p);
+    else
+      k_seed<M2S_SIGN_NORMAL><<<sb, 256, 0, s>>>(g, m.tris, T, snap_keys.p, d_status, state.p);
+    M2S_CUDA(cudaGetLastError());
+    ++launches;
+    mark(1);
+
+    // ---- propagation
+    const uint32_t cap = (uint32_t)std::min<unsigned long long>(
+        std::max<unsigned long long>(N / 4, std::min<unsigned long long>(N, 1ull << 20)), 0x7FFFFFFFull);
+    DevBuf<uint2> lists;
+    DevBuf<uint32_t> touched;
+    DevBuf<uint8_t> dirty;
+    if ((st = work_keys.alloc(N, s)) || (st = tags.alloc(N, s)) || (st = lists.alloc((kRing + 1ull) * cap, s)) ||
+        (st = touched.alloc(cap, s)) || (st = dirty.alloc(N, s)))
+      return st;
+    M2S_CUDA(cudaMemcpyAsync(work_keys.p, snap_keys.p, N * 8, cudaMemcpyDeviceToDevice, s));
+    M2S_CUDA(cudaMemsetAsync(tags.p, 0xFF, N * 8, s));
+    M2S_CUDA(cudaMemsetAsync(dirty.p, 0, N, s));
+    PropState* hst = nullptr;
+    M2S_CUDA(cudaMallocHost(&hst, sizeof(PropState)));
+    struct HostFree {
+      PropState* p;
+      ~HostFree() { cudaFreeHost(p); }
+    } hf{hst};
+
+    bool from_dirty = false;
+    uint32_t rounds_launched = 0, recoveries = 0;
+    unsigned relax_blocks = 148u * 8u;
+    for (int phase = 0;; ++phase) {
+      // min bucket of the cells to (re)start from, then bin them
+      unsigned long long ull_max = ULLONG_MAX;
+      M2S_CUDA(cudaMemcpyAsync(&state.p->min_bucket, &ull_max, 8, cudaMemcpyHostToDevice, s));
+      k_min_bucket<<<blocks_for(N, 256), 256, 0, s>>>(g, snap_keys.p, from_dirty ? dirty.p : nullptr, state.p);
+      k_state_init<<<1, 1, 0, s>>>(state.p);
+      k_collect<<<blocks_for(N, 256), 256, 0, s>>>(g, snap_keys.p, dirty.p, from_dirty, state.p, lists.p, cap);
+      k_advance<<<1, 1, 0, s>>>(state.p, cap);
+      M2S_CUDA(cudaGetLastError());
+      launches += 4;
+      while (true) {
+        for (int r = 0; r < kRoundsPerCheck; ++r) {
+          if (sign == M2S_SIGN_RAYCAST)
+            k_relax<M2S_SIGN_RAYCAST><<<relax_blocks, 256, 0, s>>>(g, m.tris, snap_keys.p, work_keys.p, tags.p,
+                                                                   lists.p, cap, touched.p, dirty.p, state.p,
+                                                                   d_status);
+          else
+            k_relax<M2S_SIGN_NORMAL><<<relax_blocks, 256, 0, s>>>(g, m.tris, snap_keys.p, work_keys.p, tags.p,
+                                                                  lists.p, cap, touched.p, dirty.p, state.p,
+                                                                  d_status);
+          k_sync<<<relax_blocks, 256, 0, s>>>(g, work_keys.p, snap_keys.p, touched.p, cap, state.p);
+          k_advance<<<1, 1, 0, s>>>(state.p, cap);
+        }
+        M2S_CUDA(cudaGetLastError());
+        rounds_launched += kRoundsPerCheck;
+        launches += 3ull * kRoundsPerCheck;
+        M2S_CUDA(cudaMemcpyAsync(hst, state.p, sizeof(PropState), cudaMemcpyDeviceToHost, s));
+        M2S_CUDA(cudaStreamSynchronize(s));
+        if (hst->done) break;
+        if (rounds_launched > kMaxRounds) return M2S_ERR_LIMIT;
+      }
+      if (!hst->overflow) break;
+      from_dirty = true;  // entries that did not fit: restart from their cells
+      ++recoveries;
+      if (phase > 64) return M2S_ERR_LIMIT;
+    }
+    if (stats) {
+      stats[0] = hst->seeds;
+      stats[1] = hst->round;
+      stats[2] = hst->entries;
+      stats[3] = hst->evals;
+      stats[5] = recoveries;
+      stats[7] = rounds_launched;
+    }
+  } else {
+    mark(1);
+  }
+  mark(2);
+
+  // ---- sign: rays + finalize
+  RayK rk{};
+  DevBuf<uint32_t> rbits[3];
+  if (sign == M2S_SIGN_RAYCAST) {
+    for (int a = 0; a < 3; ++a) {
+      unsigned long long ncols = N / gd.n[a];
+      rk.words[a] = (uint32_t)((gd.n[a] + 31) / 32);
+      if ((st = rbits[a].alloc(ncols * rk.words[a], s))) return st;
+      M2S_CUDA(cudaMemsetAsync(rbits[a].p, 0, ncols * rk.words[a] * 4, s));
+      rk.bits[a] = rbits[a].p;
+    }
+    if (T > 0) {
+      unsigned rb = (unsigned)((T * 32ull + 255) / 256);
+      k_rays<0><<<rb, 256, 0, s>>>(g, m.tris, T, rk, state.p);
+      k_rays<1><<<rb, 256, 0, s>>>(g, m.tris, T, rk, state.p);
+      k_rays<2><<<rb, 256, 0, s>>>(g, m.tris, T, rk, state.p);
+      M2S_CUDA(cudaGetLastError());
+      launches += 3;
+    }
+    for (int a = 0; a < 3; ++a) {
+      unsigned long long ncols = N / gd.n[a];
+      k_suffix<<<blocks_for(ncols, 256), 256, 0, s>>>(rk.bits[a], ncols, rk.words[a]);
+    }
+    launches += 3;
+    mark(3);
+    k_finalize<M2S_SIGN_RAYCAST><<<blocks_for(N, 256, 148u * 32u), 256, 0, s>>>(g, snap_keys.p, rk, d_out);
+    if (stats) {
+      unsigned long long h = 0;
+      M2S_CUDA(cudaMemcpyAsync(&h, &state.p->ray_hits, 8, cudaMemcpyDeviceToHost, s));
+      M2S_CUDA(cudaStreamSynchronize(s));
+      stats[4] = h;
+    }
+  } else {
+    mark(3);
+    k_finalize<M2S_SIGN_NORMAL><<<blocks_for(N, 256, 148u * 32u), 256, 0, s>>>(g, snap_keys.p, rk, d_out);
+  }
+  M2S_CUDA(cudaGetLastError());
+  ++launches;
+  mark(4);
+  if (stats) stats[6] = launches;
+  if (phase_ms) {
+    M2S_CUDA(cudaEventSynchronize(ev[4]));
+    for (int i = 0; i < 4; ++i) cudaEventElapsedTime(&phase_ms[i], ev[i], ev[i + 1]);
+  }
+  return M2S_OK;
+}
+
+}  // namespace m2s

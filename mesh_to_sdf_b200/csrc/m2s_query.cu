@@ -1,0 +1,478 @@
+// Point queries: generate_sdf / query_sdf for every AccelerationMethod.
+//
+//  * None  (generate/generic/default.rs:22-85): k_brute — every query against
+//    every triangle.  Triangle tiles are staged in shared memory by the bulk
+//    copy engine (cp.async.bulk + mbarrier, double-buffered); each thread owns
+//    one query and folds the tile in triangle order, exactly the reference's
+//    fold order.
+//  * Bvh(Raycast) / RtreeBvh (bvh.rs:256-332, rtree_bvh.rs:143-201): exact
+//    nearest triangle on the LBVH, then the 3-axis ray vote.
+//  * Rtree (rtree.rs:306-326): the nearest triangle's signed distance.
+//  * Bvh(Normal) (bvh.rs:268-281): compare_distances folded over the near-tie
+//    band of the nearest distance, in triangle order.
+//  * query_vector_to_closest_point_rtree_bvh (rtree_bvh.rs:217-276).
+#include <cuda_runtime.h>
+
+#include <cfloat>
+
+#include "m2s_internal.cuh"
+#include "m2s_tma.cuh"
+
+namespace m2s {
+namespace {
+
+constexpr float F32_MAX = 3.40282347e+38f;
+
+__device__ __forceinline__ P3 load_query(const float* q, uint64_t i) { return {q[3 * i], q[3 * i + 1], q[3 * i + 2]}; }
+
+// ---------------------------------------------------------------------------
+// K1: brute force over all triangles (AccelerationMethod::None).
+constexpr int kBfThreads = 128;
+constexpr int kBfTile = 256;  // triangles per stage: 256 * 48 B = 12 KiB
+
+template <int SIGN>
+__global__ void __launch_bounds__(kBfThreads) k_brute(const TriRec* __restrict__ tris, uint32_t T,
+                                                      const float* __restrict__ q, uint64_t nq,
+                                                      float* __restrict__ out, uint32_t* status) {
+  __shared__ __align__(128) TriRec tile[2][kBfTile];
+  __shared__ __align__(8) uint64_t bar[2];
+  const int tid = threadIdx.x;
+  const uint64_t qi = (uint64_t)blockIdx.x * kBfThreads + tid;
+  const bool valid = qi < nq;
+  const P3 p = valid ? load_query(q, qi) : P3{0.0f, 0.0f, 0.0f};
+  const uint32_t ntile = (T + kBfTile - 1) / kBfTile;
+
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  auto issue = [&](uint32_t i) {
+    uint32_t cnt = min((uint32_t)kBfTile, T - i * kBfTile);
+    uint32_t bytes = cnt * (uint32_t)sizeof(TriRec);
+    mbar_arrive_expect_tx(&bar[i & 1], bytes);
+    bulk_g2s(&tile[i & 1][0], tris + (uint64_t)i * kBfTile, bytes, &bar[i & 1]);
+  };
+  if (tid == 0) {
+    if (ntile > 0) issue(0);
+    if (ntile > 1) issue(1);
+  }
+
+  float best = SIGN == 0 ? INFINITY : F32_MAX;  // Raycast keeps the squared distance
+  uint32_t hits = 0;
+  bool nan = false, lost = false;
+  for (uint32_t i = 0; i < ntile; ++i) {
+    const int buf = i & 1;
+    if (!mbar_wait_bounded(&bar[buf], (i >> 1) & 1)) lost = true;
+    const uint32_t cnt = min((uint32_t)kBfTile, T - i * kBfTile);
+    const TriRec* tl = tile[buf];
+    if (!lost) {
+#pragma unroll 2
+      for (uint32_t j = 0; j < cnt; ++j) {
+        const float4 ra = tl[j].a, rb = tl[j].b, rc = tl[j].c;
+        const P3 a = p3(ra), b = p3(rb), c = p3(rc);
+        const int kind = __float_as_int(ra.w);
+        if (SIGN == 0) {
+          // default.rs:45-49 then :59-62 — min of distances, count of +X hits.
+          float d2 = point_triangle_distance2(p, a, b, c, kind);
+          best = fminf(best, d2);
+          float t;
+          hits += ray_hit_aligned<0>(p, a, b, c, &t) ? 1u : 0u;
+        } else {
+          // default.rs:51-53 then :63-70 — compare_distances fold.
+          float d = point_triangle_signed_distance(p, a, b, c, kind);
+          if (compare_distances(d, best, &nan) == -1) best = d;
+        }
+      }
+    }
+    __syncthreads();
+    if (tid == 0 && i + 2 < ntile) {
+      fence_proxy_async_smem();
+      issue(i + 2);
+    }
+  }
+  if (lost) atomicOr(status, bit(M2S_ERR_LIMIT));
+  if (nan) atomicOr(status, bit(M2S_ERR_NAN_DISTANCE));
+  if (!valid) return;
+  float r;
+  if (SIGN == 0) {
+    // sqrt(min d2) == min sqrt(d2) (IEEE sqrt is monotone); f32::MAX start value.
+    float d = fminf(F32_MAX, fsqrt(best));
+    r = (hits & 1u) ? -d : d;
+  } else {
+    r = best;
+  }
+  out[qi] = r;
+}
+
+// ---------------------------------------------------------------------------
+// LBVH traversals.
+constexpr int kStack = 64;
+
+__device__ __forceinline__ float box_dist2(P3 p, float4 lo, float4 hi) {
+  float dx = fmaxf(fmaxf(lo.x - p.x, p.x - hi.x), 0.0f);
+  float dy = fmaxf(fmaxf(lo.y - p.y, p.y - hi.y), 0.0f);
+  float dz = fmaxf(fmaxf(lo.z - p.z, p.z - hi.z), 0.0f);
+  return dx * dx + dy * dy + dz * dz;
+}
+
+__device__ __forceinline__ BvhNode load_node(const BvhNode* nodes, uint32_t i) {
+  const float4* f = reinterpret_cast<const float4*>(nodes + i);
+  BvhNode n;
+  n.l_lo = __ldg(f);
+  n.l_hi = __ldg(f + 1);
+  n.r_lo = __ldg(f + 2);
+  n.r_hi = __ldg(f + 3);
+  return n;
+}
+
+__device__ __forceinline__ TriRec load_tri(const TriRec* t, uint32_t i) {
+  const float4* f = reinterpret_cast<const float4*>(t + i);
+  return {__ldg(f), __ldg(f + 1), __ldg(f + 2)};
+}
+
+struct Nearest {
+  float d2;
+  uint32_t tri;   // crate triangle index
+  uint32_t leaf;  // LBVH leaf position
+};
+
+// Exact nearest triangle under the f32 point_triangle_distance2 (geo.rs:33-37),
+// ties to the lowest triangle index.  Boxes are padded by 1e-4 (geo.rs:4-22),
+// which keeps the f32 box test conservative.
+__device__ Nearest nearest_triangle(const MeshView& m, P3 p, bool* overflow) {
+  Nearest best{INFINITY, 0xFFFFFFFFu, 0};
+  auto eval = [&](uint32_t leaf) {
+    TriRec r = load_tri(m.stris, leaf);
+    float d2 = point_triangle_distance2(p, p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
+    uint32_t idx = __float_as_uint(r.b.w);
+    if (d2 < best.d2 || (d2 == best.d2 && idx < best.tri)) best = {d2, idx, leaf};
+  };
+  if (m.root & LEAF_BIT) {
+    eval(m.root & ~LEAF_BIT);
+    return best;
+  }
+  uint32_t st_node[kStack];
+  float st_dist[kStack];
+  int sp = 0;
+  uint32_t node = 0;
+  while (true) {
+    BvhNode nd = load_node(m.nodes, node);
+    float dl = box_dist2(p, nd.l_lo, nd.l_hi), dr = box_dist2(p, nd.r_lo, nd.r_hi);
+    uint32_t L = __float_as_uint(nd.l_lo.w), R = __float_as_uint(nd.l_hi.w);
+    bool goL = dl <= best.d2, goR = dr <= best.d2;
+    if (goL && (L & LEAF_BIT)) {
+      eval(L & ~LEAF_BIT);
+      goL = false;
+    }
+    if (goR && (R & LEAF_BIT)) {
+      eval(R & ~LEAF_BIT);
+      goR = false;
+    }
+    goL = goL && dl <= best.d2;
+    goR = goR && dr <= best.d2;
+    if (goL && goR) {
+      bool lfirst = dl <= dr;
+      if (sp < kStack) {
+        st_node[sp] = lfirst ? R : L;
+        st_dist[sp] = lfirst ? dr : dl;
+        ++sp;
+      } else {
+        *overflow = true;
+      }
+      node = lfirst ? L : R;
+      continue;
+    }
+    if (goL) {
+      node = L;
+      continue;
+    }
+    if (goR) {
+      node = R;
+      continue;
+    }
+    bool found = false;
+    while (sp > 0) {
+      --sp;
+      if (st_dist[sp] <= best.d2) {
+        node = st_node[sp];
+        found = true;
+        break;
+      }
+    }
+    if (!found) break;
+  }
+  return best;
+}
+
+// Number of triangles the +AXIS ray from o crosses (geo.rs:165-216).  A box is
+// entered when the ray's (y, z) lies inside it and its far side is ahead of o.
+template <int AXIS>
+__device__ uint32_t ray_crossings(const MeshView& m, P3 o, bool* overflow) {
+  constexpr int IY = (AXIS + 1) % 3, IZ = (AXIS + 2) % 3;
+  const float oy = vget(o, IY), oz = vget(o, IZ), ox = vget(o, AXIS);
+  uint32_t count = 0;
+  auto test = [&](uint32_t leaf) {
+    TriRec r = load_tri(m.stris, leaf);
+    float t;
+    count += ray_hit_aligned<AXIS>(o, p3(r.a), p3(r.b), p3(r.c), &t) ? 1u : 0u;
+  };
+  auto inside = [&](float4 lo, float4 hi) {
+    float loy = IY == 0 ? lo.x : (IY == 1 ? lo.y : lo.z), hiy = IY == 0 ? hi.x : (IY == 1 ? hi.y : hi.z);
+    float loz = IZ == 0 ? lo.x : (IZ == 1 ? lo.y : lo.z), hiz = IZ == 0 ? hi.x : (IZ == 1 ? hi.y : hi.z);
+    float hix = AXIS == 0 ? hi.x : (AXIS == 1 ? hi.y : hi.z);
+    return oy >= loy && oy <= hiy && oz >= loz && oz <= hiz && hix >= ox;
+  };
+  if (m.root & LEAF_BIT) {
+    test(m.root & ~LEAF_BIT);
+    return count;
+  }
+  uint32_t stack[kStack];
+  int sp = 0;
+  uint32_t node = 0;
+  while (true) {
+    BvhNode nd = load_node(m.nodes, node);
+    uint32_t L = __float_as_uint(nd.l_lo.w), R = __float_as_uint(nd.l_hi.w);
+    bool goL = inside(nd.l_lo, nd.l_hi), goR = inside(nd.r_lo, nd.r_hi);
+    if (goL && (L & LEAF_BIT)) {
+      test(L & ~LEAF_BIT);
+      goL = false;
+    }
+    if (goR && (R & LEAF_BIT)) {
+      test(R & ~LEAF_BIT);
+      goR = false;
+    }
+    if (goL && goR) {
+      if (sp < kStack) stack[sp++] = R;
+      else *overflow = true;
+      node = L;
+      continue;
+    }
+    if (goL) {
+      node = L;
+      continue;
+    }
+    if (goR) {
+      node = R;
+      continue;
+    }
+    if (sp == 0) break;
+    node = stack[--sp];
+  }
+  return count;
+}
+
+// bvh.rs:293-328 / rtree_bvh.rs:163-199: inside when >= 2 of 3 axis rays are odd.
+__device__ __forceinline__ bool vote_inside(const MeshView& m, P3 p, bool* overflow) {
+  int insides = (ray_crossings<0>(m, p, overflow) & 1u) + (ray_crossings<1>(m, p, overflow) & 1u) +
+                (ray_crossings<2>(m, p, overflow) & 1u);
+  return insides > 1;
+}
+
+// Bvh(Normal): compare_distances over every triangle whose |signed distance|
+// lies in the near-tie band of the nearest distance, folded in triangle order
+// from f32::MAX with the rule of bvh.rs:277-279.
+constexpr int kBand = 32;
+
+__device__ float normal_band_fold(const MeshView& m, P3 p, float d2min, bool* nan, bool* overflow) {
+  const double band = sqrt((double)d2min) * (1.0 + 1e-5) + 4e-6;
+  const float reach = (float)((band + 2e-4) * (1.0 + 1e-6));
+  const float reach2 = reach * reach;
+  uint32_t c_idx[kBand];
+  float c_d[kBand];
+  int n = 0;
+  bool full = false;
+  auto consider = [&](const TriRec& r) {
+    float d = point_triangle_signed_distance(p, p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
+    if (!(fabs((double)d) <= band)) return;
+    if (n < kBand) {
+      c_idx[n] = __float_as_uint(r.b.w);
+      c_d[n] = d;
+      ++n;
+    } else {
+      full = true;
+    }
+  };
+  if (m.root & LEAF_BIT) {
+    consider(load_tri(m.stris, m.root & ~LEAF_BIT));
+  } else {
+    uint32_t stack[kStack];
+    int sp = 0;
+    uint32_t node = 0;
+    while (true) {
+      BvhNode nd = load_node(m.nodes, node);
+      uint32_t L = __float_as_uint(nd.l_lo.w), R = __float_as_uint(nd.l_hi.w);
+      bool goL = box_dist2(p, nd.l_lo, nd.l_hi) <= reach2, goR = box_dist2(p, nd.r_lo, nd.r_hi) <= reach2;
+      if (goL && (L & LEAF_BIT)) {
+        consider(load_tri(m.stris, L & ~LEAF_BIT));
+        goL = false;
+      }
+      if (goR && (R & LEAF_BIT)) {
+        consider(load_tri(m.stris, R & ~LEAF_BIT));
+        goR = false;
+      }
+      if (goL && goR) {
+        if (sp < kStack) stack[sp++] = R;
+        else *overflow = true;
+        node = L;
+        continue;
+      }
+      if (goL) {
+        node = L;
+        continue;
+      }
+      if (goR) {
+        node = R;
+        continue;
+      }
+      if (sp == 0) break;
+      node = stack[--sp];
+    }
+  }
+  float best = F32_MAX;
+  if (full) {
+    // More ties than the register list holds: scan the band in triangle order.
+    for (uint32_t t = 0; t < m.n_tris; ++t) {
+      TriRec r = load_tri(m.tris, t);
+      float d = point_triangle_signed_distance(p, p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
+      if (!(fabs((double)d) <= band)) continue;
+      if (compare_distances(best, d, nan) == 1) best = d;
+    }
+    return best;
+  }
+  for (int i = 1; i < n; ++i) {  // insertion sort by triangle index
+    uint32_t ki = c_idx[i];
+    float di = c_d[i];
+    int j = i - 1;
+    while (j >= 0 && c_idx[j] > ki) {
+      c_idx[j + 1] = c_idx[j];
+      c_d[j + 1] = c_d[j];
+      --j;
+    }
+    c_idx[j + 1] = ki;
+    c_d[j + 1] = di;
+  }
+  for (int i = 0; i < n; ++i)
+    if (compare_distances(best, c_d[i], nan) == 1) best = c_d[i];
+  return best;
+}
+
+enum QueryMode { Q_BVH_RAYCAST = 0, Q_BVH_NORMAL = 1, Q_RTREE = 2, Q_VECTOR = 3 };
+
+template <int MODE>
+__global__ void __launch_bounds__(128) k_query(MeshView m, const float* __restrict__ q,
+                                               const uint32_t* __restrict__ order, uint64_t nq,
+                                               float* __restrict__ out, float* __restrict__ vec,
+                                               uint8_t* __restrict__ inside_out, uint32_t* status) {
+  uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nq) return;
+  uint64_t i = order ? order[k] : k;
+  P3 p = load_query(q, i);
+  bool overflow = false, nan = false;
+  Nearest nn = nearest_triangle(m, p, &overflow);
+  if (nn.tri == 0xFFFFFFFFu) nn = {INFINITY, 0u, 0u};  // every distance NaN
+  if (MODE == Q_BVH_RAYCAST) {
+    float d = fminf(F32_MAX, fsqrt(nn.d2));
+    out[i] = vote_inside(m, p, &overflow) ? -d : d;
+  } else if (MODE == Q_RTREE) {
+    TriRec r = load_tri(m.tris, nn.tri);
+    out[i] = point_triangle_signed_distance(p, p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
+  } else if (MODE == Q_BVH_NORMAL) {
+    out[i] = normal_band_fold(m, p, nn.d2, &nan, &overflow);
+  } else {
+    TriRec r = load_tri(m.tris, nn.tri);
+    P3 cp = closest_point_triangle(p, p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
+    P3 v = vsub(cp, p);  // rtree_bvh.rs:273
+    vec[3 * i] = v.x;
+    vec[3 * i + 1] = v.y;
+    vec[3 * i + 2] = v.z;
+    inside_out[i] = vote_inside(m, p, &overflow) ? 1 : 0;
+  }
+  if (overflow) atomicOr(status, bit(M2S_ERR_LIMIT));
+  if (nan) atomicOr(status, bit(M2S_ERR_NAN_DISTANCE));
+}
+
+// Morton order of the queries (spatially coherent warps).
+__global__ void k_query_keys(const float* __restrict__ q, uint64_t nq, MeshView m, uint32_t* keys, uint32_t* vals) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nq) return;
+  float4 lo, hi;
+  if (m.root & LEAF_BIT) {
+    TriRec r = m.stris[0];
+    lo = make_float4(fminf(r.a.x, fminf(r.b.x, r.c.x)), fminf(r.a.y, fminf(r.b.y, r.c.y)),
+                     fminf(r.a.z, fminf(r.b.z, r.c.z)), 0);
+    hi = make_float4(fmaxf(r.a.x, fmaxf(r.b.x, r.c.x)), fmaxf(r.a.y, fmaxf(r.b.y, r.c.y)),
+                     fmaxf(r.a.z, fmaxf(r.b.z, r.c.z)), 0);
+  } else {
+    BvhNode nd = m.nodes[0];
+    lo = make_float4(fminf(nd.l_lo.x, nd.r_lo.x), fminf(nd.l_lo.y, nd.r_lo.y), fminf(nd.l_lo.z, nd.r_lo.z), 0);
+    hi = make_float4(fmaxf(nd.l_hi.x, nd.r_hi.x), fmaxf(nd.l_hi.y, nd.r_hi.y), fmaxf(nd.l_hi.z, nd.r_hi.z), 0);
+  }
+  P3 p = load_query(q, i);
+  float c[3] = {p.x, p.y, p.z}, l[3] = {lo.x, lo.y, lo.z}, h[3] = {hi.x, hi.y, hi.z};
+  uint32_t key = 0;
+  for (int d = 0; d < 3; ++d) {
+    float ext = h[d] - l[d];
+    float u = ext > 0.0f ? (c[d] - l[d]) / ext : 0.0f;
+    uint32_t v = (uint32_t)fminf(fmaxf(u * 1024.0f, 0.0f), 1023.0f);
+    for (int b = 0; b < 10; ++b) key |= ((v >> b) & 1u) << (3 * b + (2 - d));
+  }
+  keys[i] = key;
+  vals[i] = (uint32_t)i;
+}
+
+}  // namespace
+
+int brute_force_sdf(const MeshView& m, int sign, const float* d_q, uint64_t nq, float* d_out, uint32_t* d_status,
+                    cudaStream_t s) {
+  if (nq == 0) return M2S_OK;
+  unsigned blocks = (unsigned)((nq + kBfThreads - 1) / kBfThreads);
+  if (sign == M2S_SIGN_RAYCAST)
+    k_brute<0><<<blocks, kBfThreads, 0, s>>>(m.tris, m.n_tris, d_q, nq, d_out, d_status);
+  else
+    k_brute<1><<<blocks, kBfThreads, 0, s>>>(m.tris, m.n_tris, d_q, nq, d_out, d_status);
+  M2S_CUDA(cudaGetLastError());
+  return M2S_OK;
+}
+
+int query_points(const MeshView& m, int accel, int sign, const float* d_q, uint64_t nq, float* d_out, float* d_vec,
+                 uint8_t* d_inside, uint32_t* d_status, cudaStream_t s) {
+  if (nq == 0) return M2S_OK;
+  if (accel == M2S_ACCEL_NONE && !d_vec) return brute_force_sdf(m, sign, d_q, nq, d_out, d_status, s);
+  if (m.n_tris == 0) return M2S_ERR_EMPTY_MESH;
+  if (nq > 0xFFFFFFFFull) return M2S_ERR_INVALID_ARGUMENT;
+  // Morton-ordered launch for large batches.
+  DevBuf<uint32_t> keys, order;
+  const uint32_t* ord = nullptr;
+  int st;
+  if (nq >= 4096) {
+    if ((st = keys.alloc(nq, s)) || (st = order.alloc(nq, s))) return st;
+    k_query_keys<<<(unsigned)((nq + 255) / 256), 256, 0, s>>>(d_q, nq, m, keys.p, order.p);
+    M2S_CUDA(cudaGetLastError());
+    if ((st = radix_sort_pairs(keys.p, order.p, nq, 30, s))) return st;
+    ord = order.p;
+  }
+  unsigned blocks = (unsigned)((nq + 127) / 128);
+  int mode = d_vec ? Q_VECTOR
+                   : (accel == M2S_ACCEL_RTREE ? Q_RTREE
+                                               : ((accel == M2S_ACCEL_BVH && sign == M2S_SIGN_NORMAL) ? Q_BVH_NORMAL
+                                                                                                      : Q_BVH_RAYCAST));
+  switch (mode) {
+    case Q_BVH_RAYCAST:
+      k_query<Q_BVH_RAYCAST><<<blocks, 128, 0, s>>>(m, d_q, ord, nq, d_out, nullptr, nullptr, d_status);
+      break;
+    case Q_BVH_NORMAL:
+      k_query<Q_BVH_NORMAL><<<blocks, 128, 0, s>>>(m, d_q, ord, nq, d_out, nullptr, nullptr, d_status);
+      break;
+    case Q_RTREE:
+      k_query<Q_RTREE><<<blocks, 128, 0, s>>>(m, d_q, ord, nq, d_out, nullptr, nullptr, d_status);
+      break;
+    default:
+      k_query<Q_VECTOR><<<blocks, 128, 0, s>>>(m, d_q, ord, nq, nullptr, d_vec, d_inside, d_status);
+  }
+  M2S_CUDA(cudaGetLastError());
+  return M2S_OK;
+}
+
+}  // namespace m2s

@@ -1,0 +1,336 @@
+"""GPU parity: the CUDA path (through the C ABI) against the CPU oracle.
+
+Bars, as stated per test:
+  * point queries: bit-exact (every method; Rtree and Bvh(Normal) use the
+    oracle's pinned tie order, lowest triangle index first);
+  * grids: signs exact cell for cell (Raycast); distances are values of real
+    triangles (never below the exact nearest distance) and differ from the
+    single-heap reference only in a small fraction of cells — the reference's
+    own propagation is order-dependent (its 8-thread run differs from its
+    1-thread run), and the tests bound the GPU by that envelope.
+"""
+import numpy as np
+import pytest
+
+import mesh_to_sdf_b200 as m2s
+from mesh_to_sdf_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+T = m2s.Topology
+A = m2s.AccelerationMethod
+S = m2s.SignMethod
+
+ORC_ACCEL = {A.NONE: "none", A.BVH: "bvh", A.RTREE: "rtree", A.RTREE_BVH: "rtree_bvh"}
+
+TETRA_V = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, -1]], np.float32)
+TETRA_IDX = np.array([0, 1, 2, 0, 2, 3, 0, 3, 1, 1, 3, 2], np.uint32)
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _device():
+    if not m2s.device_available():
+        pytest.fail("no sm_100 device: the GPU suite must run on a B200")
+
+
+def bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+
+
+def assert_bit_equal(gpu, ref, what):
+    gpu, ref = np.asarray(gpu, np.float32), np.asarray(ref, np.float32)
+    assert gpu.shape == ref.shape, what
+    bad = np.nonzero(bits(gpu) != bits(ref))[0]
+    assert len(bad) == 0, f"{what}: {len(bad)} of {len(gpu)} differ, e.g. idx {bad[:5]} gpu {gpu[bad[:5]]} ref {ref[bad[:5]]}"
+
+
+def orc_sdf(orc, v, idx, q, am, strip=False):
+    return orc.generate_sdf(v, idx, q, ORC_ACCEL[am.kind], int(am.sign), strip=strip)
+
+
+# ----------------------------------------------------------------- known answers
+def test_waterproof_tetra_all_methods(orc):
+    # lib.rs:494-524 points, every method, bit-exact against the oracle
+    q = np.array([[0, 0, 0], [0.5, 0, 0], [0.2, 0.2, 0], [0.2, 0.2, 0.05], [0.2, 0.2, -0.05], [1, 1, 0.05],
+                  [1, 1, -0.05], [1, 1, 0], [0, 0, -1.05], [0, 0, -0.95], [0.5, 0.5, -0.5], [0.5 - 1e-6, 0.5, -0.5],
+                  [0.5, 0.5 - 1e-6, -0.5], [0.5, 0.5, -0.5 - 1e-6]], np.float32)
+    for am in m2s.ALL_SDF_ACCELERATION_METHODS:
+        gpu = m2s.generate_sdf(TETRA_V, T.TriangleList(TETRA_IDX), q, am)
+        assert_bit_equal(gpu, orc_sdf(orc, TETRA_V, TETRA_IDX, q, am), repr(am))
+
+
+def test_hole_and_reversed_normal(orc):
+    # lib.rs:526-555
+    sdf = m2s.generate_sdf(TETRA_V, T.TriangleList(TETRA_IDX[:-3]), [[1.0, 1.0, -0.05]], A.bvh(S.Raycast))
+    assert sdf[0] == np.sqrt(np.float32(0.05 * 0.05 + 0.5 * 0.5 + 0.5 * 0.5), dtype=np.float32)
+    idx = TETRA_IDX.copy()
+    idx[0], idx[2] = TETRA_IDX[2], TETRA_IDX[0]
+    assert m2s.generate_sdf(TETRA_V, T.TriangleList(idx), [[0.2, 0.2, 0.05]], A.bvh(S.Raycast))[0] == np.float32(0.05)
+
+
+def test_doc_examples():
+    # lib.rs:10-31, 342-362, 440-461; generate/grid.rs:204-231
+    v = [[0.5, 1.5, 0.5], [1.0, 2.0, 3.0], [1.0, 3.0, 7.0]]
+    idx = np.array([0, 1, 2], np.uint32)
+    assert m2s.generate_sdf(v, T.TriangleList(idx), [[0.5, 0.5, 0.5]], A.rtree_bvh()).tolist() == [1.0]
+    v = [[0.0, 1.0, 0.0], [1.0, 2.0, 3.0], [1.0, 3.0, 4.0]]
+    assert m2s.generate_sdf(v, T.TriangleList(idx), [[0.0, 0.0, 0.0]], A.rtree_bvh()).tolist() == [1.0]
+    acc = m2s.build_sdf_acceleration(v, T.TriangleList(idx), A.rtree_bvh())
+    assert m2s.query_sdf(acc, [[0.0, 0.0, 0.0]]).tolist() == [1.0]
+    v = [[0.5, 1.5, 0.5], [1.0, 2.0, 3.0], [1.0, 3.0, 4.0]]
+    grid = m2s.Grid.from_bounding_box([0, 0, 0], [10, 10, 10], [10, 10, 10])
+    assert m2s.generate_grid_sdf(v, T.TriangleList(idx), grid, S.Raycast)[0] == 1.0
+
+
+def test_cube_normal_methods():
+    # lib.rs:587-683
+    cv = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1], [1, 1, 0], [1, 0, 1], [0, 1, 1], [1, 1, 1]], np.float32)
+    ci = np.array([0, 2, 4, 0, 4, 1, 3, 5, 7, 3, 7, 6, 0, 1, 5, 0, 5, 3, 2, 6, 7, 2, 7, 4, 0, 3, 6, 0, 6, 2, 1, 4, 7,
+                   1, 7, 5], np.uint32)
+    inner = np.array([[a, b, c] for a in (0.2, 0.8) for b in (0.2, 0.8) for c in (0.2, 0.8)], np.float32)
+    outer = np.array([[a, b, c] for a in (-0.2, 1.2) for b in (-0.2, 1.2) for c in (-0.2, 1.2)], np.float32)
+    for am in (A.none(S.Normal), A.bvh(S.Normal), A.rtree()):
+        assert np.all(np.abs(m2s.generate_sdf(cv, T.TriangleList(ci), inner, am) + 0.2) < 1e-6), am
+        assert np.all(np.abs(m2s.generate_sdf(cv, T.TriangleList(ci), outer, am) - np.sqrt(0.12)) < 1e-6), am
+
+
+def test_vector_known_points(orc):
+    # rtree_bvh.rs:383-419
+    acc = m2s.build_sdf_acceleration(TETRA_V, T.TriangleList(TETRA_IDX), A.rtree_bvh())
+    pts = np.array([[0, 0, 0], [0, 0.5, 0], [0.2, 0.2, 0], [-0.1, -0.1, 0.2], [0.1, -0.1, 0.2], [0.2, 0.2, 0.2],
+                    [0.2, 0.2, -0.1]], np.float32)
+    exp = np.array([[0, 0, 0], [0, 0, 0], [0, 0, 0], [0.1, 0.1, -0.2], [0, 0.1, -0.2], [0, 0, -0.2], [0, 0, 0.1]])
+    vec, inside = m2s.query_vector_to_closest_point_rtree_bvh(acc, pts)
+    assert np.all(np.linalg.norm(vec - exp, axis=1) < 1e-6)
+    assert inside[-1] and not inside[3:6].any()
+    ov, oi = orc.query_vector_to_closest_point(TETRA_V, TETRA_IDX, pts)
+    assert_bit_equal(vec.reshape(-1), ov.reshape(-1), "vector")
+    assert np.array_equal(inside, oi)
+
+
+# ----------------------------------------------------------------- methods vs oracle
+MESHES = {
+    "icosphere_s3": lambda: (*synth.icosphere(3), False),
+    "star_s4": lambda: (*synth.star(4, seed=3), False),
+    "terrain_40_strip": lambda: (*synth.terrain(40, seed=1), True),
+}
+
+
+@pytest.mark.parametrize("mesh", list(MESHES))
+def test_every_method_bit_exact(orc, mesh):
+    v, idx, strip = MESHES[mesh]()
+    q = synth.mixed_points(v, idx if not strip else None, 3000, seed=11) if not strip else \
+        synth.uniform_points(3000, *synth.padded_bbox(v), seed=11)
+    topo = T.TriangleStrip(idx) if strip else T.TriangleList(idx)
+    for am in m2s.ALL_SDF_ACCELERATION_METHODS:
+        gpu = m2s.generate_sdf(v, topo, q, am)
+        assert_bit_equal(gpu, orc_sdf(orc, v, idx, q, am, strip=strip), f"{mesh} {am!r}")
+
+
+def test_topology_encodings(orc):
+    # generate/grid.rs:844-901 and lib.rs:193-215: u16, u32, no-index list, strips
+    v, idx = synth.icosphere(2)
+    q = synth.uniform_points(500, [-1.3] * 3, [1.3] * 3, seed=2)
+    ref = orc.generate_sdf(v, idx, q, "bvh", "raycast")
+    flat = v[idx.astype(np.int64)]
+    for topo in (T.TriangleList(idx), T.TriangleList(idx.astype(np.uint16))):
+        assert_bit_equal(m2s.generate_sdf(v, topo, q, A.bvh(S.Raycast)), ref, "list")
+    assert_bit_equal(m2s.generate_sdf(flat, T.TriangleList(None), q, A.bvh(S.Raycast)), ref, "list none")
+    tv, ti = synth.terrain(24, seed=4)
+    tq = synth.uniform_points(400, *synth.padded_bbox(tv), seed=5)
+    ref = orc.generate_sdf(tv, ti, tq, "rtree", "normal", strip=True)
+    assert_bit_equal(m2s.generate_sdf(tv, T.TriangleStrip(ti.astype(np.uint32)), tq, A.rtree()), ref, "strip")
+    sv = tv[ti.astype(np.int64)]
+    assert_bit_equal(m2s.generate_sdf(sv, T.TriangleStrip(None), tq, A.rtree()), ref, "strip none")
+
+
+def test_build_query_equals_generate():
+    # default.rs:146-150, bvh.rs:383-387, rtree.rs:374-378, rtree_bvh.rs:330-334
+    v, idx = synth.star(3, seed=7)
+    q = synth.mixed_points(v, idx, 2000, seed=8)
+    for am in m2s.ALL_SDF_ACCELERATION_METHODS:
+        acc = m2s.build_sdf_acceleration(v, T.TriangleList(idx), am)
+        assert_bit_equal(m2s.query_sdf(acc, q), m2s.generate_sdf(v, T.TriangleList(idx), q, am), repr(am))
+
+
+def test_vector_query_matches_oracle(orc):
+    v, idx = synth.star(4, seed=1)
+    q = synth.mixed_points(v, idx, 3000, seed=3)
+    acc = m2s.build_sdf_acceleration(v, T.TriangleList(idx), A.rtree_bvh())
+    vec, inside = m2s.query_vector_to_closest_point_rtree_bvh(acc, q)
+    ov, oi = orc.query_vector_to_closest_point(v, idx, q)
+    assert_bit_equal(vec.reshape(-1), ov.reshape(-1), "vectors")
+    assert np.array_equal(inside, oi)
+    sdf = m2s.query_sdf(acc, q)  # rtree_bvh.rs:337-380
+    assert np.all(np.abs(np.linalg.norm(vec, axis=1) - np.abs(sdf)) < 1e-3)
+    assert np.array_equal(inside, sdf < 0)
+
+
+def test_large_batch_morton_order(orc):
+    # >= 4096 queries take the Morton-sorted launch; results stay in input order
+    v, idx = synth.star(5, seed=2)
+    q = synth.mixed_points(v, idx, 20000, seed=4)
+    for am in (A.bvh(S.Raycast), A.rtree(), A.rtree_bvh()):
+        assert_bit_equal(m2s.generate_sdf(v, T.TriangleList(idx), q, am), orc_sdf(orc, v, idx, q, am), repr(am))
+
+
+def test_fp64_error_report(orc):
+    # north_star error report: distance error against an FP64 brute force
+    v, idx = synth.star(4, seed=9)
+    q = synth.mixed_points(v, idx, 4000, seed=10)
+    gpu = m2s.generate_sdf(v, T.TriangleList(idx), q, A.rtree_bvh())
+    d64, inside64 = orc.generate_sdf_f64(v, idx, q)
+    lo, hi = synth.bbox(v)
+    diag = float(np.linalg.norm(hi.astype(np.float64) - lo))
+    err = np.abs(np.abs(gpu.astype(np.float64)) - d64)
+    assert err.max() <= 1e-6 * diag, (err.max(), diag)
+    assert np.mean((gpu < 0) != inside64) < 1e-3
+
+
+# ----------------------------------------------------------------- errors / edge cases
+def test_error_statuses():
+    bad = TETRA_IDX.copy()
+    bad[0] = 100
+    with pytest.raises(m2s.M2SError) as e:  # lib.rs:557-566
+        m2s.generate_sdf(TETRA_V, T.TriangleList(bad), [[0.2, 0.2, 0.05]], A.bvh(S.Raycast))
+    assert e.value.status == 4
+    empty = np.zeros(0, np.uint32)
+    q = [[0.1, 0.2, 0.3], [1, 1, 1]]
+    out = m2s.generate_sdf(TETRA_V, T.TriangleList(empty), q, A.none(S.Raycast))
+    assert out.tolist() == [np.finfo(np.float32).max] * 2  # default.rs:56
+    assert len(m2s.generate_sdf(TETRA_V, T.TriangleList(empty), q, A.rtree_bvh())) == 0  # rtree_bvh.rs:96-97
+    assert m2s.build_sdf_acceleration(TETRA_V, T.TriangleList(empty), A.rtree_bvh()) is None
+    with pytest.raises(m2s.M2SError) as e:  # rtree.rs:317
+        m2s.generate_sdf(TETRA_V, T.TriangleList(empty), q, A.rtree())
+    assert e.value.status == 6
+    # a single triangle (the LBVH root is a leaf)
+    one = m2s.generate_sdf(TETRA_V, T.TriangleList(TETRA_IDX[:3]), q, A.bvh(S.Raycast))
+    assert np.all(one > 0)
+    # degenerate triangles fall back to segments (geo.rs:73-88)
+    deg = np.array([0, 0, 1, 1, 2, 2, 3, 3, 3], np.uint32)
+    qq = synth.uniform_points(200, [-1, -1, -2], [2, 2, 1], seed=1)
+    for am in m2s.ALL_SDF_ACCELERATION_METHODS:
+        m2s.generate_sdf(TETRA_V, T.TriangleList(deg), qq, am)
+
+
+def test_degenerate_mesh_matches_oracle(orc):
+    deg = np.array([0, 0, 1, 1, 2, 2, 3, 3, 3, 0, 1, 2], np.uint32)
+    qq = synth.uniform_points(300, [-1, -1, -2], [2, 2, 1], seed=1)
+    for am in m2s.ALL_SDF_ACCELERATION_METHODS:
+        assert_bit_equal(m2s.generate_sdf(TETRA_V, T.TriangleList(deg), qq, am),
+                         orc_sdf(orc, TETRA_V, deg, qq, am), repr(am))
+
+
+def test_radix_sort_bit_exact_against_stable_sort():
+    import torch
+
+    rng = np.random.default_rng(0)
+    for n, kb in ((1, 30), (1000, 30), (70001, 30), (1 << 20, 32), (300000, 8)):
+        keys = rng.integers(0, 1 << min(kb, 31), n, dtype=np.uint64).astype(np.uint32)
+        keys[: n // 3] = keys[n // 2] if n > 2 else keys[: n // 3]  # many duplicates
+        vals = np.arange(n, dtype=np.uint32)
+        k = torch.from_numpy(keys.view(np.int32)).cuda()
+        v = torch.from_numpy(vals.view(np.int32)).cuda()
+        m2s.radix_sort_pairs_device(k, v, kb)
+        torch.cuda.synchronize()
+        order = np.argsort(keys, kind="stable")
+        assert np.array_equal(k.cpu().numpy().view(np.uint32), keys[order])
+        assert np.array_equal(v.cpu().numpy().view(np.uint32), vals[order])
+
+
+# ----------------------------------------------------------------- grids
+def test_grid_equals_none_raycast():
+    # generate/grid.rs:693-724: bit for bit
+    v = np.array([[0, 1, 0], [1, 2, 3], [1, 3, 4], [2, 0, 0]], np.float32)
+    idx = np.array([0, 1, 2, 1, 2, 3], np.uint32)
+    grid = m2s.Grid.from_bounding_box([0, 0, 0], [5, 5, 5], [5, 5, 5])
+    gsdf = m2s.generate_grid_sdf(v, T.TriangleList(idx), grid, S.Raycast)
+    psdf = m2s.generate_sdf(v, T.TriangleList(idx), grid.cell_centers(), A.none(S.Raycast))
+    assert_bit_equal(gsdf, psdf, "grid vs None(Raycast)")
+
+
+def grid_report(orc, v, idx, grid, sign, strip=False):
+    topo = T.TriangleStrip(idx) if strip else T.TriangleList(idx)
+    gpu = m2s.generate_grid_sdf(v, topo, grid, sign)
+    args = (v, idx, grid.first_cell, grid.cell_size, grid.cell_count, int(sign))
+    ref1 = orc.generate_grid_sdf(*args, strip=strip, n_threads=1)
+    ref8 = orc.generate_grid_sdf(*args, strip=strip, n_threads=8)
+    centers = grid.cell_centers()
+    nn = np.abs(orc.generate_sdf(v, idx, centers, "rtree_bvh" if not strip else "rtree", strip=strip))
+    return gpu, ref1, ref8, nn
+
+
+def check_grid(gpu, ref1, ref8, nn, cell, sign, label):
+    n = len(gpu)
+    a, r = np.abs(gpu), np.abs(ref1)
+    # every GPU value is the distance of a real triangle
+    assert np.all(a >= nn), label
+    # the GPU stays within a cell diagonal of the exact nearest distance
+    assert np.all(a - nn <= cell), label
+    diff_gpu = np.mean(bits(a) != bits(r))
+    diff_ref8 = np.mean(bits(np.abs(ref8)) != bits(r))
+    assert diff_gpu <= max(1.5 * diff_ref8, 0.01), (label, diff_gpu, diff_ref8)
+    if sign == S.Raycast:
+        assert np.array_equal(np.signbit(gpu), np.signbit(ref1)), label
+    return diff_gpu, diff_ref8
+
+
+def test_grid_icosphere_c1_shape(orc):
+    # the small grid config: icosphere s3, 32^3 over [-1.2, 1.2]^3, Raycast
+    v, idx = synth.icosphere(3)
+    grid = m2s.Grid.from_bounding_box([-1.2] * 3, [1.2] * 3, [32, 32, 32])
+    gpu, ref1, ref8, nn = grid_report(orc, v, idx, grid, S.Raycast)
+    check_grid(gpu, ref1, ref8, nn, float(np.linalg.norm(grid.cell_size)), S.Raycast, "c1")
+
+
+def test_grid_star(orc):
+    v, idx = synth.star(5, seed=0)
+    lo, hi = synth.padded_bbox(v)
+    grid = m2s.Grid.from_bounding_box(lo, hi, [48, 40, 56])
+    gpu, ref1, ref8, nn = grid_report(orc, v, idx, grid, S.Raycast)
+    check_grid(gpu, ref1, ref8, nn, float(np.linalg.norm(grid.cell_size)), S.Raycast, "star")
+    again = m2s.generate_grid_sdf(v, T.TriangleList(idx), grid, S.Raycast)
+    assert_bit_equal(again, gpu, "grid determinism")
+
+
+def test_grid_terrain_normal(orc):
+    v, idx = synth.terrain(48, seed=2)
+    lo, hi = synth.padded_bbox(v)
+    grid = m2s.Grid.from_bounding_box(lo, hi, [36, 36, 12])
+    gpu, ref1, ref8, nn = grid_report(orc, v, idx, grid, S.Normal, strip=True)
+    check_grid(gpu, ref1, ref8, nn, float(np.linalg.norm(grid.cell_size)), S.Normal, "terrain")
+    same_mag = bits(np.abs(gpu)) == bits(np.abs(ref1))
+    flips = np.mean(np.signbit(gpu[same_mag]) != np.signbit(ref1[same_mag]))
+    assert flips < 0.01, flips
+
+
+def test_grid_out_of_bounds_rays(orc):
+    # generate/grid.rs:808-840: the grid covers only part of the mesh
+    v, idx = synth.star(4, seed=5)
+    lo, hi = synth.bbox(v)
+    grid = m2s.Grid.from_bounding_box(lo, hi * np.float32(0.5), [32, 32, 32])
+    gpu, ref1, ref8, nn = grid_report(orc, v, idx, grid, S.Raycast)
+    check_grid(gpu, ref1, ref8, nn, float(np.linalg.norm(grid.cell_size)), S.Raycast, "oob")
+
+
+def test_grid_continuity():
+    # generate/grid.rs:729-804 on a watertight star, bbox grown by 20 %
+    v, idx = synth.star(4, seed=6)
+    lo, hi = synth.padded_bbox(v, 0.2)
+    grid = m2s.Grid.from_bounding_box(lo, hi, [32, 32, 32])
+    sdf = m2s.generate_grid_sdf(v, T.TriangleList(idx), grid, S.Raycast).reshape(32, 32, 32)
+    size = grid.cell_size
+    for axis in range(3):
+        a = np.take(sdf, range(31), axis=axis)
+        b = np.take(sdf, range(1, 32), axis=axis)
+        assert np.all(np.abs(np.abs(a) - np.abs(b)) <= size[axis] * 1.0001)
+        flip = np.sign(a) * np.sign(b) < 0
+        assert np.all(np.abs(a[flip]) <= size[axis]) and np.all(np.abs(b[flip]) <= size[axis])
+
+
+def test_grid_negative_and_anisotropic_sizes(orc):
+    v, idx = synth.icosphere(2)
+    grid = m2s.Grid.new([1.1, -1.1, 1.0], [-0.1, 0.1, -0.25], [22, 23, 9])
+    gpu, ref1, ref8, nn = grid_report(orc, v, idx, grid, S.Raycast)
+    assert np.array_equal(np.signbit(gpu), np.signbit(ref1))
+    assert np.all(np.abs(gpu) >= nn)
