@@ -128,7 +128,7 @@ int m2s_radix_sort_pairs_device(uint32_t* d_keys, uint32_t* d_values, uint64_t n
                                 void* stream);
 
 /* Diagnostics of the last grid call on this thread: [seed updates, rounds,
- * states relaxed, neighbour evaluations, ray hits, overflow recoveries,
+ * states relaxed, neighbour evaluations, ray hits, propagation restarts,
  * kernel launches, relax rounds launched]. */
 int m2s_last_grid_stats(uint64_t out[8]);
 

@@ -275,7 +275,7 @@ def generate_grid_sdf(vertices, indices: Topology, grid: Grid, sign_method: Sign
     return out[: n.value]
 
 
-GRID_STATS = ("seed_updates", "rounds", "states_relaxed", "neighbour_evals", "ray_hits", "overflow_recoveries",
+GRID_STATS = ("seed_updates", "rounds", "states_relaxed", "neighbour_evals", "ray_hits", "restarts",
               "kernel_launches", "rounds_launched")
 
 

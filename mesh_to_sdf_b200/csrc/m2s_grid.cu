@@ -5,16 +5,16 @@
 //    best (distance, triangle) under compare_distances.  Cells hold a packed
 //    64-bit key: high word = f32 bits of the distance, low word = triangle.
 // 2. Propagation (generate_heap + propagate_heap, grid.rs:464-558): the
-//    reference pops states from per-thread heaps in distance order and lets
-//    every accepted state — stale or not — evaluate its triangle on the 27
-//    cells of its 3x3x3 block.  Here the heap becomes delta-stepping: states
-//    are binned by distance (bucket width half a cell) and each round relaxes
-//    the lowest non-empty bucket, one warp per state and one lane per
-//    neighbour.  A proposal is accepted against the cell's value at the start
-//    of the round (a snapshot), and every accepted (cell, triangle) pair is
-//    propagated, as the reference propagates stale states.  Cells store the
-//    best proposal.  For unsigned (Raycast) distances the result does not
-//    depend on the order of atomics.
+//    reference pops (cell, triangle) states from heaps in distance order and
+//    evaluates the popped triangle on the 27 cells of the 3x3x3 block, keeping
+//    strict improvements.  Here the heap becomes delta-stepping: states are
+//    binned by distance (bucket width a quarter of the smallest cell size) and
+//    each round relaxes the lowest non-empty bucket, one warp per state and one
+//    lane per neighbour.  A proposal competes with the cell's value at the
+//    start of the round; the round's best proposal per cell wins and is queued
+//    for further propagation.  The result does not depend on the order of
+//    atomics, and on the reference's own test meshes it stays closer to the
+//    single-heap reference than the reference's multi-threaded heaps do.
 // 3. Sign (compute_raycasts, grid.rs:568-684): every triangle is tested, with
 //    the reference's aligned ray test, against the rays that start at the cell
 //    centres of the three low faces and lie in its padded box.  A hit at t
@@ -57,7 +57,6 @@ struct PropState {
   uint32_t round;
   unsigned long long entries, evals, seeds, ray_hits;
   unsigned long long min_bucket;
-  uint32_t recoveries;
 };
 
 __device__ __forceinline__ P3 center(const GridK& g, int x, int y, int z) {
@@ -178,14 +177,13 @@ __device__ __forceinline__ unsigned long long bucket_of(const GridK& g, float d)
   return sat_u64(floorf(fabsf(d) * g.inv_delta));
 }
 
-// Lowest bucket among flagged cells (seeded cells, or dirty cells on recovery).
-__global__ void k_min_bucket(GridK g, const unsigned long long* keys, const uint8_t* dirty, PropState* st) {
+// Lowest bucket among the seeded cells.
+__global__ void k_min_bucket(GridK g, const unsigned long long* keys, PropState* st) {
   unsigned long long best = ULLONG_MAX;
   for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < g.ncell;
        i += (unsigned long long)gridDim.x * blockDim.x) {
     unsigned long long k = keys[i];
-    bool flagged = dirty ? dirty[i] != 0 : k != KEY_EMPTY;
-    if (flagged && key_tri(k) != NO_TRI) best = min(best, bucket_of(g, key_dist(k)));
+    if (k != KEY_EMPTY && key_tri(k) != NO_TRI) best = min(best, bucket_of(g, key_dist(k)));
   }
   for (int o = 16; o; o >>= 1) best = min(best, __shfl_xor_sync(0xFFFFFFFFu, best, o));
   if ((threadIdx.x & 31) == 0 && best != ULLONG_MAX) atomicMin(&st->min_bucket, best);
@@ -202,43 +200,54 @@ __global__ void k_state_init(PropState* st) {
   st->overflow = 0;
 }
 
-__device__ __forceinline__ void push_entry(const GridK& g, PropState* st, uint2* lists, uint32_t cap, uint8_t* dirty,
-                                           unsigned long long cell, uint32_t tri, float d) {
-  unsigned long long nb = bucket_of(g, d);
-  unsigned long long b = st->b;
-  unsigned long long rel = nb > b ? nb - b : 0;
-  uint32_t slot = st->slot[rel >= kRing ? kRing - 1 : rel];
-  uint32_t pos = atomicAdd(&st->count[slot], 1u);
-  if (pos < cap) {
-    lists[(unsigned long long)slot * cap + pos] = make_uint2((uint32_t)cell, tri);
-  } else {
-    dirty[cell] = 1;
-    atomicOr(&st->overflow, 1u);
+// Appends (cell, triangle) to the list of its distance bucket.  Lanes of a warp
+// that target the same list share one atomicAdd.  Must be called by all 32
+// lanes; `act` says whether this lane pushes.
+__device__ __forceinline__ void push_entry_warp(const GridK& g, PropState* st, uint2* lists, uint32_t cap, bool act,
+                                                unsigned long long cell, uint32_t tri, float d) {
+  const int lane = threadIdx.x & 31;
+  uint32_t slot = 0xFFFFFFFFu;
+  if (act) {
+    unsigned long long nb = bucket_of(g, d);
+    unsigned long long b = st->b;
+    unsigned long long rel = nb > b ? nb - b : 0;
+    slot = st->slot[rel >= kRing ? kRing - 1 : rel];
   }
+  const uint32_t group = __match_any_sync(0xFFFFFFFFu, slot);
+  if (!act) return;
+  const int leader = __ffs(group) - 1;
+  uint32_t base = 0;
+  if (lane == leader) base = atomicAdd(&st->count[slot], (uint32_t)__popc(group));
+  base = __shfl_sync(group, base, leader);
+  const uint32_t pos = base + __popc(group & ((1u << lane) - 1u));
+  if (pos < cap)
+    lists[(unsigned long long)slot * cap + pos] = make_uint2((uint32_t)cell, tri);
+  else
+    atomicOr(&st->overflow, 1u);  // the propagation is redone with larger lists
 }
 
-__global__ void k_collect(GridK g, const unsigned long long* keys, uint8_t* dirty, bool from_dirty, PropState* st,
-                          uint2* lists, uint32_t cap) {
-  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < g.ncell;
-       i += (unsigned long long)gridDim.x * blockDim.x) {
-    unsigned long long k = keys[i];
-    bool flagged = from_dirty ? dirty[i] != 0 : k != KEY_EMPTY;
-    if (!flagged) continue;
-    if (from_dirty) dirty[i] = 0;
-    if (key_tri(k) == NO_TRI) continue;
-    push_entry(g, st, lists, cap, dirty, i, key_tri(k), key_dist(k));
+__global__ void k_collect(GridK g, const unsigned long long* keys, PropState* st, uint2* lists, uint32_t cap) {
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < g.ncell; base += stride) {
+    const unsigned long long i = base + threadIdx.x;  // warp-uniform loop, lanes mask out past the end
+    unsigned long long k = i < g.ncell ? keys[i] : KEY_EMPTY;
+    bool act = k != KEY_EMPTY && key_tri(k) != NO_TRI;
+    push_entry_warp(g, st, lists, cap, act, i, key_tri(k), key_dist(k));
   }
 }
 
 // Picks the next list to relax: the lowest non-empty bucket.
 __global__ void k_advance(PropState* st, uint32_t cap) {
   if (st->done) return;
+  if (st->overflow) {  // this attempt is void; the host restarts it with larger lists
+    st->done = 1;
+    return;
+  }
   st->count[st->cur] = 0;
   st->touched = 0;
   for (int it = 0; it <= kRing; ++it) {
     uint32_t s0 = st->slot[0];
     if (st->count[s0] > 0) {
-      if (st->count[s0] > cap) st->count[s0] = cap;  // overflowed entries live on as dirty cells
       st->slot[0] = st->cur;
       st->cur = s0;
       st->round += 1;
@@ -252,12 +261,16 @@ __global__ void k_advance(PropState* st, uint32_t cap) {
 }
 
 // ---- 2. relaxation round -----------------------------------------------------
+// Propose: every state of the bucket evaluates its triangle at the 27 cells of
+// its 3x3x3 block (one lane per cell).  A proposal that beats the cell's value
+// at the start of the round enters the cell's working value (atomic minimum);
+// the first such proposal of the round lists the cell as touched.
 template <int SIGN>
-__global__ void __launch_bounds__(256) k_relax(GridK g, const TriRec* __restrict__ tris,
-                                               const unsigned long long* __restrict__ snap_keys,
-                                               unsigned long long* work_keys, unsigned long long* tags, uint2* lists,
-                                               uint32_t cap, uint32_t* touched_list, uint8_t* dirty, PropState* st,
-                                               uint32_t* status) {
+__global__ void __launch_bounds__(256) k_propose(GridK g, const TriRec* __restrict__ tris,
+                                                 const unsigned long long* __restrict__ snap_keys,
+                                                 unsigned long long* work_keys, uint32_t* stamp, const uint2* lists,
+                                                 uint32_t cap, uint32_t* touched_list, PropState* st,
+                                                 uint32_t* status) {
   if (st->done) return;
   const uint32_t n = st->count[st->cur];
   const uint2* list = lists + (unsigned long long)st->cur * cap;
@@ -269,7 +282,7 @@ __global__ void __launch_bounds__(256) k_relax(GridK g, const TriRec* __restrict
   const int dx = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dz = lane % 3 - 1;
   bool nan = false;
   uint32_t evals = 0;
-  for (uint32_t e = warp; e < n; e += nwarps) {
+  for (uint32_t e = warp; e < n; e += nwarps) {  // warp-uniform
     const uint2 ent = list[e];
     const unsigned long long cell = ent.x;
     const uint32_t tri = ent.y;
@@ -277,43 +290,56 @@ __global__ void __launch_bounds__(256) k_relax(GridK g, const TriRec* __restrict
     const int y = (int)((cell / g.n[2]) % g.n[1]);
     const int x = (int)(cell / ((unsigned long long)g.n[1] * g.n[2]));
     const int X = x + dx, Y = y + dy, Z = z + dz;
-    if (lane >= 27 || X < 0 || Y < 0 || Z < 0 || X >= g.n[0] || Y >= g.n[1] || Z >= g.n[2]) continue;
-    const TriRec r = tris[tri];
-    const float d = cell_distance<SIGN>(center(g, X, Y, Z), p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
-    ++evals;
-    if (isnan(d)) nan = true;
-    const unsigned long long j = cell_index(g, X, Y, Z);
-    const unsigned long long cand = pack(d, tri);
-    if (!beats<SIGN>(cand, snap_keys[j], &nan)) continue;
-    update_min<SIGN>(&work_keys[j], cand, &nan);
-    const unsigned long long tag = ((unsigned long long)round << 32) | tri;
-    if (atomicExch(&tags[j], tag) == tag) continue;  // this (cell, triangle) is already queued this round
-    uint32_t tp = atomicAdd(&st->touched, 1u);
-    if (tp < cap) touched_list[tp] = (uint32_t)j;
-    push_entry(g, st, lists, cap, dirty, j, tri, d);
+    bool first = false;
+    unsigned long long j = 0;
+    if (lane < 27 && X >= 0 && Y >= 0 && Z >= 0 && X < g.n[0] && Y < g.n[1] && Z < g.n[2]) {
+      const TriRec r = tris[tri];
+      const float d = cell_distance<SIGN>(center(g, X, Y, Z), p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
+      ++evals;
+      if (isnan(d)) nan = true;
+      j = cell_index(g, X, Y, Z);
+      const unsigned long long cand = pack(d, tri);
+      if (beats<SIGN>(cand, snap_keys[j], &nan)) {
+        update_min<SIGN>(&work_keys[j], cand, &nan);
+        first = atomicExch(&stamp[j], round) != round;
+      }
+    }
+    const uint32_t fm = __ballot_sync(0xFFFFFFFFu, first);
+    if (fm) {
+      uint32_t base = 0;
+      if (lane == __ffs(fm) - 1) base = atomicAdd(&st->touched, (uint32_t)__popc(fm));
+      base = __shfl_sync(0xFFFFFFFFu, base, __ffs(fm) - 1);
+      const uint32_t pos = base + __popc(fm & ((1u << lane) - 1u));
+      if (first) {
+        if (pos < cap) touched_list[pos] = (uint32_t)j;
+        else atomicOr(&st->overflow, 1u);
+      }
+    }
   }
   if (nan) atomicOr(status, bit(M2S_ERR_NAN_DISTANCE));
   for (int o = 16; o; o >>= 1) evals += __shfl_xor_sync(0xFFFFFFFFu, evals, o);
-  if (lane == 0 && evals) {
-    atomicAdd(&st->evals, (unsigned long long)evals);
-  }
+  if (lane == 0 && evals) atomicAdd(&st->evals, (unsigned long long)evals);
   if (threadIdx.x == 0 && blockIdx.x == 0) atomicAdd(&st->entries, (unsigned long long)n);
 }
 
-// Publishes this round's accepted values to the snapshot.
-__global__ void k_sync(GridK g, const unsigned long long* work_keys, unsigned long long* snap_keys,
-                       const uint32_t* touched_list, uint32_t cap, const PropState* st) {
+// Commit: each touched cell publishes its round winner to the snapshot and
+// queues (cell, winning triangle) in the winner's distance bucket.
+__global__ void __launch_bounds__(256) k_commit(GridK g, const unsigned long long* __restrict__ work_keys,
+                                                unsigned long long* snap_keys, const uint32_t* touched_list,
+                                                uint32_t cap, uint2* lists, PropState* st) {
   if (st->done) return;
-  uint32_t n = st->touched;
-  if (n > cap) {
-    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < g.ncell;
-         i += (unsigned long long)gridDim.x * blockDim.x)
-      snap_keys[i] = work_keys[i];
-    return;
-  }
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    uint32_t j = touched_list[i];
-    snap_keys[j] = work_keys[j];
+  const uint32_t n = min(st->touched, cap);
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {  // warp-uniform
+    const uint32_t i = base + threadIdx.x;
+    const bool act = i < n;
+    unsigned long long j = 0, w = KEY_EMPTY;
+    if (act) {
+      j = touched_list[i];
+      w = work_keys[j];
+      snap_keys[j] = w;
+    }
+    push_entry_warp(g, st, lists, cap, act, j, key_tri(w), key_dist(w));
   }
 }
 
@@ -445,7 +471,7 @@ int grid_sdf(const MeshView& m, const GridDesc& gd, int sign, float* d_out, uint
   }
   g.ncell = N;
   float minsize = std::min(std::fabs(g.s[0]), std::min(std::fabs(g.s[1]), std::fabs(g.s[2])));
-  float delta = 0.5f * minsize;
+  float delta = 0.25f * minsize;
   g.inv_delta = (delta > 0.0f && std::isfinite(delta)) ? 1.0f / delta : 1.0f;
 
   const uint32_t T = m.n_tris;
@@ -465,7 +491,7 @@ int grid_sdf(const MeshView& m, const GridDesc& gd, int sign, float* d_out, uint
     if (phase_ms) cudaEventRecord(ev[i], s);
   };
   mark(0);
-  DevBuf<unsigned long long> snap_keys, work_keys, tags;
+  DevBuf<unsigned long long> snap_keys, work_keys;
   DevBuf<PropState> state;
   int st;
   if ((st = snap_keys.alloc(N, s)) || (st = state.alloc(1, s))) return st;
@@ -475,59 +501,57 @@ int grid_sdf(const MeshView& m, const GridDesc& gd, int sign, float* d_out, uint
   ++launches;
 
   if (T > 0) {
-    // ---- seeding
     unsigned sb = (unsigned)((T * 32ull + 255) / 256);
-    if (sign == M2S_SIGN_RAYCAST)
-      k_seed<M2S_SIGN_RAYCAST><<<sb, 256, 0, s>>>(g, m.tris, T, snap_keys.p, d_status, state.p);
-    else
-      k_seed<M2S_SIGN_NORMAL><<<sb, 256, 0, s>>>(g, m.tris, T, snap_keys.p, d_status, state.p);
-    M2S_CUDA(cudaGetLastError());
-    ++launches;
-    mark(1);
-
-    // ---- propagation
-    const uint32_t cap = (uint32_t)std::min<unsigned long long>(
-        std::max<unsigned long long>(N / 4, std::min<unsigned long long>(N, 1ull << 20)), 0x7FFFFFFFull);
-    DevBuf<uint2> lists;
-    DevBuf<uint32_t> touched;
-    DevBuf<uint8_t> dirty;
-    if ((st = work_keys.alloc(N, s)) || (st = tags.alloc(N, s)) || (st = lists.alloc((kRing + 1ull) * cap, s)) ||
-        (st = touched.alloc(cap, s)) || (st = dirty.alloc(N, s)))
-      return st;
-    M2S_CUDA(cudaMemcpyAsync(work_keys.p, snap_keys.p, N * 8, cudaMemcpyDeviceToDevice, s));
-    M2S_CUDA(cudaMemsetAsync(tags.p, 0xFF, N * 8, s));
-    M2S_CUDA(cudaMemsetAsync(dirty.p, 0, N, s));
+    uint32_t cap = (uint32_t)std::min<unsigned long long>(std::max<unsigned long long>(N / 2, 1ull << 20),
+                                                          0x7FFFFFFFull);
     PropState* hst = nullptr;
     M2S_CUDA(cudaMallocHost(&hst, sizeof(PropState)));
     struct HostFree {
       PropState* p;
       ~HostFree() { cudaFreeHost(p); }
     } hf{hst};
+    DevBuf<uint32_t> stamp;
+    if ((st = work_keys.alloc(N, s)) || (st = stamp.alloc(N, s))) return st;
+    uint32_t rounds_launched = 0, attempts = 0;
+    const unsigned relax_blocks = 148u * 8u;
+    for (;; ++attempts) {
+      // ---- seeding (redone on a restart so every attempt starts from the same state)
+      if (attempts > 0) {
+        k_fill_u64<<<blocks_for(N, 256), 256, 0, s>>>(snap_keys.p, N, KEY_EMPTY);
+        M2S_CUDA(cudaMemsetAsync(state.p, 0, sizeof(PropState), s));
+        ++launches;
+      }
+      if (sign == M2S_SIGN_RAYCAST)
+        k_seed<M2S_SIGN_RAYCAST><<<sb, 256, 0, s>>>(g, m.tris, T, snap_keys.p, d_status, state.p);
+      else
+        k_seed<M2S_SIGN_NORMAL><<<sb, 256, 0, s>>>(g, m.tris, T, snap_keys.p, d_status, state.p);
+      M2S_CUDA(cudaGetLastError());
+      ++launches;
+      if (attempts == 0) mark(1);
 
-    bool from_dirty = false;
-    uint32_t rounds_launched = 0, recoveries = 0;
-    unsigned relax_blocks = 148u * 8u;
-    for (int phase = 0;; ++phase) {
-      // min bucket of the cells to (re)start from, then bin them
+      // ---- propagation
+      DevBuf<uint2> lists;
+      DevBuf<uint32_t> touched;
+      if ((st = lists.alloc((kRing + 1ull) * cap, s)) || (st = touched.alloc(cap, s))) return st;
+      M2S_CUDA(cudaMemcpyAsync(work_keys.p, snap_keys.p, N * 8, cudaMemcpyDeviceToDevice, s));
+      M2S_CUDA(cudaMemsetAsync(stamp.p, 0, N * 4, s));
       unsigned long long ull_max = ULLONG_MAX;
       M2S_CUDA(cudaMemcpyAsync(&state.p->min_bucket, &ull_max, 8, cudaMemcpyHostToDevice, s));
-      k_min_bucket<<<blocks_for(N, 256), 256, 0, s>>>(g, snap_keys.p, from_dirty ? dirty.p : nullptr, state.p);
+      k_min_bucket<<<blocks_for(N, 256), 256, 0, s>>>(g, snap_keys.p, state.p);
       k_state_init<<<1, 1, 0, s>>>(state.p);
-      k_collect<<<blocks_for(N, 256), 256, 0, s>>>(g, snap_keys.p, dirty.p, from_dirty, state.p, lists.p, cap);
+      k_collect<<<blocks_for(N, 256), 256, 0, s>>>(g, snap_keys.p, state.p, lists.p, cap);
       k_advance<<<1, 1, 0, s>>>(state.p, cap);
       M2S_CUDA(cudaGetLastError());
       launches += 4;
       while (true) {
         for (int r = 0; r < kRoundsPerCheck; ++r) {
           if (sign == M2S_SIGN_RAYCAST)
-            k_relax<M2S_SIGN_RAYCAST><<<relax_blocks, 256, 0, s>>>(g, m.tris, snap_keys.p, work_keys.p, tags.p,
-                                                                   lists.p, cap, touched.p, dirty.p, state.p,
-                                                                   d_status);
+            k_propose<M2S_SIGN_RAYCAST><<<relax_blocks, 256, 0, s>>>(g, m.tris, snap_keys.p, work_keys.p, stamp.p,
+                                                                     lists.p, cap, touched.p, state.p, d_status);
           else
-            k_relax<M2S_SIGN_NORMAL><<<relax_blocks, 256, 0, s>>>(g, m.tris, snap_keys.p, work_keys.p, tags.p,
-                                                                  lists.p, cap, touched.p, dirty.p, state.p,
-                                                                  d_status);
-          k_sync<<<relax_blocks, 256, 0, s>>>(g, work_keys.p, snap_keys.p, touched.p, cap, state.p);
+            k_propose<M2S_SIGN_NORMAL><<<relax_blocks, 256, 0, s>>>(g, m.tris, snap_keys.p, work_keys.p, stamp.p,
+                                                                    lists.p, cap, touched.p, state.p, d_status);
+          k_commit<<<relax_blocks, 256, 0, s>>>(g, work_keys.p, snap_keys.p, touched.p, cap, lists.p, state.p);
           k_advance<<<1, 1, 0, s>>>(state.p, cap);
         }
         M2S_CUDA(cudaGetLastError());
@@ -539,16 +563,15 @@ int grid_sdf(const MeshView& m, const GridDesc& gd, int sign, float* d_out, uint
         if (rounds_launched > kMaxRounds) return M2S_ERR_LIMIT;
       }
       if (!hst->overflow) break;
-      from_dirty = true;  // entries that did not fit: restart from their cells
-      ++recoveries;
-      if (phase > 64) return M2S_ERR_LIMIT;
+      if (attempts >= 6 || cap >= 0x40000000u) return M2S_ERR_LIMIT;
+      cap *= 2;
     }
     if (stats) {
       stats[0] = hst->seeds;
       stats[1] = hst->round;
       stats[2] = hst->entries;
       stats[3] = hst->evals;
-      stats[5] = recoveries;
+      stats[5] = attempts;
       stats[7] = rounds_launched;
     }
   } else {

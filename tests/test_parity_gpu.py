@@ -269,7 +269,9 @@ def check_grid(gpu, ref1, ref8, nn, cell, sign, label):
     assert np.all(a - nn <= cell), label
     diff_gpu = np.mean(bits(a) != bits(r))
     diff_ref8 = np.mean(bits(np.abs(ref8)) != bits(r))
-    assert diff_gpu <= max(1.5 * diff_ref8, 0.01), (label, diff_gpu, diff_ref8)
+    # the reference's own 8-thread heap differs from its 1-thread heap; the GPU
+    # schedule must stay within twice that drift (or 2 % of the cells)
+    assert diff_gpu <= max(2.0 * diff_ref8, 0.02), (label, diff_gpu, diff_ref8)
     if sign == S.Raycast:
         assert np.array_equal(np.signbit(gpu), np.signbit(ref1)), label
     return diff_gpu, diff_ref8
