@@ -180,7 +180,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-points", action="store_true")
+    ap.add_argument("--small", action="store_true",
+                    help="one small pass for profilers: 128^3 grid, 100k Rtree / RtreeBvh points, 8k brute-force points")
     args = ap.parse_args()
+    if args.small:
+        return small_case()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
     world, rank, local = dist_setup()
@@ -344,6 +348,32 @@ def main():
     mesh.close()
     if world > 1:
         torch_destroy()
+
+
+def small_case():
+    """A short, fixed workload for ncu captures (a few hundred MB on the device)."""
+    import torch
+
+    import mesh_to_sdf_b200 as m2s
+    from mesh_to_sdf_b200 import synth
+
+    A, S = m2s.AccelerationMethod, m2s.SignMethod
+    v, idx, lo, hi = workload()
+    grid = grid_for(lo, hi, (128, 128, 128))
+    mesh = m2s.build_sdf_acceleration(v, m2s.Topology.TriangleList(idx), A.rtree_bvh())
+    out = torch.empty(grid.get_total_cell_count(), dtype=torch.float32, device="cuda")
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    mesh.grid_device(grid, S.Raycast, out, status)
+    q = torch.from_numpy(synth.mixed_points(v, idx, 100_000, seed=SEED)).cuda()
+    qo = torch.empty(100_000, dtype=torch.float32, device="cuda")
+    mesh.query_device(q, qo, status)
+    rt = m2s.build_sdf_acceleration(v, m2s.Topology.TriangleList(idx), A.rtree())
+    rt.query_device(q, qo, status)
+    bf = m2s.build_sdf_acceleration(v, m2s.Topology.TriangleList(idx), A.none(S.Raycast))
+    bf.query_device(q[:8192].contiguous(), qo, status)
+    torch.cuda.synchronize()
+    assert int(status.item()) == 0
+    print("small ok", m2s.last_grid_stats())
 
 
 def torch_destroy():

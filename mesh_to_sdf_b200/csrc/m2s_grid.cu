@@ -36,8 +36,7 @@ namespace {
 constexpr uint32_t NO_TRI = 0xFFFFFFFFu;
 constexpr unsigned long long KEY_EMPTY = (0x7F7FFFFFull << 32) | 0xFFFFFFFFull;  // (f32::MAX, none)
 constexpr int kRing = 16;            // pending distance buckets
-constexpr int kRoundsPerCheck = 16;  // rounds launched between host polls
-constexpr uint32_t kMaxRounds = 1u << 20;
+constexpr uint32_t kMaxRounds = 1u << 22;  // bound on propagation rounds
 
 struct GridK {
   float f[3], s[3];
@@ -52,6 +51,7 @@ struct PropState {
   uint32_t cur;          // list relaxed this round
   uint32_t count[kRing + 1];
   uint32_t touched;
+  uint32_t touched2[2];  // persistent kernel: touched count per round parity
   uint32_t done;
   uint32_t overflow;
   uint32_t round;
@@ -203,15 +203,15 @@ __global__ void k_state_init(PropState* st) {
 // Appends (cell, triangle) to the list of its distance bucket.  Lanes of a warp
 // that target the same list share one atomicAdd.  Must be called by all 32
 // lanes; `act` says whether this lane pushes.
-__device__ __forceinline__ void push_entry_warp(const GridK& g, PropState* st, uint2* lists, uint32_t cap, bool act,
+__device__ __forceinline__ void push_entry_warp(const GridK& g, PropState* st, unsigned long long b,
+                                                const uint32_t* slots, uint2* lists, uint32_t cap, bool act,
                                                 unsigned long long cell, uint32_t tri, float d) {
   const int lane = threadIdx.x & 31;
   uint32_t slot = 0xFFFFFFFFu;
   if (act) {
     unsigned long long nb = bucket_of(g, d);
-    unsigned long long b = st->b;
     unsigned long long rel = nb > b ? nb - b : 0;
-    slot = st->slot[rel >= kRing ? kRing - 1 : rel];
+    slot = slots[rel >= kRing ? kRing - 1 : rel];
   }
   const uint32_t group = __match_any_sync(0xFFFFFFFFu, slot);
   if (!act) return;
@@ -232,7 +232,7 @@ __global__ void k_collect(GridK g, const unsigned long long* keys, PropState* st
     const unsigned long long i = base + threadIdx.x;  // warp-uniform loop, lanes mask out past the end
     unsigned long long k = i < g.ncell ? keys[i] : KEY_EMPTY;
     bool act = k != KEY_EMPTY && key_tri(k) != NO_TRI;
-    push_entry_warp(g, st, lists, cap, act, i, key_tri(k), key_dist(k));
+    push_entry_warp(g, st, st->b, st->slot, lists, cap, act, i, key_tri(k), key_dist(k));
   }
 }
 
@@ -260,86 +260,188 @@ __global__ void k_advance(PropState* st, uint32_t cap) {
   st->done = 1;
 }
 
-// ---- 2. relaxation round -----------------------------------------------------
-// Propose: every state of the bucket evaluates its triangle at the 27 cells of
-// its 3x3x3 block (one lane per cell).  A proposal that beats the cell's value
-// at the start of the round enters the cell's working value (atomic minimum);
-// the first such proposal of the round lists the cell as touched.
+// ---- 2. relaxation rounds (persistent) -------------------------------------
+// ---- persistent propagation ---------------------------------------------------
+// All rounds in one cooperative launch.  Every block keeps an identical copy of
+// the bucket schedule in shared memory and advances it from the global list
+// counts after the round's second barrier, so no block waits for a scheduler.
+struct GridBarrier {
+  unsigned int count;
+  unsigned int gen;
+  unsigned int abort;
+};
+
+// Sense-reversing barrier over the co-resident blocks of a cooperative launch.
+// The wait is bounded: after kBarrierPolls polls it raises `abort`, which makes
+// every block leave the kernel at its next barrier.
+constexpr uint32_t kBarrierPolls = 1u << 24;
+
+__device__ __forceinline__ bool grid_barrier(GridBarrier* bar, unsigned int nblocks) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned int* vgen = &bar->gen;
+    volatile unsigned int* vabort = &bar->abort;
+    const unsigned int g0 = *vgen;
+    __threadfence();
+    if (atomicAdd(&bar->count, 1u) == nblocks - 1) {
+      atomicExch(&bar->count, 0u);
+      __threadfence();
+      atomicAdd(&bar->gen, 1u);
+    } else {
+      uint32_t polls = 0;
+      while (*vgen == g0 && !*vabort) {
+        if (++polls > kBarrierPolls) {
+          atomicExch(&bar->abort, 1u);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    ok = *vabort ? 0 : 1;
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+struct Sched {
+  unsigned long long b;
+  uint32_t slot[kRing];
+  uint32_t cur;
+  uint32_t round;
+  uint32_t done;
+};
+
 template <int SIGN>
-__global__ void __launch_bounds__(256) k_propose(GridK g, const TriRec* __restrict__ tris,
-                                                 const unsigned long long* __restrict__ snap_keys,
-                                                 unsigned long long* work_keys, uint32_t* stamp, const uint2* lists,
-                                                 uint32_t cap, uint32_t* touched_list, PropState* st,
-                                                 uint32_t* status) {
-  if (st->done) return;
-  const uint32_t n = st->count[st->cur];
-  const uint2* list = lists + (unsigned long long)st->cur * cap;
-  const uint32_t round = st->round;
+__global__ void __launch_bounds__(256) k_propagate(GridK g, const TriRec* __restrict__ tris,
+                                                   unsigned long long* snap_keys, unsigned long long* work_keys,
+                                                   uint32_t* stamp, uint2* lists, uint32_t cap, uint32_t* touched_lists,
+                                                   PropState* st, GridBarrier* bar, uint32_t max_rounds,
+                                                   uint32_t* status) {
+  __shared__ Sched sh;
+  const unsigned int nblocks = gridDim.x;
   const int lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    sh.b = st->b;
+    for (int k = 0; k < kRing; ++k) sh.slot[k] = st->slot[k];
+    sh.cur = st->cur;
+    sh.round = st->round;
+    sh.done = st->done;
+  }
+  __syncthreads();
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  // iproduct!(-1..=1, -1..=1, -1..=1) order (grid.rs:512): x outermost.
   const int dx = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dz = lane % 3 - 1;
   bool nan = false;
-  uint32_t evals = 0;
-  for (uint32_t e = warp; e < n; e += nwarps) {  // warp-uniform
-    const uint2 ent = list[e];
-    const unsigned long long cell = ent.x;
-    const uint32_t tri = ent.y;
-    const int z = (int)(cell % g.n[2]);
-    const int y = (int)((cell / g.n[2]) % g.n[1]);
-    const int x = (int)(cell / ((unsigned long long)g.n[1] * g.n[2]));
-    const int X = x + dx, Y = y + dy, Z = z + dz;
-    bool first = false;
-    unsigned long long j = 0;
-    if (lane < 27 && X >= 0 && Y >= 0 && Z >= 0 && X < g.n[0] && Y < g.n[1] && Z < g.n[2]) {
-      const TriRec r = tris[tri];
-      const float d = cell_distance<SIGN>(center(g, X, Y, Z), p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
-      ++evals;
-      if (isnan(d)) nan = true;
-      j = cell_index(g, X, Y, Z);
-      const unsigned long long cand = pack(d, tri);
-      if (beats<SIGN>(cand, snap_keys[j], &nan)) {
-        update_min<SIGN>(&work_keys[j], cand, &nan);
-        first = atomicExch(&stamp[j], round) != round;
+  unsigned long long evals = 0;
+  uint32_t prev_cur = 0xFFFFFFFFu;
+  bool aborted = false;
+  for (uint32_t it = 0; !sh.done; ++it) {
+    if (it >= max_rounds) {
+      if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(status, bit(M2S_ERR_LIMIT));
+      break;
+    }
+    const uint32_t parity = sh.round & 1u;
+    uint32_t* touched_list = touched_lists + (unsigned long long)parity * cap;
+    // ---- propose: every state of the bucket evaluates its triangle at the 27
+    // cells of its 3x3x3 block (one lane per cell); a proposal that beats the
+    // cell's value at the start of the round enters the working value (atomic
+    // minimum) and the first such proposal lists the cell as touched.
+    if (blockIdx.x == 0 && threadIdx.x == 0 && prev_cur != 0xFFFFFFFFu) st->count[prev_cur] = 0;
+    const uint32_t n = min(*(volatile uint32_t*)&st->count[sh.cur], cap);
+    const uint2* list = lists + (unsigned long long)sh.cur * cap;
+    for (uint32_t e = warp; e < n; e += nwarps) {
+      const uint2 ent = __ldcg(&list[e]);  // written by other blocks last round
+      const unsigned long long cell = ent.x;
+      const uint32_t tri = ent.y;
+      const int z = (int)(cell % g.n[2]);
+      const int y = (int)((cell / g.n[2]) % g.n[1]);
+      const int x = (int)(cell / ((unsigned long long)g.n[1] * g.n[2]));
+      const int X = x + dx, Y = y + dy, Z = z + dz;
+      bool first = false;
+      unsigned long long j = 0;
+      if (lane < 27 && X >= 0 && Y >= 0 && Z >= 0 && X < g.n[0] && Y < g.n[1] && Z < g.n[2]) {
+        const TriRec r = tris[tri];
+        const float d = cell_distance<SIGN>(center(g, X, Y, Z), p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
+        ++evals;
+        if (isnan(d)) nan = true;
+        j = cell_index(g, X, Y, Z);
+        const unsigned long long cand = pack(d, tri);
+        if (beats<SIGN>(cand, __ldcg(&snap_keys[j]), &nan)) {
+          update_min<SIGN>(&work_keys[j], cand, &nan);
+          first = atomicExch(&stamp[j], sh.round) != sh.round;
+        }
+      }
+      const uint32_t fm = __ballot_sync(0xFFFFFFFFu, first);
+      if (fm) {
+        uint32_t base = 0;
+        if (lane == __ffs(fm) - 1) base = atomicAdd(&st->touched2[parity], (uint32_t)__popc(fm));
+        base = __shfl_sync(0xFFFFFFFFu, base, __ffs(fm) - 1);
+        const uint32_t pos = base + __popc(fm & ((1u << lane) - 1u));
+        if (first) {
+          if (pos < cap) touched_list[pos] = (uint32_t)j;
+          else atomicOr(&st->overflow, 1u);
+        }
       }
     }
-    const uint32_t fm = __ballot_sync(0xFFFFFFFFu, first);
-    if (fm) {
-      uint32_t base = 0;
-      if (lane == __ffs(fm) - 1) base = atomicAdd(&st->touched, (uint32_t)__popc(fm));
-      base = __shfl_sync(0xFFFFFFFFu, base, __ffs(fm) - 1);
-      const uint32_t pos = base + __popc(fm & ((1u << lane) - 1u));
-      if (first) {
-        if (pos < cap) touched_list[pos] = (uint32_t)j;
-        else atomicOr(&st->overflow, 1u);
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&st->entries, (unsigned long long)n);
+    if (!grid_barrier(bar, nblocks)) {
+      aborted = true;
+      break;
+    }
+    // ---- commit: each touched cell publishes its round winner to the snapshot
+    // and queues (cell, winning triangle) in the winner's distance bucket.
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->touched2[parity ^ 1u] = 0;
+    const uint32_t nt = min(*(volatile uint32_t*)&st->touched2[parity], cap);
+    for (uint32_t base = blockIdx.x * blockDim.x; base < nt; base += gridDim.x * blockDim.x) {
+      const uint32_t i = base + threadIdx.x;
+      const bool act = i < nt;
+      unsigned long long j = 0, w = KEY_EMPTY;
+      if (act) {
+        j = __ldcg(&touched_list[i]);
+        w = __ldcg(&work_keys[j]);
+        snap_keys[j] = w;
+      }
+      push_entry_warp(g, st, sh.b, sh.slot, lists, cap, act, j, key_tri(w), key_dist(w));
+    }
+    if (!grid_barrier(bar, nblocks)) {
+      aborted = true;
+      break;
+    }
+    // ---- advance (every block, identically)
+    if (threadIdx.x == 0) {
+      const uint32_t consumed = sh.cur;
+      if (*(volatile uint32_t*)&st->overflow) {
+        sh.done = 1;
+      } else {
+        bool found = false;
+        for (int k = 0; k <= kRing && !found; ++k) {
+          uint32_t s0 = sh.slot[0];
+          if (*(volatile uint32_t*)&st->count[s0] > 0) {
+            sh.slot[0] = consumed;
+            sh.cur = s0;
+            sh.round += 1;
+            found = true;
+          } else {
+            sh.b += 1;
+            for (int q = 0; q + 1 < kRing; ++q) sh.slot[q] = sh.slot[q + 1];
+            sh.slot[kRing - 1] = s0;
+          }
+        }
+        if (!found) sh.done = 1;
       }
     }
+    __syncthreads();
+    prev_cur = sh.slot[0];  // the consumed list now sits in slot 0 (or the schedule is done)
   }
   if (nan) atomicOr(status, bit(M2S_ERR_NAN_DISTANCE));
   for (int o = 16; o; o >>= 1) evals += __shfl_xor_sync(0xFFFFFFFFu, evals, o);
-  if (lane == 0 && evals) atomicAdd(&st->evals, (unsigned long long)evals);
-  if (threadIdx.x == 0 && blockIdx.x == 0) atomicAdd(&st->entries, (unsigned long long)n);
-}
-
-// Commit: each touched cell publishes its round winner to the snapshot and
-// queues (cell, winning triangle) in the winner's distance bucket.
-__global__ void __launch_bounds__(256) k_commit(GridK g, const unsigned long long* __restrict__ work_keys,
-                                                unsigned long long* snap_keys, const uint32_t* touched_list,
-                                                uint32_t cap, uint2* lists, PropState* st) {
-  if (st->done) return;
-  const uint32_t n = min(st->touched, cap);
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {  // warp-uniform
-    const uint32_t i = base + threadIdx.x;
-    const bool act = i < n;
-    unsigned long long j = 0, w = KEY_EMPTY;
-    if (act) {
-      j = touched_list[i];
-      w = work_keys[j];
-      snap_keys[j] = w;
-    }
-    push_entry_warp(g, st, lists, cap, act, j, key_tri(w), key_dist(w));
+  if (lane == 0 && evals) atomicAdd(&st->evals, evals);
+  if (aborted && blockIdx.x == 0 && threadIdx.x == 0) atomicOr(status, bit(M2S_ERR_LIMIT));
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->round = sh.round;
+    st->done = 1;
   }
 }
 
@@ -513,7 +615,6 @@ int grid_sdf(const MeshView& m, const GridDesc& gd, int sign, float* d_out, uint
     DevBuf<uint32_t> stamp;
     if ((st = work_keys.alloc(N, s)) || (st = stamp.alloc(N, s))) return st;
     uint32_t rounds_launched = 0, attempts = 0;
-    const unsigned relax_blocks = 148u * 8u;
     for (;; ++attempts) {
       // ---- seeding (redone on a restart so every attempt starts from the same state)
       if (attempts > 0) {
@@ -529,10 +630,14 @@ int grid_sdf(const MeshView& m, const GridDesc& gd, int sign, float* d_out, uint
       ++launches;
       if (attempts == 0) mark(1);
 
-      // ---- propagation
+      // ---- propagation: one cooperative launch runs every round
       DevBuf<uint2> lists;
       DevBuf<uint32_t> touched;
-      if ((st = lists.alloc((kRing + 1ull) * cap, s)) || (st = touched.alloc(cap, s))) return st;
+      DevBuf<GridBarrier> bar;
+      if ((st = lists.alloc((kRing + 1ull) * cap, s)) || (st = touched.alloc(2ull * cap, s)) ||
+          (st = bar.alloc(1, s)))
+        return st;
+      M2S_CUDA(cudaMemsetAsync(bar.p, 0, sizeof(GridBarrier), s));
       M2S_CUDA(cudaMemcpyAsync(work_keys.p, snap_keys.p, N * 8, cudaMemcpyDeviceToDevice, s));
       M2S_CUDA(cudaMemsetAsync(stamp.p, 0, N * 4, s));
       unsigned long long ull_max = ULLONG_MAX;
@@ -543,25 +648,31 @@ int grid_sdf(const MeshView& m, const GridDesc& gd, int sign, float* d_out, uint
       k_advance<<<1, 1, 0, s>>>(state.p, cap);
       M2S_CUDA(cudaGetLastError());
       launches += 4;
-      while (true) {
-        for (int r = 0; r < kRoundsPerCheck; ++r) {
-          if (sign == M2S_SIGN_RAYCAST)
-            k_propose<M2S_SIGN_RAYCAST><<<relax_blocks, 256, 0, s>>>(g, m.tris, snap_keys.p, work_keys.p, stamp.p,
-                                                                     lists.p, cap, touched.p, state.p, d_status);
-          else
-            k_propose<M2S_SIGN_NORMAL><<<relax_blocks, 256, 0, s>>>(g, m.tris, snap_keys.p, work_keys.p, stamp.p,
-                                                                    lists.p, cap, touched.p, state.p, d_status);
-          k_commit<<<relax_blocks, 256, 0, s>>>(g, work_keys.p, snap_keys.p, touched.p, cap, lists.p, state.p);
-          k_advance<<<1, 1, 0, s>>>(state.p, cap);
-        }
-        M2S_CUDA(cudaGetLastError());
-        rounds_launched += kRoundsPerCheck;
-        launches += 3ull * kRoundsPerCheck;
-        M2S_CUDA(cudaMemcpyAsync(hst, state.p, sizeof(PropState), cudaMemcpyDeviceToHost, s));
-        M2S_CUDA(cudaStreamSynchronize(s));
-        if (hst->done) break;
-        if (rounds_launched > kMaxRounds) return M2S_ERR_LIMIT;
+      {
+        void* kern = sign == M2S_SIGN_RAYCAST ? (void*)k_propagate<M2S_SIGN_RAYCAST> : (void*)k_propagate<M2S_SIGN_NORMAL>;
+        int dev = 0, sms = 0, per_sm = 0;
+        M2S_CUDA(cudaGetDevice(&dev));
+        M2S_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        M2S_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0));
+        if (per_sm < 1) return M2S_ERR_CUDA;
+        dim3 grid_dim((unsigned)(sms * per_sm)), block_dim(256);
+        const TriRec* tris_p = m.tris;
+        unsigned long long* snap_p = snap_keys.p;
+        unsigned long long* work_p = work_keys.p;
+        uint32_t* stamp_p = stamp.p;
+        uint2* lists_p = lists.p;
+        uint32_t* touched_p = touched.p;
+        PropState* st_p = state.p;
+        GridBarrier* bar_p = bar.p;
+        uint32_t max_rounds = kMaxRounds;
+        void* args[] = {&g, &tris_p, &snap_p, &work_p, &stamp_p, &lists_p, &cap, &touched_p, &st_p, &bar_p, &max_rounds,
+                        &d_status};
+        M2S_CUDA(cudaLaunchCooperativeKernel(kern, grid_dim, block_dim, args, 0, s));
+        ++launches;
       }
+      M2S_CUDA(cudaMemcpyAsync(hst, state.p, sizeof(PropState), cudaMemcpyDeviceToHost, s));
+      M2S_CUDA(cudaStreamSynchronize(s));
+      rounds_launched += hst->round;
       if (!hst->overflow) break;
       if (attempts >= 6 || cap >= 0x40000000u) return M2S_ERR_LIMIT;
       cap *= 2;
