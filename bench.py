@@ -181,10 +181,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-points", action="store_true")
     ap.add_argument("--small", action="store_true",
-                    help="one small pass for profilers: 128^3 grid, 100k Rtree / RtreeBvh points, 8k brute-force points")
+                    help="one short pass for profilers: one grid, 100k Rtree / RtreeBvh points, 8k brute-force points")
+    ap.add_argument("--grid", type=int, default=128, help="grid edge of the --small pass")
     args = ap.parse_args()
     if args.small:
-        return small_case()
+        return small_case(args.grid)
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
     world, rank, local = dist_setup()
@@ -350,8 +351,8 @@ def main():
         torch_destroy()
 
 
-def small_case():
-    """A short, fixed workload for ncu captures (a few hundred MB on the device)."""
+def small_case(edge=128):
+    """A short, fixed workload for ncu captures (at most ~1.5 GB on the device)."""
     import torch
 
     import mesh_to_sdf_b200 as m2s
@@ -359,7 +360,7 @@ def small_case():
 
     A, S = m2s.AccelerationMethod, m2s.SignMethod
     v, idx, lo, hi = workload()
-    grid = grid_for(lo, hi, (128, 128, 128))
+    grid = grid_for(lo, hi, (edge, edge, edge))
     mesh = m2s.build_sdf_acceleration(v, m2s.Topology.TriangleList(idx), A.rtree_bvh())
     out = torch.empty(grid.get_total_cell_count(), dtype=torch.float32, device="cuda")
     status = torch.zeros(1, dtype=torch.int32, device="cuda")

@@ -115,6 +115,22 @@ __device__ __forceinline__ bool beats(unsigned long long cand, unsigned long lon
   return c == -1 || (c == 0 && (uint32_t)(cand >> 32) == (uint32_t)(cur >> 32) && key_tri(cand) < key_tri(cur));
 }
 
+// Lowers *slot to cand if cand beats it; returns true when this call moved the
+// cell off `snap`, its value at the start of the round — exactly one proposal
+// per touched cell and round sees that.
+template <int SIGN>
+__device__ __forceinline__ bool improve_first(unsigned long long* slot, unsigned long long cand, unsigned long long snap,
+                                              bool* nan) {
+  if (SIGN == M2S_SIGN_RAYCAST) return atomicMin(slot, cand) == snap;
+  unsigned long long old = *(volatile unsigned long long*)slot;
+  while (beats<SIGN>(cand, old, nan)) {
+    unsigned long long prev = atomicCAS(slot, old, cand);
+    if (prev == old) return old == snap;
+    old = prev;
+  }
+  return false;
+}
+
 template <int SIGN>
 __device__ __forceinline__ bool update_min(unsigned long long* slot, unsigned long long cand, bool* nan) {
   if (SIGN == M2S_SIGN_RAYCAST) return atomicMin(slot, cand) > cand;
@@ -173,8 +189,14 @@ __global__ void k_seed(GridK g, const TriRec* __restrict__ tris, uint32_t T, uns
   if (lane == 0 && updates) atomicAdd(&st->seeds, (unsigned long long)updates);
 }
 
+// Distance bucket of a state.  Buckets are a quarter cell wide for the first
+// kLinearBuckets (8 cells) and widen in proportion to the distance beyond, so
+// the far field, where many triangles are nearly equidistant, takes few rounds.
+constexpr float kLinearBuckets = 32.0f;
 __device__ __forceinline__ unsigned long long bucket_of(const GridK& g, float d) {
-  return sat_u64(floorf(fabsf(d) * g.inv_delta));
+  float u = fabsf(d) * g.inv_delta;
+  if (u > kLinearBuckets) u = kLinearBuckets * (1.0f + logf(u / kLinearBuckets));
+  return sat_u64(floorf(u));
 }
 
 // Lowest bucket among the seeded cells.
@@ -265,45 +287,71 @@ __global__ void k_advance(PropState* st, uint32_t cap) {
 // All rounds in one cooperative launch.  Every block keeps an identical copy of
 // the bucket schedule in shared memory and advances it from the global list
 // counts after the round's second barrier, so no block waits for a scheduler.
+// Two-level arrival counters (groups of kBarrierFan blocks, then the group
+// leaders) keep the atomics of a barrier from queueing on one address.  Each
+// counter lives in its own 128-byte line.
+constexpr int kBarrierFan = 16;
+constexpr int kBarrierGroups = 128;  // supports up to 2048 co-resident blocks
 struct GridBarrier {
-  unsigned int count;
   unsigned int gen;
   unsigned int abort;
+  unsigned int pad0[30];
+  unsigned int top[32];
+  unsigned int group[kBarrierGroups][32];
 };
+
+__device__ __forceinline__ unsigned int atom_add_acq_rel(unsigned int* p, unsigned int v) {
+  unsigned int old;
+  asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+__device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(unsigned int* p, unsigned int v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 
 // Sense-reversing barrier over the co-resident blocks of a cooperative launch.
 // The wait is bounded: after kBarrierPolls polls it raises `abort`, which makes
 // every block leave the kernel at its next barrier.
-constexpr uint32_t kBarrierPolls = 1u << 24;
+constexpr uint32_t kBarrierPolls = 1u << 22;  // about a second of polling
 
 __device__ __forceinline__ bool grid_barrier(GridBarrier* bar, unsigned int nblocks) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned int* vgen = &bar->gen;
-    volatile unsigned int* vabort = &bar->abort;
-    const unsigned int g0 = *vgen;
-    __threadfence();
-    if (atomicAdd(&bar->count, 1u) == nblocks - 1) {
-      atomicExch(&bar->count, 0u);
-      __threadfence();
-      atomicAdd(&bar->gen, 1u);
+    const unsigned int g0 = ld_acquire(&bar->gen);
+    const unsigned int grp = blockIdx.x / kBarrierFan;
+    const unsigned int ngroups = (nblocks + kBarrierFan - 1) / kBarrierFan;
+    const unsigned int in_grp = min((unsigned)kBarrierFan, nblocks - grp * kBarrierFan);
+    bool last = false;
+    if (atom_add_acq_rel(&bar->group[grp][0], 1u) == in_grp - 1) {
+      bar->group[grp][0] = 0;  // nobody touches this counter again before the release below
+      last = atom_add_acq_rel(&bar->top[0], 1u) == ngroups - 1;
+    }
+    if (last) {
+      bar->top[0] = 0;
+      st_release(&bar->gen, g0 + 1);
     } else {
       uint32_t polls = 0;
-      while (*vgen == g0 && !*vabort) {
+      while (ld_acquire(&bar->gen) == g0) {
+        if (ld_acquire(&bar->abort)) break;
         if (++polls > kBarrierPolls) {
           atomicExch(&bar->abort, 1u);
           break;
         }
-        __nanosleep(64);
       }
     }
-    __threadfence();
-    ok = *vabort ? 0 : 1;
+    ok = ld_acquire(&bar->abort) ? 0 : 1;
   }
   __syncthreads();
   return ok != 0;
 }
+
+constexpr int kTouchStage = 2048;  // touched cells staged per block and round
 
 struct Sched {
   unsigned long long b;
@@ -316,13 +364,16 @@ struct Sched {
 template <int SIGN>
 __global__ void __launch_bounds__(256) k_propagate(GridK g, const TriRec* __restrict__ tris,
                                                    unsigned long long* snap_keys, unsigned long long* work_keys,
-                                                   uint32_t* stamp, uint2* lists, uint32_t cap, uint32_t* touched_lists,
+                                                   uint2* lists, uint32_t cap, uint32_t* touched_lists,
                                                    PropState* st, GridBarrier* bar, uint32_t max_rounds,
                                                    uint32_t* status) {
   __shared__ Sched sh;
+  __shared__ uint32_t s_touch[kTouchStage];
+  __shared__ uint32_t s_ntouch, s_touch_base;
   const unsigned int nblocks = gridDim.x;
   const int lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
+    s_ntouch = 0;
     sh.b = st->b;
     for (int k = 0; k < kRing; ++k) sh.slot[k] = st->slot[k];
     sh.cur = st->cur;
@@ -330,9 +381,6 @@ __global__ void __launch_bounds__(256) k_propagate(GridK g, const TriRec* __rest
     sh.done = st->done;
   }
   __syncthreads();
-  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  const int dx = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dz = lane % 3 - 1;
   bool nan = false;
   unsigned long long evals = 0;
   uint32_t prev_cur = 0xFFFFFFFFu;
@@ -351,38 +399,81 @@ __global__ void __launch_bounds__(256) k_propagate(GridK g, const TriRec* __rest
     if (blockIdx.x == 0 && threadIdx.x == 0 && prev_cur != 0xFFFFFFFFu) st->count[prev_cur] = 0;
     const uint32_t n = min(*(volatile uint32_t*)&st->count[sh.cur], cap);
     const uint2* list = lists + (unsigned long long)sh.cur * cap;
-    for (uint32_t e = warp; e < n; e += nwarps) {
-      const uint2 ent = __ldcg(&list[e]);  // written by other blocks last round
-      const unsigned long long cell = ent.x;
-      const uint32_t tri = ent.y;
-      const int z = (int)(cell % g.n[2]);
-      const int y = (int)((cell / g.n[2]) % g.n[1]);
-      const int x = (int)(cell / ((unsigned long long)g.n[1] * g.n[2]));
-      const int X = x + dx, Y = y + dy, Z = z + dz;
-      bool first = false;
-      unsigned long long j = 0;
-      if (lane < 27 && X >= 0 && Y >= 0 && Z >= 0 && X < g.n[0] && Y < g.n[1] && Z < g.n[2]) {
+    // One thread per (state, neighbour) proposal; consecutive threads share a
+    // state, so its entry and triangle loads are warp broadcasts.  Two
+    // independent proposals per iteration keep two load chains in flight.
+    const unsigned long long P = (unsigned long long)n * 27ull;
+    const unsigned long long T = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long p0 = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; p0 < P; p0 += 2 * T) {
+      bool first[2] = {false, false};
+      unsigned long long jj[2] = {0, 0};
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const unsigned long long p = p0 + (unsigned long long)u * T;
+        if (p >= P) continue;
+        const uint32_t e = (uint32_t)(p / 27ull);
+        const int k = (int)(p - 27ull * e);
+        const uint2 ent = __ldcg(&list[e]);  // written by other blocks last round
+        const unsigned long long cell = ent.x;
+        const uint32_t tri = ent.y;
+        const int z = (int)(cell % g.n[2]);
+        const int y = (int)((cell / g.n[2]) % g.n[1]);
+        const int x = (int)(cell / ((unsigned long long)g.n[1] * g.n[2]));
+        // iproduct!(-1..=1, -1..=1, -1..=1) order (grid.rs:512): x outermost.
+        const int X = x + k / 9 - 1, Y = y + (k / 3) % 3 - 1, Z = z + k % 3 - 1;
+        if (X < 0 || Y < 0 || Z < 0 || X >= g.n[0] || Y >= g.n[1] || Z >= g.n[2]) continue;
+        const unsigned long long j = cell_index(g, X, Y, Z);
+        const unsigned long long snap = __ldcg(&snap_keys[j]);
         const TriRec r = tris[tri];
-        const float d = cell_distance<SIGN>(center(g, X, Y, Z), p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
+        const P3 a = p3(r.a), b = p3(r.b), c = p3(r.c);
+        const P3 pos = center(g, X, Y, Z);
+        // The padded box (1e-4, geo.rs:4-22) is a lower bound on the f32
+        // distance with room to spare: a box farther than the cell's value
+        // cannot beat it, so the exact evaluation is skipped.
+        P3 lo, hi;
+        padded_box(a, b, c, &lo, &hi);
+        const float ex = fmaxf(fmaxf(lo.x - pos.x, pos.x - hi.x), 0.0f);
+        const float ey = fmaxf(fmaxf(lo.y - pos.y, pos.y - hi.y), 0.0f);
+        const float ez = fmaxf(fmaxf(lo.z - pos.z, pos.z - hi.z), 0.0f);
+        const float sd = fabsf(key_dist(snap));
+        if (ex * ex + ey * ey + ez * ez > sd * sd) continue;
+        const float d = cell_distance<SIGN>(pos, a, b, c, __float_as_int(r.a.w));
         ++evals;
         if (isnan(d)) nan = true;
-        j = cell_index(g, X, Y, Z);
         const unsigned long long cand = pack(d, tri);
-        if (beats<SIGN>(cand, __ldcg(&snap_keys[j]), &nan)) {
-          update_min<SIGN>(&work_keys[j], cand, &nan);
-          first = atomicExch(&stamp[j], sh.round) != sh.round;
+        if (beats<SIGN>(cand, snap, &nan)) {
+          first[u] = improve_first<SIGN>(&work_keys[j], cand, snap, &nan);
+          jj[u] = j;
         }
       }
-      const uint32_t fm = __ballot_sync(0xFFFFFFFFu, first);
-      if (fm) {
-        uint32_t base = 0;
-        if (lane == __ffs(fm) - 1) base = atomicAdd(&st->touched2[parity], (uint32_t)__popc(fm));
-        base = __shfl_sync(0xFFFFFFFFu, base, __ffs(fm) - 1);
-        const uint32_t pos = base + __popc(fm & ((1u << lane) - 1u));
-        if (first) {
-          if (pos < cap) touched_list[pos] = (uint32_t)j;
-          else atomicOr(&st->overflow, 1u);
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const unsigned long long j = jj[u];
+        if (first[u]) {
+          const uint32_t q = atomicAdd(&s_ntouch, 1u);
+          if (q < kTouchStage) {
+            s_touch[q] = (uint32_t)j;
+          } else {
+            const uint32_t pos = atomicAdd(&st->touched2[parity], 1u);
+            if (pos < cap) touched_list[pos] = (uint32_t)j;
+            else atomicOr(&st->overflow, 1u);
+          }
         }
+      }
+    }
+    // flush this block's staged touched cells with one global atomic
+    __syncthreads();
+    {
+      const uint32_t nloc = min(s_ntouch, (uint32_t)kTouchStage);
+      if (threadIdx.x == 0) {
+        s_touch_base = nloc ? atomicAdd(&st->touched2[parity], nloc) : 0;
+        s_ntouch = 0;
+      }
+      __syncthreads();
+      for (uint32_t i = threadIdx.x; i < nloc; i += blockDim.x) {
+        const uint32_t pos = s_touch_base + i;
+        if (pos < cap) touched_list[pos] = s_touch[i];
+        else atomicOr(&st->overflow, 1u);
       }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&st->entries, (unsigned long long)n);
@@ -612,8 +703,7 @@ int grid_sdf(const MeshView& m, const GridDesc& gd, int sign, float* d_out, uint
       PropState* p;
       ~HostFree() { cudaFreeHost(p); }
     } hf{hst};
-    DevBuf<uint32_t> stamp;
-    if ((st = work_keys.alloc(N, s)) || (st = stamp.alloc(N, s))) return st;
+    if ((st = work_keys.alloc(N, s))) return st;
     uint32_t rounds_launched = 0, attempts = 0;
     for (;; ++attempts) {
       // ---- seeding (redone on a restart so every attempt starts from the same state)
@@ -639,7 +729,6 @@ int grid_sdf(const MeshView& m, const GridDesc& gd, int sign, float* d_out, uint
         return st;
       M2S_CUDA(cudaMemsetAsync(bar.p, 0, sizeof(GridBarrier), s));
       M2S_CUDA(cudaMemcpyAsync(work_keys.p, snap_keys.p, N * 8, cudaMemcpyDeviceToDevice, s));
-      M2S_CUDA(cudaMemsetAsync(stamp.p, 0, N * 4, s));
       unsigned long long ull_max = ULLONG_MAX;
       M2S_CUDA(cudaMemcpyAsync(&state.p->min_bucket, &ull_max, 8, cudaMemcpyHostToDevice, s));
       k_min_bucket<<<blocks_for(N, 256), 256, 0, s>>>(g, snap_keys.p, state.p);
@@ -655,17 +744,17 @@ int grid_sdf(const MeshView& m, const GridDesc& gd, int sign, float* d_out, uint
         M2S_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         M2S_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0));
         if (per_sm < 1) return M2S_ERR_CUDA;
+        if (sms * per_sm > kBarrierFan * kBarrierGroups) per_sm = (kBarrierFan * kBarrierGroups) / sms;
         dim3 grid_dim((unsigned)(sms * per_sm)), block_dim(256);
         const TriRec* tris_p = m.tris;
         unsigned long long* snap_p = snap_keys.p;
         unsigned long long* work_p = work_keys.p;
-        uint32_t* stamp_p = stamp.p;
         uint2* lists_p = lists.p;
         uint32_t* touched_p = touched.p;
         PropState* st_p = state.p;
         GridBarrier* bar_p = bar.p;
         uint32_t max_rounds = kMaxRounds;
-        void* args[] = {&g, &tris_p, &snap_p, &work_p, &stamp_p, &lists_p, &cap, &touched_p, &st_p, &bar_p, &max_rounds,
+        void* args[] = {&g, &tris_p, &snap_p, &work_p, &lists_p, &cap, &touched_p, &st_p, &bar_p, &max_rounds,
                         &d_status};
         M2S_CUDA(cudaLaunchCooperativeKernel(kern, grid_dim, block_dim, args, 0, s));
         ++launches;
