@@ -38,12 +38,45 @@ constexpr unsigned long long KEY_EMPTY = (0x7F7FFFFFull << 32) | 0xFFFFFFFFull; 
 constexpr int kRing = 16;            // pending distance buckets
 constexpr uint32_t kMaxRounds = 1u << 22;  // bound on propagation rounds
 
+// Unsigned 32-bit division by an invariant divisor with a multiply-high and
+// two shifts (Granlund & Montgomery, "Division by invariant integers using
+// multiplication", PLDI 1994, Figure 4.1): exact for every 32-bit dividend.
+struct FastDiv {
+  uint32_t d, m, s1, s2;
+};
+inline FastDiv make_fastdiv(uint32_t d) {
+  uint32_t l = 0;
+  while (l < 32 && (1ull << l) < d) ++l;  // l = ceil(log2 d)
+  unsigned __int128 num = ((unsigned __int128)1 << 32) * (((unsigned __int128)1 << l) - d);
+  FastDiv f;
+  f.d = d;
+  f.m = (uint32_t)(num / d + 1);
+  f.s1 = l < 1 ? l : 1;
+  f.s2 = l > 0 ? l - 1 : 0;
+  return f;
+}
+__device__ __forceinline__ uint32_t fdiv(const FastDiv& f, uint32_t n) {
+  uint32_t t = __umulhi(f.m, n);
+  return (t + ((n - t) >> f.s1)) >> f.s2;
+}
+
 struct GridK {
   float f[3], s[3];
   int n[3];
   unsigned long long ncell;
   float inv_delta;  // 1 / bucket width
+  FastDiv div_z;    // by n[2]
+  FastDiv div_y;    // by n[1]
 };
+
+// (x, y, z) of a cell index (grid.rs:127-132), 32-bit indices.
+__device__ __forceinline__ void cell_coords(const GridK& g, uint32_t cell, int* x, int* y, int* z) {
+  uint32_t q = fdiv(g.div_z, cell);
+  *z = (int)(cell - q * (uint32_t)g.n[2]);
+  uint32_t xx = fdiv(g.div_y, q);
+  *y = (int)(q - xx * (uint32_t)g.n[1]);
+  *x = (int)xx;
+}
 
 struct PropState {
   unsigned long long b;  // current bucket
@@ -402,42 +435,36 @@ __global__ void __launch_bounds__(256) k_propagate(GridK g, const TriRec* __rest
     // One thread per (state, neighbour) proposal; consecutive threads share a
     // state, so its entry and triangle loads are warp broadcasts.  Two
     // independent proposals per iteration keep two load chains in flight.
-    const unsigned long long P = (unsigned long long)n * 27ull;
-    const unsigned long long T = (unsigned long long)gridDim.x * blockDim.x;
-    for (unsigned long long p0 = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; p0 < P; p0 += 2 * T) {
+    // Thread t takes proposals t, t + T, t + 2T, ... as (state e, neighbour k)
+    // pairs advanced without division: T = 27 * dE + dK.
+    const uint32_t T = gridDim.x * blockDim.x;
+    const uint32_t dE = T / 27u, dK = T % 27u;
+    const uint32_t t0 = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t e = t0 / 27u, k = t0 % 27u;
+    while (e < n) {
       bool first[2] = {false, false};
       unsigned long long jj[2] = {0, 0};
 #pragma unroll
       for (int u = 0; u < 2; ++u) {
-        const unsigned long long p = p0 + (unsigned long long)u * T;
-        if (p >= P) continue;
-        const uint32_t e = (uint32_t)(p / 27ull);
-        const int k = (int)(p - 27ull * e);
-        const uint2 ent = __ldcg(&list[e]);  // written by other blocks last round
-        const unsigned long long cell = ent.x;
+        const uint32_t eu = e, ku = k;
+        k += dK;
+        e += dE;
+        if (k >= 27u) {
+          k -= 27u;
+          ++e;
+        }
+        if (eu >= n) continue;
+        const uint2 ent = __ldcg(&list[eu]);  // written by other blocks last round
         const uint32_t tri = ent.y;
-        const int z = (int)(cell % g.n[2]);
-        const int y = (int)((cell / g.n[2]) % g.n[1]);
-        const int x = (int)(cell / ((unsigned long long)g.n[1] * g.n[2]));
+        int x, y, z;
+        cell_coords(g, ent.x, &x, &y, &z);
         // iproduct!(-1..=1, -1..=1, -1..=1) order (grid.rs:512): x outermost.
-        const int X = x + k / 9 - 1, Y = y + (k / 3) % 3 - 1, Z = z + k % 3 - 1;
+        const int X = x + (int)(ku / 9u) - 1, Y = y + (int)((ku / 3u) % 3u) - 1, Z = z + (int)(ku % 3u) - 1;
         if (X < 0 || Y < 0 || Z < 0 || X >= g.n[0] || Y >= g.n[1] || Z >= g.n[2]) continue;
-        const unsigned long long j = cell_index(g, X, Y, Z);
+        const uint32_t j = (uint32_t)Z + (uint32_t)Y * (uint32_t)g.n[2] + (uint32_t)X * ((uint32_t)g.n[1] * (uint32_t)g.n[2]);
         const unsigned long long snap = __ldcg(&snap_keys[j]);
         const TriRec r = tris[tri];
-        const P3 a = p3(r.a), b = p3(r.b), c = p3(r.c);
-        const P3 pos = center(g, X, Y, Z);
-        // The padded box (1e-4, geo.rs:4-22) is a lower bound on the f32
-        // distance with room to spare: a box farther than the cell's value
-        // cannot beat it, so the exact evaluation is skipped.
-        P3 lo, hi;
-        padded_box(a, b, c, &lo, &hi);
-        const float ex = fmaxf(fmaxf(lo.x - pos.x, pos.x - hi.x), 0.0f);
-        const float ey = fmaxf(fmaxf(lo.y - pos.y, pos.y - hi.y), 0.0f);
-        const float ez = fmaxf(fmaxf(lo.z - pos.z, pos.z - hi.z), 0.0f);
-        const float sd = fabsf(key_dist(snap));
-        if (ex * ex + ey * ey + ez * ez > sd * sd) continue;
-        const float d = cell_distance<SIGN>(pos, a, b, c, __float_as_int(r.a.w));
+        const float d = cell_distance<SIGN>(center(g, X, Y, Z), p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
         ++evals;
         if (isnan(d)) nan = true;
         const unsigned long long cand = pack(d, tri);
@@ -663,6 +690,8 @@ int grid_sdf(const MeshView& m, const GridDesc& gd, int sign, float* d_out, uint
     g.n[d] = (int)gd.n[d];
   }
   g.ncell = N;
+  g.div_z = make_fastdiv((uint32_t)g.n[2]);
+  g.div_y = make_fastdiv((uint32_t)g.n[1]);
   float minsize = std::min(std::fabs(g.s[0]), std::min(std::fabs(g.s[1]), std::fabs(g.s[2])));
   float delta = 0.25f * minsize;
   g.inv_delta = (delta > 0.0f && std::isfinite(delta)) ? 1.0f / delta : 1.0f;
