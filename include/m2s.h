@@ -119,6 +119,26 @@ int m2s_grid_sdf_device(const m2s_mesh* mesh, const float first_cell[3],
                         const float cell_size[3], const uint64_t cell_count[3], int sign,
                         float* d_out, uint32_t* d_status, void* stream);
 
+/* generate_sdf with AccelerationMethod::None for callers that cannot allocate
+ * device memory.  No counterpart in the reference: the crate allocates freely.
+ * Every input and output is a caller-owned device pointer; the only scratch
+ * (the mesh's triangle records and a status word) is a fixed 12 MiB
+ * `static __device__` array inside this library, so the call itself performs
+ * no cudaMalloc/cudaFree.  Callers that need this: real-time loops that cannot
+ * risk the device-wide synchronisation an allocation may cause, and
+ * applications that have already given their whole device-memory budget to
+ * their own pool.  Limits: at most 262,144 triangles (more returns
+ * M2S_ERR_INVALID_ARGUMENT); the array is held by every device that loads the
+ * library until the process exits; all calls share it, so calls that overlap
+ * on the GPU race and must be serialised by the caller.  The first call on a
+ * device looks up the array's address with that device current — make it
+ * before any stream capture.  Returns once d_out is written, with the status
+ * of the kernels (same codes and checks as m2s_generate_sdf). */
+int m2s_generate_sdf_none_noalloc(const float* d_vertices, uint64_t n_vertices,
+                                  const void* d_indices, uint64_t n_indices, int index_bits,
+                                  int topology, const float* d_query_points, uint64_t n_queries,
+                                  int sign, float* d_out, void* stream);
+
 /* ---- utilities ----------------------------------------------------------- */
 
 /* Stable LSD radix sort of (uint32 key, uint32 value) pairs on the device, the

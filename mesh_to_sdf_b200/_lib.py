@@ -27,6 +27,7 @@ SIGNATURES = {
     "m2s_query_sdf_device": (I, [P, P, U64, P, P, P]),
     "m2s_grid_sdf_device": (I, [P, P, P, P, I, P, P, P]),
     "m2s_radix_sort_pairs_device": (I, [P, P, U64, I, P]),
+    "m2s_generate_sdf_none_noalloc": (I, [P, U64, P, U64, I, I, P, U64, I, P, P]),
     "m2s_last_grid_stats": (I, [P]),
     "m2s_set_profiling": (None, [I]),
     "m2s_last_grid_phase_ms": (I, [P]),
