@@ -159,6 +159,13 @@ int m2s_last_grid_stats(uint64_t out[8]);
 void m2s_set_profiling(int enable);
 int m2s_last_grid_phase_ms(float out[4]);
 
+/* Point queries run one thread per query; a query that visits more than
+ * `node_visits` LBVH nodes is continued by a whole warp (points deep inside a
+ * closed mesh see most triangles at nearly the same distance).  0 keeps every
+ * query on one thread.  Process-wide tuning knob; the autotuner sets it. */
+void m2s_set_query_budget(uint32_t node_visits);
+uint32_t m2s_query_budget(void);
+
 const char* m2s_status_string(int status);
 /* Detail of the last failure on the calling thread ("" if none). */
 const char* m2s_last_error(void);

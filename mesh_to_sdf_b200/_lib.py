@@ -31,6 +31,8 @@ SIGNATURES = {
     "m2s_last_grid_stats": (I, [P]),
     "m2s_set_profiling": (None, [I]),
     "m2s_last_grid_phase_ms": (I, [P]),
+    "m2s_set_query_budget": (None, [ctypes.c_uint32]),
+    "m2s_query_budget": (ctypes.c_uint32, []),
     "m2s_status_string": (ctypes.c_char_p, [I]),
     "m2s_last_error": (ctypes.c_char_p, []),
     "m2s_device_available": (I, []),

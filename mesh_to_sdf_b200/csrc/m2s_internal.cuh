@@ -120,8 +120,13 @@ int exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint64_t n, uint32_t* 
 int query_points(const MeshView& m, int accel, int sign, const float* d_q, uint64_t nq, float* d_out,
                  float* d_vec, uint8_t* d_inside, uint32_t* d_status, cudaStream_t s);
 
+// Node visits a query may spend in the one-thread-per-query pass before it is
+// continued one warp per query (0 disables the second pass).
+extern uint32_t g_query_budget;
+
+// allow_alloc = false keeps the brute force in one pass with no scratch buffer.
 int brute_force_sdf(const MeshView& m, int sign, const float* d_q, uint64_t nq, float* d_out,
-                    uint32_t* d_status, cudaStream_t s);
+                    uint32_t* d_status, cudaStream_t s, bool allow_alloc = true);
 
 // ---- grid (m2s_grid.cu) ------------------------------------------------------
 

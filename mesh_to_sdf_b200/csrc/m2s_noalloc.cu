@@ -143,7 +143,8 @@ extern "C" int m2s_generate_sdf_none_noalloc(const float* d_vertices, uint64_t n
                                                                                                3 * n_queries, d_status);
   M2S_CUDA(cudaGetLastError());
   MeshView view{recs, nullptr, nullptr, (uint32_t)T, 0};
-  if ((st = brute_force_sdf(view, sign, d_query_points, n_queries, d_out, d_status, s))) return st;
+  if ((st = brute_force_sdf(view, sign, d_query_points, n_queries, d_out, d_status, s, /*allow_alloc=*/false)))
+    return st;
   uint32_t bits = 0;  // host stack: the copy from pageable memory completes before it returns
   M2S_CUDA(cudaMemcpyAsync(&bits, d_status, sizeof(bits), cudaMemcpyDeviceToHost, s));
   M2S_CUDA(cudaStreamSynchronize(s));

@@ -13,6 +13,7 @@
 //  * query_vector_to_closest_point_rtree_bvh (rtree_bvh.rs:217-276).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cfloat>
 
 #include "m2s_internal.cuh"
@@ -30,17 +31,28 @@ __device__ __forceinline__ P3 load_query(const float* q, uint64_t i) { return {q
 constexpr int kBfThreads = 128;
 constexpr int kBfTile = 256;  // triangles per stage: 256 * 48 B = 12 KiB
 
+// Raycast splits the triangle range into gridDim.y chunks (min and hit parity
+// commute): each chunk folds its part and merges into `part` (atomicMin on the
+// squared distance bits, atomicXor on the parity).  Normal folds all
+// triangles in order in one chunk (compare_distances ties depend on order).
 template <int SIGN>
 __global__ void __launch_bounds__(kBfThreads) k_brute(const TriRec* __restrict__ tris, uint32_t T,
                                                       const float* __restrict__ q, uint64_t nq,
-                                                      float* __restrict__ out, uint32_t* status) {
+                                                      float* __restrict__ out, uint32_t* status,
+                                                      uint2* __restrict__ part) {
   __shared__ __align__(128) TriRec tile[2][kBfTile];
   __shared__ __align__(8) uint64_t bar[2];
   const int tid = threadIdx.x;
   const uint64_t qi = (uint64_t)blockIdx.x * kBfThreads + tid;
   const bool valid = qi < nq;
   const P3 p = valid ? load_query(q, qi) : P3{0.0f, 0.0f, 0.0f};
-  const uint32_t ntile = (T + kBfTile - 1) / kBfTile;
+  // this block's chunk of triangles: whole tiles [t_begin, t_end)
+  const uint32_t all_tiles = (T + kBfTile - 1) / kBfTile;
+  const uint32_t per = (all_tiles + gridDim.y - 1) / gridDim.y;
+  const uint32_t t_begin = min(all_tiles, blockIdx.y * per), t_end = min(all_tiles, t_begin + per);
+  const uint32_t ntile = t_end - t_begin;
+  tris += (uint64_t)t_begin * kBfTile;
+  T = ntile == 0 ? 0u : (t_end == all_tiles ? T - t_begin * kBfTile : ntile * kBfTile);
 
   if (tid == 0) {
     mbar_init(&bar[0], 1);
@@ -95,6 +107,11 @@ __global__ void __launch_bounds__(kBfThreads) k_brute(const TriRec* __restrict__
   if (lost) atomicOr(status, bit(M2S_ERR_LIMIT));
   if (nan) atomicOr(status, bit(M2S_ERR_NAN_DISTANCE));
   if (!valid) return;
+  if (SIGN == 0 && part) {
+    atomicMin(&part[qi].x, __float_as_uint(best));  // non-negative floats order like their bits
+    if (hits & 1u) atomicXor(&part[qi].y, 1u);
+    return;
+  }
   float r;
   if (SIGN == 0) {
     // sqrt(min d2) == min sqrt(d2) (IEEE sqrt is monotone); f32::MAX start value.
@@ -104,6 +121,19 @@ __global__ void __launch_bounds__(kBfThreads) k_brute(const TriRec* __restrict__
     r = best;
   }
   out[qi] = r;
+}
+
+__global__ void k_brute_init(uint2* part, uint64_t nq) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += (uint64_t)gridDim.x * blockDim.x)
+    part[i] = make_uint2(0x7F800000u, 0u);  // +inf, even
+}
+
+__global__ void k_brute_finish(const uint2* __restrict__ part, uint64_t nq, float* __restrict__ out) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint2 pp = part[i];
+    const float d = fminf(F32_MAX, fsqrt(__uint_as_float(pp.x)));
+    out[i] = pp.y ? -d : d;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -140,15 +170,19 @@ struct Nearest {
 
 // Exact nearest triangle under the f32 point_triangle_distance2 (geo.rs:33-37),
 // ties to the lowest triangle index.  Boxes are padded by 1e-4 (geo.rs:4-22),
-// which keeps the f32 box test conservative.
-__device__ Nearest nearest_triangle(const MeshView& m, P3 p, bool* overflow) {
-  Nearest best{INFINITY, 0xFFFFFFFFu, 0};
+// which keeps the f32 box test conservative.  Starts from `best` (an upper
+// bound from an earlier, unfinished search, or +inf).  With a budget, the
+// search gives up after `budget` node visits and clears *finished; `best` is
+// then still a valid upper bound for a second pass.
+__device__ Nearest nearest_triangle(const MeshView& m, P3 p, bool* overflow, Nearest best = {INFINITY, 0xFFFFFFFFu, 0},
+                                    uint32_t budget = 0xFFFFFFFFu, bool* finished = nullptr) {
   auto eval = [&](uint32_t leaf) {
     TriRec r = load_tri(m.stris, leaf);
     float d2 = point_triangle_distance2(p, p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
     uint32_t idx = __float_as_uint(r.b.w);
     if (d2 < best.d2 || (d2 == best.d2 && idx < best.tri)) best = {d2, idx, leaf};
   };
+  if (finished) *finished = true;
   if (m.root & LEAF_BIT) {
     eval(m.root & ~LEAF_BIT);
     return best;
@@ -157,7 +191,12 @@ __device__ Nearest nearest_triangle(const MeshView& m, P3 p, bool* overflow) {
   float st_dist[kStack];
   int sp = 0;
   uint32_t node = 0;
+  uint32_t visits = 0;
   while (true) {
+    if (++visits > budget) {
+      *finished = false;
+      break;
+    }
     BvhNode nd = load_node(m.nodes, node);
     float dl = box_dist2(p, nd.l_lo, nd.l_hi), dr = box_dist2(p, nd.r_lo, nd.r_hi);
     uint32_t L = __float_as_uint(nd.l_lo.w), R = __float_as_uint(nd.l_hi.w);
@@ -204,6 +243,114 @@ __device__ Nearest nearest_triangle(const MeshView& m, P3 p, bool* overflow) {
     if (!found) break;
   }
   return best;
+}
+
+// (d2, triangle) packed so that the unsigned order is the search order.
+__device__ __forceinline__ unsigned long long nn_key(float d2, uint32_t tri) {
+  return ((unsigned long long)__float_as_uint(d2) << 32) | tri;
+}
+__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v) {
+  for (int o = 16; o; o >>= 1) {
+    unsigned long long w = __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    v = w < v ? w : v;
+  }
+  return v;
+}
+
+// One warp per query: the 32 lanes pop the 32 top entries of a shared-memory
+// stack of (node, box distance), test both children of each, evaluate child
+// leaves in parallel and share the running best through a warp minimum.  Used
+// for the queries whose single-thread search ran over its node budget (points
+// deep inside a closed mesh, where many triangles are nearly equidistant).
+// Returns false if the stack would overflow (the caller then finishes the
+// search on one lane).
+constexpr int kWarpStack = 2048;
+
+__device__ bool nearest_triangle_warp(const MeshView& m, P3 p, Nearest* io, uint32_t* s_node, float* s_dist) {
+  const int lane = threadIdx.x & 31;
+  // Non-negative d2 (or +inf / NaN-free boxes) order like their bits.
+  unsigned long long best = nn_key(io->d2, io->tri);
+  uint32_t best_leaf = io->leaf;
+  int sp = 0;
+  if (lane == 0) {
+    s_node[0] = 0;
+    s_dist[0] = 0.0f;
+  }
+  sp = 1;
+  __syncwarp();
+  while (sp > 0) {
+    const int take = min(sp, 32);
+    const int base = sp - take;
+    uint32_t node = 0xFFFFFFFFu;
+    float nd2 = INFINITY;
+    if (lane < take) {
+      node = s_node[base + lane];
+      nd2 = s_dist[base + lane];
+    }
+    __syncwarp();
+    sp = base;
+    const float bound = __uint_as_float((uint32_t)(best >> 32));
+    uint32_t push_ref[2] = {0, 0};
+    float push_d[2] = {0.0f, 0.0f};
+    int npush = 0;
+    unsigned long long cand = ~0ull;
+    uint32_t cand_leaf = 0;
+    if (node != 0xFFFFFFFFu && nd2 <= bound) {
+      BvhNode nd = load_node(m.nodes, node);
+      const uint32_t ch[2] = {__float_as_uint(nd.l_lo.w), __float_as_uint(nd.l_hi.w)};
+      const float cd[2] = {box_dist2(p, nd.l_lo, nd.l_hi), box_dist2(p, nd.r_lo, nd.r_hi)};
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        if (!(cd[c] <= bound)) continue;
+        if (ch[c] & LEAF_BIT) {
+          const uint32_t leaf = ch[c] & ~LEAF_BIT;
+          TriRec r = load_tri(m.stris, leaf);
+          float d2 = point_triangle_distance2(p, p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
+          if (!(d2 <= d2)) continue;  // NaN distances never win
+          unsigned long long k = nn_key(d2, __float_as_uint(r.b.w));
+          if (k < cand) {
+            cand = k;
+            cand_leaf = leaf;
+          }
+        } else {
+          push_ref[npush] = ch[c];
+          push_d[npush] = cd[c];
+          ++npush;
+        }
+      }
+    }
+    // share the best of this step
+    const unsigned long long wmin = warp_min_u64(cand);
+    if (wmin < best) {
+      const uint32_t who = __ffs(__ballot_sync(0xFFFFFFFFu, cand == wmin)) - 1;
+      best_leaf = __shfl_sync(0xFFFFFFFFu, cand_leaf, who);
+      best = wmin;
+    }
+    // push surviving children (deepest first: they go on top)
+    const float nb = __uint_as_float((uint32_t)(best >> 32));
+    int keep = 0;
+    for (int c = 0; c < npush; ++c) keep += push_d[c] <= nb ? 1 : 0;
+    int incl = keep;
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    if (sp + total > kWarpStack) return false;
+    int pos = sp + incl - keep;
+    for (int c = 0; c < npush; ++c)
+      if (push_d[c] <= nb) {
+        s_node[pos] = push_ref[c];
+        s_dist[pos] = push_d[c];
+        ++pos;
+      }
+    sp += total;
+    __syncwarp();
+  }
+  io->d2 = __uint_as_float((uint32_t)(best >> 32));
+  io->tri = (uint32_t)best;
+  io->leaf = best_leaf;
+  return true;
 }
 
 // Number of triangles the +AXIS ray from o crosses (geo.rs:165-216).  A box is
@@ -360,26 +507,30 @@ __device__ float normal_band_fold(const MeshView& m, P3 p, float d2min, bool* na
 
 enum QueryMode { Q_BVH_RAYCAST = 0, Q_BVH_NORMAL = 1, Q_RTREE = 2, Q_VECTOR = 3 };
 
+// A query whose single-thread search ran over its node budget, with its
+// partial result (an upper bound) and its ray vote.
+struct HardQuery {
+  uint32_t i;
+  float d2;
+  uint32_t tri;
+  uint32_t leaf_inside;  // leaf | inside << 31
+};
+
+// Result of a query from its nearest triangle (and ray vote), per method.
 template <int MODE>
-__global__ void __launch_bounds__(128) k_query(MeshView m, const float* __restrict__ q,
-                                               const uint32_t* __restrict__ order, uint64_t nq,
-                                               float* __restrict__ out, float* __restrict__ vec,
-                                               uint8_t* __restrict__ inside_out, uint32_t* status) {
-  uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= nq) return;
-  uint64_t i = order ? order[k] : k;
-  P3 p = load_query(q, i);
-  bool overflow = false, nan = false;
-  Nearest nn = nearest_triangle(m, p, &overflow);
+__device__ __forceinline__ void finish_query(const MeshView& m, uint64_t i, P3 p, Nearest nn, bool inside,
+                                             float* out, float* vec, uint8_t* inside_out, bool* nan, bool* overflow) {
   if (nn.tri == 0xFFFFFFFFu) nn = {INFINITY, 0u, 0u};  // every distance NaN
   if (MODE == Q_BVH_RAYCAST) {
+    // bvh.rs:283-328 / rtree_bvh.rs:156-199: unsigned distance, 3-ray vote.
     float d = fminf(F32_MAX, fsqrt(nn.d2));
-    out[i] = vote_inside(m, p, &overflow) ? -d : d;
+    out[i] = inside ? -d : d;
   } else if (MODE == Q_RTREE) {
+    // rtree.rs:316-323: signed distance of the nearest triangle.
     TriRec r = load_tri(m.tris, nn.tri);
     out[i] = point_triangle_signed_distance(p, p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
   } else if (MODE == Q_BVH_NORMAL) {
-    out[i] = normal_band_fold(m, p, nn.d2, &nan, &overflow);
+    out[i] = normal_band_fold(m, p, nn.d2, nan, overflow);
   } else {
     TriRec r = load_tri(m.tris, nn.tri);
     P3 cp = closest_point_triangle(p, p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
@@ -387,7 +538,63 @@ __global__ void __launch_bounds__(128) k_query(MeshView m, const float* __restri
     vec[3 * i] = v.x;
     vec[3 * i + 1] = v.y;
     vec[3 * i + 2] = v.z;
-    inside_out[i] = vote_inside(m, p, &overflow) ? 1 : 0;
+    inside_out[i] = inside ? 1 : 0;
+  }
+}
+
+// Pass 1: one thread per query.  Searches that exceed `budget` node visits
+// are handed to pass 2 (k_query_hard) with their partial result.
+template <int MODE>
+__global__ void __launch_bounds__(128) k_query(MeshView m, const float* __restrict__ q,
+                                               const uint32_t* __restrict__ order, uint64_t nq,
+                                               float* __restrict__ out, float* __restrict__ vec,
+                                               uint8_t* __restrict__ inside_out, uint32_t* status, uint32_t budget,
+                                               HardQuery* hard, uint32_t* hard_count) {
+  uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nq) return;
+  uint64_t i = order ? order[k] : k;
+  P3 p = load_query(q, i);
+  bool overflow = false, nan = false;
+  bool inside = false;
+  if (MODE == Q_BVH_RAYCAST || MODE == Q_VECTOR) inside = vote_inside(m, p, &overflow);
+  bool finished = true;
+  Nearest nn = nearest_triangle(m, p, &overflow, Nearest{INFINITY, 0xFFFFFFFFu, 0},
+                                (MODE == Q_BVH_NORMAL || !hard) ? 0xFFFFFFFFu : budget, &finished);
+  if (finished) {
+    finish_query<MODE>(m, i, p, nn, inside, out, vec, inside_out, &nan, &overflow);
+  } else {
+    uint32_t pos = atomicAdd(hard_count, 1u);
+    hard[pos] = HardQuery{(uint32_t)i, nn.d2, nn.tri, nn.leaf | (inside ? 0x80000000u : 0u)};
+  }
+  if (overflow) atomicOr(status, bit(M2S_ERR_LIMIT));
+  if (nan) atomicOr(status, bit(M2S_ERR_NAN_DISTANCE));
+}
+
+// Pass 2: one warp per hard query (see nearest_triangle_warp).
+constexpr int kHardWarps = 2;  // warps per block; each owns a kWarpStack-entry stack
+
+template <int MODE>
+__global__ void __launch_bounds__(32 * kHardWarps) k_query_hard(MeshView m, const float* __restrict__ q,
+                                                               const HardQuery* __restrict__ hard,
+                                                               const uint32_t* hard_count, float* __restrict__ out,
+                                                               float* __restrict__ vec, uint8_t* __restrict__ inside_out,
+                                                               uint32_t* status) {
+  __shared__ uint32_t s_node[kHardWarps][kWarpStack];
+  __shared__ float s_dist[kHardWarps][kWarpStack];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t n = *hard_count;
+  bool overflow = false, nan = false;
+  for (uint32_t h = blockIdx.x * kHardWarps + w; h < n; h += gridDim.x * kHardWarps) {
+    const HardQuery hq = hard[h];
+    const P3 p = load_query(q, hq.i);
+    Nearest nn{hq.d2, hq.tri, hq.leaf_inside & 0x7FFFFFFFu};
+    const bool inside = (hq.leaf_inside >> 31) != 0;
+    const bool ok = nearest_triangle_warp(m, p, &nn, s_node[w], s_dist[w]);
+    if (lane == 0) {
+      if (!ok) nn = nearest_triangle(m, p, &overflow, nn);  // stack full: finish on one lane
+      finish_query<MODE>(m, hq.i, p, nn, inside, out, vec, inside_out, &nan, &overflow);
+    }
+    __syncwarp();
   }
   if (overflow) atomicOr(status, bit(M2S_ERR_LIMIT));
   if (nan) atomicOr(status, bit(M2S_ERR_NAN_DISTANCE));
@@ -424,14 +631,31 @@ __global__ void k_query_keys(const float* __restrict__ q, uint64_t nq, MeshView 
 
 }  // namespace
 
+// Node-visit budget of the single-thread search (0: single pass only).
+uint32_t g_query_budget = 768;
+
 int brute_force_sdf(const MeshView& m, int sign, const float* d_q, uint64_t nq, float* d_out, uint32_t* d_status,
-                    cudaStream_t s) {
+                    cudaStream_t s, bool allow_alloc) {
   if (nq == 0) return M2S_OK;
   unsigned blocks = (unsigned)((nq + kBfThreads - 1) / kBfThreads);
-  if (sign == M2S_SIGN_RAYCAST)
-    k_brute<0><<<blocks, kBfThreads, 0, s>>>(m.tris, m.n_tris, d_q, nq, d_out, d_status);
-  else
-    k_brute<1><<<blocks, kBfThreads, 0, s>>>(m.tris, m.n_tris, d_q, nq, d_out, d_status);
+  if (sign == M2S_SIGN_RAYCAST) {
+    // Enough (query, triangle chunk) blocks to fill the GPU ~4 deep.
+    const uint32_t tiles = (m.n_tris + kBfTile - 1) / kBfTile;
+    uint32_t chunks = (uint32_t)std::max<uint64_t>(1, (148ull * 16ull + blocks - 1) / blocks);
+    chunks = std::max(1u, std::min(chunks, std::min(tiles, 64u)));
+    if (chunks == 1 || !allow_alloc) {
+      k_brute<0><<<blocks, kBfThreads, 0, s>>>(m.tris, m.n_tris, d_q, nq, d_out, d_status, nullptr);
+    } else {
+      DevBuf<uint2> part;
+      int st = part.alloc(nq, s);
+      if (st) return st;
+      k_brute_init<<<(unsigned)std::min<uint64_t>((nq + 255) / 256, 148u * 16u), 256, 0, s>>>(part.p, nq);
+      k_brute<0><<<dim3(blocks, chunks), kBfThreads, 0, s>>>(m.tris, m.n_tris, d_q, nq, d_out, d_status, part.p);
+      k_brute_finish<<<(unsigned)std::min<uint64_t>((nq + 255) / 256, 148u * 16u), 256, 0, s>>>(part.p, nq, d_out);
+    }
+  } else {
+    k_brute<1><<<blocks, kBfThreads, 0, s>>>(m.tris, m.n_tris, d_q, nq, d_out, d_status, nullptr);
+  }
   M2S_CUDA(cudaGetLastError());
   return M2S_OK;
 }
@@ -458,18 +682,39 @@ int query_points(const MeshView& m, int accel, int sign, const float* d_q, uint6
                    : (accel == M2S_ACCEL_RTREE ? Q_RTREE
                                                : ((accel == M2S_ACCEL_BVH && sign == M2S_SIGN_NORMAL) ? Q_BVH_NORMAL
                                                                                                       : Q_BVH_RAYCAST));
+  // Queries over the node budget continue one warp per query.
+  DevBuf<HardQuery> hard;
+  DevBuf<uint32_t> hard_count;
+  const bool two_pass = mode != Q_BVH_NORMAL && g_query_budget > 0;
+  if (two_pass) {
+    if ((st = hard.alloc(nq, s)) || (st = hard_count.alloc(1, s))) return st;
+    M2S_CUDA(cudaMemsetAsync(hard_count.p, 0, 4, s));
+  }
+  const uint32_t budget = g_query_budget;
+  HardQuery* hp = two_pass ? hard.p : nullptr;
+  uint32_t* hc = two_pass ? hard_count.p : nullptr;
+  const unsigned hard_blocks = 148u * 32u;
   switch (mode) {
     case Q_BVH_RAYCAST:
-      k_query<Q_BVH_RAYCAST><<<blocks, 128, 0, s>>>(m, d_q, ord, nq, d_out, nullptr, nullptr, d_status);
+      k_query<Q_BVH_RAYCAST><<<blocks, 128, 0, s>>>(m, d_q, ord, nq, d_out, nullptr, nullptr, d_status, budget, hp, hc);
+      if (two_pass)
+        k_query_hard<Q_BVH_RAYCAST><<<hard_blocks, 32 * kHardWarps, 0, s>>>(m, d_q, hp, hc, d_out, nullptr, nullptr,
+                                                                              d_status);
       break;
     case Q_BVH_NORMAL:
-      k_query<Q_BVH_NORMAL><<<blocks, 128, 0, s>>>(m, d_q, ord, nq, d_out, nullptr, nullptr, d_status);
+      k_query<Q_BVH_NORMAL><<<blocks, 128, 0, s>>>(m, d_q, ord, nq, d_out, nullptr, nullptr, d_status, budget, nullptr,
+                                                   nullptr);
       break;
     case Q_RTREE:
-      k_query<Q_RTREE><<<blocks, 128, 0, s>>>(m, d_q, ord, nq, d_out, nullptr, nullptr, d_status);
+      k_query<Q_RTREE><<<blocks, 128, 0, s>>>(m, d_q, ord, nq, d_out, nullptr, nullptr, d_status, budget, hp, hc);
+      if (two_pass)
+        k_query_hard<Q_RTREE><<<hard_blocks, 32 * kHardWarps, 0, s>>>(m, d_q, hp, hc, d_out, nullptr, nullptr, d_status);
       break;
     default:
-      k_query<Q_VECTOR><<<blocks, 128, 0, s>>>(m, d_q, ord, nq, nullptr, d_vec, d_inside, d_status);
+      k_query<Q_VECTOR><<<blocks, 128, 0, s>>>(m, d_q, ord, nq, nullptr, d_vec, d_inside, d_status, budget, hp, hc);
+      if (two_pass)
+        k_query_hard<Q_VECTOR><<<hard_blocks, 32 * kHardWarps, 0, s>>>(m, d_q, hp, hc, nullptr, d_vec, d_inside,
+                                                                         d_status);
   }
   M2S_CUDA(cudaGetLastError());
   return M2S_OK;
