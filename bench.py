@@ -183,9 +183,13 @@ def main():
     ap.add_argument("--small", action="store_true",
                     help="one short pass for profilers: one grid, 100k Rtree / RtreeBvh points, 8k brute-force points")
     ap.add_argument("--grid", type=int, default=128, help="grid edge of the --small pass")
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3"],
+                    help="c2 (default): the headline line; c1 / c3: the small and the terrain configurations")
     args = ap.parse_args()
     if args.small:
         return small_case(args.grid)
+    if args.workload != "c2":
+        return other_workload(args)
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
     world, rank, local = dist_setup()
@@ -368,6 +372,63 @@ def main():
     mesh.close()
     if world > 1:
         torch_destroy()
+
+
+def other_workload(args):
+    """c1: icosphere s3, 32^3 Raycast grid over [-1.2, 1.2]^3, 10,000 RtreeBvh points.
+    c3: 512 x 512 fBm terrain as one TriangleStrip, 384 x 384 x 128 Normal grid over
+    the 10 %-padded bbox, 4M uniform Rtree points.  One JSON line per workload."""
+    import torch
+
+    import mesh_to_sdf_b200 as m2s
+    from mesh_to_sdf_b200 import synth
+
+    A, S = m2s.AccelerationMethod, m2s.SignMethod
+    if args.workload == "c1":
+        v, idx = synth.icosphere(3)
+        topo = m2s.Topology.TriangleList(idx)
+        grid = m2s.Grid.from_bounding_box([-1.2] * 3, [1.2] * 3, [32, 32, 32])
+        sign, am, npts = S.Raycast, A.rtree_bvh(), 10_000
+        q = synth.uniform_points(npts, [-1.2] * 3, [1.2] * 3, seed=SEED)
+    else:
+        v, idx = synth.terrain(512, seed=SEED)
+        topo = m2s.Topology.TriangleStrip(idx)
+        lo, hi = synth.padded_bbox(v, 0.1)
+        grid = m2s.Grid.from_bounding_box(lo, hi, [384, 384, 128])
+        sign, am, npts = S.Normal, A.rtree(), 4_000_000
+        q = synth.uniform_points(npts, lo, hi, seed=SEED)
+    N = grid.get_total_cell_count()
+    mesh = m2s.build_sdf_acceleration(v, topo, am)
+    out = torch.empty(N, dtype=torch.float32, device="cuda")
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for _ in range(args.warmup):
+        mesh.grid_device(grid, sign, out, status)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for i in range(args.steps):
+        flush.fill_(i & 0xFF)
+        ev[i][0].record()
+        mesh.grid_device(grid, sign, out, status)
+        ev[i][1].record()
+    torch.cuda.synchronize()
+    gms = float(np.mean([a.elapsed_time(b_) for a, b_ in ev]))
+    stats = m2s.last_grid_stats()
+    qd = torch.from_numpy(q).cuda()
+    qo = torch.empty(npts, dtype=torch.float32, device="cuda")
+    for _ in range(2):
+        mesh.query_device(qd, qo, status)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    mesh.query_device(qd, qo, status)
+    e1.record()
+    torch.cuda.synchronize()
+    qms = e0.elapsed_time(e1)
+    assert int(status.item()) == 0, int(status.item())
+    print(json.dumps({"workload": args.workload, "triangles": mesh.triangle_count, "grid": list(grid.cell_count),
+                      "sign": sign.name, "grid_ms": gms, "cells_per_s": N / (gms / 1e3), "grid_stats": stats,
+                      "points": npts, "method": repr(am), "points_ms": qms, "pts_per_s": npts / (qms / 1e3)}),
+          flush=True)
 
 
 def small_case(edge=128):
