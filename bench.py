@@ -183,11 +183,16 @@ def main():
     ap.add_argument("--small", action="store_true",
                     help="one short pass for profilers: one grid, 100k Rtree / RtreeBvh points, 8k brute-force points")
     ap.add_argument("--grid", type=int, default=128, help="grid edge of the --small pass")
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3"],
-                    help="c2 (default): the headline line; c1 / c3: the small and the terrain configurations")
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4"],
+                    help="c2 (default): the headline line; c1 / c3: the small and the terrain configurations; "
+                         "c4: 256 grids batched in one plan against 256 single-grid calls")
+    ap.add_argument("--batch", type=int, default=256, help="meshes of the c4 batch")
+    ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()
     if args.small:
         return small_case(args.grid)
+    if args.workload == "c4":
+        return batch_workload(args)
     if args.workload != "c2":
         return other_workload(args)
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
@@ -429,6 +434,70 @@ def other_workload(args):
                       "sign": sign.name, "grid_ms": gms, "cells_per_s": N / (gms / 1e3), "grid_stats": stats,
                       "points": npts, "method": repr(am), "points_ms": qms, "pts_per_s": npts / (qms / 1e3)}),
           flush=True)
+
+
+def batch_workload(args):
+    """c4: `--batch` displaced spheres (subdivision 2..6, scale U[0.5, 2], random
+    rotation) with cubic Raycast grids of edge 32..192 over their padded boxes,
+    all resident.  Times one pass of single-grid calls (one per mesh) against the
+    same grids as one batched plan replayed from its CUDA graph, after checking
+    that both give the same bits.  One JSON line."""
+    import torch
+
+    import mesh_to_sdf_b200 as m2s
+    from mesh_to_sdf_b200 import synth
+
+    A, S = m2s.AccelerationMethod, m2s.SignMethod
+    items = synth.batch_meshes(args.batch, seed=SEED)
+    meshes = [m2s.build_sdf_acceleration(v, m2s.Topology.TriangleList(i), A.none(S.Raycast)) for v, i, *_ in items]
+    grids = [m2s.Grid.from_bounding_box(lo, hi, [e, e, e]) for _, _, lo, hi, e in items]
+    off = m2s.grid_offsets(grids)
+    N = int(off[-1])
+    tris = sum(m.triangle_count for m in meshes)
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    plain = torch.empty(N, dtype=torch.float32, device="cuda")
+    views = [plain[int(off[k]):int(off[k + 1])] for k in range(len(grids))]
+
+    def plain_pass():
+        for m, g, o in zip(meshes, grids, views):
+            m.grid_device(g, S.Raycast, o, status)
+
+    def timed(fn, steps):
+        ms = []
+        for _ in range(steps):
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        return float(np.median(ms))
+
+    plain_pass()
+    plain_ms = timed(plain_pass, max(1, min(args.steps, 3)))
+    batched = torch.empty(N, dtype=torch.float32, device="cuda")
+    plan = m2s.GridPlan(meshes, grids, S.Raycast, batched, status)
+    blocks0 = plan.blocks
+    plan.run()
+    t0 = time.time()
+    chosen = blocks0 if args.no_autotune else plan.autotune()
+    tune_s = time.time() - t0
+    plan.run()
+    stats = m2s.last_grid_stats()
+    batch_ms = timed(plan.run, max(3, args.steps))
+    same = bool(torch.equal(plain.view(torch.int32), batched.view(torch.int32)))
+    assert int(status.item()) == 0, int(status.item())
+    line = {"workload": "c4_batch", "grids": len(grids), "cells": N, "triangles": tris,
+            "plain_ms": plain_ms, "plain_cells_per_s": N / (plain_ms / 1e3),
+            "batched_ms": batch_ms, "batched_cells_per_s": N / (batch_ms / 1e3),
+            "speedup": plain_ms / batch_ms, "bit_identical": same,
+            "blocks_default": blocks0, "blocks_autotuned": chosen, "autotune_s": tune_s,
+            "plan_device_gb": plan.device_bytes / 1e9, "grid_stats": stats}
+    plan.close()
+    print(json.dumps(line), flush=True)
+    if not same:
+        raise SystemExit("batched grids differ from single-grid calls")
 
 
 def small_case(edge=128):

@@ -114,10 +114,59 @@ int m2s_query_sdf_device(const m2s_mesh* mesh, const float* d_query_points, uint
                          float* d_out, uint32_t* d_status, void* stream);
 
 /* generate_grid_sdf against a resident mesh (built with any method; the grid
- * path uses its triangles and LBVH).  d_out: device floats. */
+ * path uses its triangles only).  d_out: device floats.  Unlike the other
+ * _device calls it returns once d_out is written: the host reads back whether
+ * the propagation lists overflowed (and reruns with larger ones if so). */
 int m2s_grid_sdf_device(const m2s_mesh* mesh, const float first_cell[3],
                         const float cell_size[3], const uint64_t cell_count[3], int sign,
                         float* d_out, uint32_t* d_status, void* stream);
+
+/* ---- batches of grids (no counterpart in the reference) ------------------ */
+
+/* The crate computes one grid per call (generate/grid.rs:265-274); a server
+ * with many small requests would pay each call's fixed cost — propagation
+ * rounds that each end in a device-wide barrier — once per grid.  These calls
+ * compute n_grids (mesh, grid) pairs in one job instead.  Grid k uses
+ * meshes[k] (a resident handle; all on the current device) and
+ * first_cells[3k..3k+2], cell_sizes[3k..3k+2], cell_counts[3k..3k+2]; its
+ * cells start at d_out + (cells of grids 0..k-1).  Every grid's result is
+ * bit-identical to m2s_grid_sdf_device on that mesh and grid alone.  The job
+ * addresses cells with 32-bit indices: fewer than 2^32 - 1 cells in total.
+ * Returns once d_out is written. */
+int m2s_grid_sdf_batch_device(const m2s_mesh* const* meshes, uint32_t n_grids,
+                              const float* first_cells, const float* cell_sizes,
+                              const uint64_t* cell_counts, int sign, float* d_out,
+                              uint32_t* d_status, void* stream);
+
+/* A batch prepared once (workspace allocated, pipeline captured into a CUDA
+ * graph) and replayed by m2s_grid_plan_run.  The meshes, d_out and d_status
+ * (required here; the kernels OR status bits into it, the caller clears it)
+ * are bound at creation and must outlive the plan.  `stream` is unused at
+ * creation (the plan allocates and captures on a stream of its own). */
+typedef struct m2s_grid_plan m2s_grid_plan;
+int m2s_grid_plan_create(const m2s_mesh* const* meshes, uint32_t n_grids,
+                         const float* first_cells, const float* cell_sizes,
+                         const uint64_t* cell_counts, int sign, float* d_out,
+                         uint32_t* d_status, void* stream, m2s_grid_plan** out_plan);
+/* Replays the plan on `stream`; returns once d_out is written. */
+int m2s_grid_plan_run(m2s_grid_plan* plan, void* stream);
+/* Times the plan at several cooperative grid sizes (results are identical at
+ * every size), keeps the fastest for this plan and for later plans of the
+ * same class (device, sign, batch or single, log2 of the cell count).
+ * *out_blocks (may be NULL) receives the chosen block count. */
+int m2s_grid_plan_autotune(m2s_grid_plan* plan, void* stream, uint32_t* out_blocks);
+uint64_t m2s_grid_plan_cells(const m2s_grid_plan* plan);
+uint64_t m2s_grid_plan_device_bytes(const m2s_grid_plan* plan);
+uint32_t m2s_grid_plan_blocks(const m2s_grid_plan* plan);
+void m2s_grid_plan_free(m2s_grid_plan* plan);
+/* Forgets every autotuned choice. */
+void m2s_clear_grid_autotune(void);
+
+/* Process-wide grid knobs; they change speed, never results.  blocks_per_sm:
+ * cooperative propagation blocks per SM (0 = occupancy limit);
+ * cells_per_block: the propagation launch uses ceil(cells / this) blocks, at
+ * least 8 (0 = 2048). */
+void m2s_set_grid_tuning(int blocks_per_sm, uint32_t cells_per_block);
 
 /* generate_sdf with AccelerationMethod::None for callers that cannot allocate
  * device memory.  No counterpart in the reference: the crate allocates freely.
@@ -147,9 +196,9 @@ int m2s_generate_sdf_none_noalloc(const float* d_vertices, uint64_t n_vertices,
 int m2s_radix_sort_pairs_device(uint32_t* d_keys, uint32_t* d_values, uint64_t n, int key_bits,
                                 void* stream);
 
-/* Diagnostics of the last grid call on this thread: [seed updates, rounds,
- * states relaxed, neighbour evaluations, ray hits, propagation restarts,
- * kernel launches, relax rounds launched]. */
+/* Diagnostics of the last grid call on this thread: [seed updates, relax
+ * rounds, states relaxed, neighbour evaluations, ray hits, propagation
+ * restarts, kernel launches, far-list redistributions]. */
 int m2s_last_grid_stats(uint64_t out[8]);
 
 /* When enabled (per thread), grid calls time their phases with CUDA events on

@@ -26,6 +26,7 @@ __all__ = [
     "SignMethod", "AccelerationMethod", "Topology", "Grid", "SnapResult", "SdfAccelerationMesh", "M2SError",
     "generate_sdf", "generate_grid_sdf", "build_sdf_acceleration", "query_sdf",
     "query_vector_to_closest_point_rtree_bvh", "ALL_SDF_ACCELERATION_METHODS", "device_available",
+    "grid_sdf_batch_device", "GridPlan", "grid_offsets", "set_grid_tuning", "clear_grid_autotune",
 ]
 
 F32 = np.float32
@@ -276,7 +277,7 @@ def generate_grid_sdf(vertices, indices: Topology, grid: Grid, sign_method: Sign
 
 
 GRID_STATS = ("seed_updates", "rounds", "states_relaxed", "neighbour_evals", "ray_hits", "restarts",
-              "kernel_launches", "rounds_launched")
+              "kernel_launches", "far_phases")
 
 
 def last_grid_stats():
@@ -379,6 +380,97 @@ def query_vector_to_closest_point_rtree_bvh(acceleration: SdfAccelerationMesh, q
                                                       ctypes.byref(n), None)
     _check(st, "query_vector_to_closest_point_rtree_bvh")
     return vec[: n.value], inside[: n.value].astype(bool)
+
+
+# ---- batches of grids (no counterpart in the crate) ---------------------------
+
+def _grid_batch_args(meshes, grids):
+    if len(meshes) != len(grids) or not grids:
+        raise ValueError("one grid per mesh, at least one")
+    handles = (ctypes.c_void_p * len(meshes))(*[m.handle.value for m in meshes])
+    first = np.ascontiguousarray(np.array([g.first_cell for g in grids], F32).reshape(-1))
+    size = np.ascontiguousarray(np.array([g.cell_size for g in grids], F32).reshape(-1))
+    count = np.ascontiguousarray(np.array([g.cell_count for g in grids], np.uint64).reshape(-1))
+    return handles, first, size, count
+
+
+def grid_offsets(grids):
+    """Start of each grid's cells in a batch output, and the total."""
+    sizes = [int(g.get_total_cell_count()) for g in grids]
+    return np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+
+
+def grid_sdf_batch_device(meshes, grids, sign_method: SignMethod, out, status=None, stream=None):
+    """Grid SDFs of (meshes[k], grids[k]) pairs in one job, into the device
+    tensor `out` (the grids' cells back to back, in order, see grid_offsets).
+    Every grid's values are bit-identical to SdfAccelerationMesh.grid_device on
+    that mesh and grid alone; the job runs as many propagation rounds as its
+    slowest grid instead of their sum."""
+    handles, first, size, count = _grid_batch_args(meshes, grids)
+    st = _lib.lib().m2s_grid_sdf_batch_device(handles, len(grids), _vp(first), _vp(size), _vp(count),
+                                              int(sign_method), ctypes.c_void_p(out.data_ptr()),
+                                              None if status is None else ctypes.c_void_p(status.data_ptr()),
+                                              None if stream is None else ctypes.c_void_p(stream))
+    _check(st, "grid_sdf_batch_device")
+
+
+class GridPlan:
+    """A batch of grids captured once into a CUDA graph and replayed with run().
+    The meshes and the device tensors `out` (float32, all cells) and `status`
+    (uint32, cleared by the caller) stay bound to the plan."""
+
+    def __init__(self, meshes, grids, sign_method: SignMethod, out, status):
+        handles, first, size, count = _grid_batch_args(meshes, grids)
+        self._keep = (list(meshes), out, status)
+        h = ctypes.c_void_p(None)
+        st = _lib.lib().m2s_grid_plan_create(handles, len(grids), _vp(first), _vp(size), _vp(count),
+                                             int(sign_method), ctypes.c_void_p(out.data_ptr()),
+                                             ctypes.c_void_p(status.data_ptr()), None, ctypes.byref(h))
+        _check(st, "grid_plan_create")
+        self._h = h
+
+    def run(self, stream=None):
+        _check(_lib.lib().m2s_grid_plan_run(self._h, None if stream is None else ctypes.c_void_p(stream)),
+               "grid_plan_run")
+
+    def autotune(self, stream=None):
+        """Picks the fastest cooperative grid size for this plan; returns it."""
+        b = ctypes.c_uint32(0)
+        _check(_lib.lib().m2s_grid_plan_autotune(self._h, None if stream is None else ctypes.c_void_p(stream),
+                                                 ctypes.byref(b)), "grid_plan_autotune")
+        return int(b.value)
+
+    @property
+    def cells(self):
+        return int(_lib.lib().m2s_grid_plan_cells(self._h))
+
+    @property
+    def device_bytes(self):
+        return int(_lib.lib().m2s_grid_plan_device_bytes(self._h))
+
+    @property
+    def blocks(self):
+        return int(_lib.lib().m2s_grid_plan_blocks(self._h))
+
+    def close(self):
+        if self._h and self._h.value:
+            _lib.lib().m2s_grid_plan_free(self._h)
+            self._h = ctypes.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def set_grid_tuning(blocks_per_sm: int = 0, cells_per_block: int = 2048):
+    """Process-wide grid propagation knobs (speed only)."""
+    _lib.lib().m2s_set_grid_tuning(int(blocks_per_sm), int(cells_per_block))
+
+
+def clear_grid_autotune():
+    _lib.lib().m2s_clear_grid_autotune()
 
 
 def radix_sort_pairs_device(keys, values, key_bits=32, stream=None):

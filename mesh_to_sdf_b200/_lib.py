@@ -26,6 +26,16 @@ SIGNATURES = {
     "m2s_mesh_accel": (I, [P]),
     "m2s_query_sdf_device": (I, [P, P, U64, P, P, P]),
     "m2s_grid_sdf_device": (I, [P, P, P, P, I, P, P, P]),
+    "m2s_grid_sdf_batch_device": (I, [P, ctypes.c_uint32, P, P, P, I, P, P, P]),
+    "m2s_grid_plan_create": (I, [P, ctypes.c_uint32, P, P, P, I, P, P, P, P]),
+    "m2s_grid_plan_run": (I, [P, P]),
+    "m2s_grid_plan_autotune": (I, [P, P, P]),
+    "m2s_grid_plan_cells": (U64, [P]),
+    "m2s_grid_plan_device_bytes": (U64, [P]),
+    "m2s_grid_plan_blocks": (ctypes.c_uint32, [P]),
+    "m2s_grid_plan_free": (None, [P]),
+    "m2s_clear_grid_autotune": (None, []),
+    "m2s_set_grid_tuning": (None, [I, ctypes.c_uint32]),
     "m2s_radix_sort_pairs_device": (I, [P, P, U64, I, P]),
     "m2s_generate_sdf_none_noalloc": (I, [P, U64, P, U64, I, I, P, U64, I, P, P]),
     "m2s_last_grid_stats": (I, [P]),

@@ -48,37 +48,6 @@ int current_pool(cudaMemPool_t* out) {
   return M2S_OK;
 }
 
-// Device check, cached per device: compute capability 10.x (sm_100a build).
-int g_dev_ok[64];  // 0 unknown, 1 ok, 2 unusable
-
-int require_device() {
-  int n = 0;
-  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
-    cudaGetLastError();
-    set_error("no CUDA device");
-    return M2S_ERR_NO_DEVICE;
-  }
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return M2S_ERR_NO_DEVICE;
-  if (g_dev_ok[dev] == 0) {
-    cudaDeviceProp p;
-    if (cudaGetDeviceProperties(&p, dev) != cudaSuccess) return M2S_ERR_NO_DEVICE;
-    g_dev_ok[dev] = p.major == 10 ? 1 : 2;
-  }
-  if (g_dev_ok[dev] != 1) {
-    set_error("the CUDA device is not compute capability 10.x (this library is built for sm_100a)");
-    return M2S_ERR_NO_DEVICE;
-  }
-  return M2S_OK;
-}
-
-int status_from_bits(uint32_t bits) {
-  if (!bits) return M2S_OK;
-  for (int s = 1; s < 32; ++s)
-    if (bits & (1u << s)) return s;
-  return M2S_ERR_CUDA;
-}
-
 // Triangle count of a topology (lib.rs:193-215); M2S_ERR_INDEX_COUNT where the
 // crate asserts len % 3 == 0.
 int triangle_count(uint64_t nv, const void* idx, uint64_t ni, int bits, int topo, uint64_t* T) {
@@ -155,6 +124,43 @@ int cuda_fail(cudaError_t e, const char* what) {
   return e == cudaErrorMemoryAllocation ? M2S_ERR_OUT_OF_MEMORY : M2S_ERR_CUDA;
 }
 
+// Device check, cached per device: compute capability 10.x (sm_100a build).
+int g_dev_ok[64];  // 0 unknown, 1 ok, 2 unusable
+
+int require_device() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    set_error("no CUDA device");
+    return M2S_ERR_NO_DEVICE;
+  }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return M2S_ERR_NO_DEVICE;
+  if (g_dev_ok[dev] == 0) {
+    cudaDeviceProp p;
+    if (cudaGetDeviceProperties(&p, dev) != cudaSuccess) return M2S_ERR_NO_DEVICE;
+    g_dev_ok[dev] = p.major == 10 ? 1 : 2;
+  }
+  if (g_dev_ok[dev] != 1) {
+    set_error("the CUDA device is not compute capability 10.x (this library is built for sm_100a)");
+    return M2S_ERR_NO_DEVICE;
+  }
+  return M2S_OK;
+}
+
+int status_from_bits(uint32_t bits) {
+  if (!bits) return M2S_OK;
+  for (int s = 1; s < 32; ++s)
+    if (bits & (1u << s)) return s;
+  return M2S_ERR_CUDA;
+}
+
+void record_grid_stats(const uint64_t stats[kGridStats]) {
+  for (int i = 0; i < kGridStats; ++i) t_grid_stats[i] = stats[i];
+}
+
+float* grid_phase_slot() { return t_profile ? t_grid_phase_ms : nullptr; }
+
 int dev_alloc(void** p, size_t bytes, cudaStream_t s) {
   cudaMemPool_t pool;
   int st = current_pool(&pool);
@@ -169,13 +175,6 @@ void dev_free(void* p, cudaStream_t s) { cudaFreeAsync(p, s); }
 }  // namespace m2s
 
 using namespace m2s;
-
-struct m2s_mesh {
-  int device = 0;
-  int accel = 0;
-  int sign = 0;
-  DeviceMesh mesh;
-};
 
 namespace {
 

@@ -1,4 +1,5 @@
-// generate_grid_sdf on the device (generate/grid.rs:265-684).
+// generate_grid_sdf on the device (generate/grid.rs:265-684), for one grid or
+// for a batch of (mesh, grid) pairs in one set of launches.
 //
 // 1. Seeding (generate_preheap, grid.rs:383-457): one warp per triangle walks
 //    the cells of its padded, snapped and widened box and keeps, per cell, the
@@ -7,26 +8,40 @@
 // 2. Propagation (generate_heap + propagate_heap, grid.rs:464-558): the
 //    reference pops (cell, triangle) states from heaps in distance order and
 //    evaluates the popped triangle on the 27 cells of the 3x3x3 block, keeping
-//    strict improvements.  Here the heap becomes delta-stepping: states are
-//    binned by distance (bucket width a quarter of the smallest cell size) and
-//    each round relaxes the lowest non-empty bucket, one warp per state and one
-//    lane per neighbour.  A proposal competes with the cell's value at the
-//    start of the round; the round's best proposal per cell wins and is queued
-//    for further propagation.  The result does not depend on the order of
-//    atomics, and on the reference's own test meshes it stays closer to the
-//    single-heap reference than the reference's multi-threaded heaps do.
+//    strict improvements.  Here the heap becomes delta-stepping in one
+//    cooperative launch.  States are binned by distance: a quarter of the
+//    smallest cell size per bucket for the first 8 cells, logarithmically
+//    wider beyond.  Each round relaxes the lowest non-empty bucket, one thread
+//    per (state, neighbour) proposal.  A proposal competes with the cell's
+//    value at the start of the round; the round's best proposal per cell wins
+//    and is queued for further propagation.  Sixteen consecutive buckets (the
+//    window) have their own lists; states beyond the window wait in a far list
+//    and are moved into the window, each to its exact bucket, when the window
+//    runs empty.  So every state is relaxed in the round of its own bucket,
+//    whatever else shares the launch, and the result does not depend on the
+//    order of atomics.
 // 3. Sign (compute_raycasts, grid.rs:568-684): every triangle is tested, with
 //    the reference's aligned ray test, against the rays that start at the cell
 //    centres of the three low faces and lie in its padded box.  A hit at t
 //    toggles bit k = min(floor(t / size), n - 1) of that ray's column; a
 //    suffix XOR turns toggles into per-cell crossing parities, and a cell is
 //    inside when at least two of its three parities are odd (grid.rs:622-639).
+//
+// Batches.  The grids of a batch share one cell index space (grid k starts at
+// a cell offset) and one triangle array (each triangle knows its grid).
+// Buckets are measured in each grid's own cell size and a grid only ever
+// touches its own cells, so a grid's states are relaxed in the same rounds, in
+// the same buckets, as when it runs alone: batched results are bit-identical
+// to single-grid results, and the batch takes as many rounds as its slowest
+// grid instead of the sum.  Kernels are instantiated with MULTI = false (the
+// grid travels in the kernel parameters) and MULTI = true (grid table).
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <climits>
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "m2s_internal.cuh"
 
@@ -35,8 +50,12 @@ namespace {
 
 constexpr uint32_t NO_TRI = 0xFFFFFFFFu;
 constexpr unsigned long long KEY_EMPTY = (0x7F7FFFFFull << 32) | 0xFFFFFFFFull;  // (f32::MAX, none)
-constexpr int kRing = 16;            // pending distance buckets
-constexpr uint32_t kMaxRounds = 1u << 22;  // bound on propagation rounds
+constexpr int kRing = 16;           // buckets of the window
+constexpr int kCur0 = kRing;        // list relaxed first (empty)
+constexpr int kFar0 = kRing + 1;    // far lists kFar0 and kFar0 + 1 (ping-pong)
+constexpr int kLists = kRing + 3;
+constexpr uint32_t kNoBucket = 0xFFFFFFFFu;
+constexpr uint32_t kMaxSteps = 1u << 22;  // bound on rounds + redistributions
 
 // Unsigned 32-bit division by an invariant divisor with a multiply-high and
 // two shifts (Granlund & Montgomery, "Division by invariant integers using
@@ -44,7 +63,7 @@ constexpr uint32_t kMaxRounds = 1u << 22;  // bound on propagation rounds
 struct FastDiv {
   uint32_t d, m, s1, s2;
 };
-inline FastDiv make_fastdiv(uint32_t d) {
+FastDiv make_fastdiv(uint32_t d) {
   uint32_t l = 0;
   while (l < 32 && (1ull << l) < d) ++l;  // l = ceil(log2 d)
   unsigned __int128 num = ((unsigned __int128)1 << 32) * (((unsigned __int128)1 << l) - d);
@@ -60,16 +79,67 @@ __device__ __forceinline__ uint32_t fdiv(const FastDiv& f, uint32_t n) {
   return (t + ((n - t) >> f.s1)) >> f.s2;
 }
 
+// One grid of a job.
 struct GridK {
   float f[3], s[3];
   int n[3];
-  unsigned long long ncell;
-  float inv_delta;  // 1 / bucket width
-  FastDiv div_z;    // by n[2]
-  FastDiv div_y;    // by n[1]
+  uint32_t ncell;     // cells of this grid
+  uint32_t cell_off;  // its first cell in the job's cell index space
+  float inv_delta;    // 1 / bucket width
+  FastDiv div_z;      // by n[2]
+  FastDiv div_y;      // by n[1]
+  uint32_t words[3];  // 32-bit words per ray column, per axis
+  unsigned long long bits_off[3];  // its first ray word, per axis
+  unsigned long long col_off[3];   // its first ray column, per axis
 };
 
-// (x, y, z) of a cell index (grid.rs:127-132), 32-bit indices.
+// Kernel view of a job.
+struct GridSet {
+  GridK g0;                               // single grid: the grid itself
+  const GridK* table;                     // batch: every grid
+  const uint32_t* tri_grid;               // batch: grid of each triangle
+  const uint32_t* cell_off;               // batch: ngrids + 1 cell offsets
+  const unsigned long long* col_off[3];   // batch: ngrids + 1 ray-column offsets per axis
+  uint32_t ngrids;
+  uint32_t ncell;                         // cells of the whole job
+  unsigned long long ncols[3];            // ray columns of the whole job, per axis
+};
+
+// Index k with off[k] <= v < off[k + 1] (off has n + 1 entries, off[0] <= v < off[n]).
+template <class T>
+__device__ __forceinline__ uint32_t find_segment(const T* off, uint32_t n, T v) {
+  uint32_t lo = 0, hi = n;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (off[mid] <= v) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Segment lookups for a thread that walks increasing values: it searches only
+// when the value leaves the segment of the previous one.
+template <class T>
+struct SegCursor {
+  uint32_t k = 0;
+  T lo = 1, hi = 0;
+  __device__ __forceinline__ uint32_t at(const T* off, uint32_t n, T v) {
+    if (v < lo || v >= hi) {
+      k = find_segment(off, n, v);
+      lo = off[k];
+      hi = off[k + 1];
+    }
+    return k;
+  }
+};
+
+template <bool MULTI>
+__device__ __forceinline__ const GridK& grid_of_tri(const GridSet& gs, uint32_t t) {
+  if constexpr (!MULTI) return gs.g0;
+  else return gs.table[__ldg(gs.tri_grid + t)];
+}
+
+// (x, y, z) of a local cell index (grid.rs:127-132).
 __device__ __forceinline__ void cell_coords(const GridK& g, uint32_t cell, int* x, int* y, int* z) {
   uint32_t q = fdiv(g.div_z, cell);
   *z = (int)(cell - q * (uint32_t)g.n[2]);
@@ -79,17 +149,19 @@ __device__ __forceinline__ void cell_coords(const GridK& g, uint32_t cell, int* 
 }
 
 struct PropState {
-  unsigned long long b;  // current bucket
+  uint32_t b;            // current bucket
+  uint32_t B;            // window: buckets B .. B + kRing - 1
   uint32_t slot[kRing];  // list holding bucket b + k
-  uint32_t cur;          // list relaxed this round
-  uint32_t count[kRing + 1];
-  uint32_t touched;
-  uint32_t touched2[2];  // persistent kernel: touched count per round parity
+  uint32_t cur;          // list relaxed in the current round
+  uint32_t fp;           // far list receiving states beyond the window
+  uint32_t count[kLists];
+  uint32_t far_min[2];   // lowest bucket in each far list
+  uint32_t touched2[2];  // touched cells per round parity
   uint32_t done;
   uint32_t overflow;
   uint32_t round;
+  uint32_t far_phases;
   unsigned long long entries, evals, seeds, ray_hits;
-  unsigned long long min_bucket;
 };
 
 __device__ __forceinline__ P3 center(const GridK& g, int x, int y, int z) {
@@ -97,8 +169,8 @@ __device__ __forceinline__ P3 center(const GridK& g, int x, int y, int z) {
   return {fa(g.f[0], fm(__int2float_rn(x), g.s[0])), fa(g.f[1], fm(__int2float_rn(y), g.s[1])),
           fa(g.f[2], fm(__int2float_rn(z), g.s[2]))};
 }
-__device__ __forceinline__ unsigned long long cell_index(const GridK& g, int x, int y, int z) {
-  return (unsigned long long)z + (unsigned long long)y * g.n[2] + (unsigned long long)x * g.n[1] * g.n[2];
+__device__ __forceinline__ uint32_t local_index(const GridK& g, int x, int y, int z) {
+  return (uint32_t)z + (uint32_t)y * (uint32_t)g.n[2] + (uint32_t)x * ((uint32_t)g.n[1] * (uint32_t)g.n[2]);
 }
 
 // Rust `f as isize` (saturating, NaN -> 0).
@@ -182,13 +254,27 @@ __global__ void k_fill_u64(unsigned long long* p, unsigned long long n, unsigned
     p[i] = v;
 }
 
+// Batch triangle array: triangle t of the job is triangle t - tri_off[k] of
+// mesh k.  Keys store the job-wide index, which keeps each mesh's triangle
+// order, so ties resolve exactly as for the mesh alone.
+__global__ void k_gather_tris(const TriRec* const* __restrict__ src, const uint32_t* __restrict__ tri_off,
+                              uint32_t ngrids, uint32_t T, TriRec* __restrict__ out, uint32_t* __restrict__ tri_grid) {
+  SegCursor<uint32_t> sc;
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
+    const uint32_t k = sc.at(tri_off, ngrids, t);
+    out[t] = src[k][t - tri_off[k]];
+    tri_grid[t] = k;
+  }
+}
+
 // ---- 1. seeding -------------------------------------------------------------
-template <int SIGN>
-__global__ void k_seed(GridK g, const TriRec* __restrict__ tris, uint32_t T, unsigned long long* keys,
-                       uint32_t* status, PropState* st) {
+template <int SIGN, bool MULTI>
+__global__ void k_seed(const __grid_constant__ GridSet gs, const TriRec* __restrict__ tris, uint32_t T,
+                       unsigned long long* keys, uint32_t* status, PropState* st) {
   const uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (t >= T) return;
+  const GridK& g = grid_of_tri<MULTI>(gs, t);
   TriRec r = tris[t];
   P3 a = p3(r.a), b = p3(r.b), c = p3(r.c);
   int kind = __float_as_int(r.a.w);
@@ -215,58 +301,51 @@ __global__ void k_seed(GridK g, const TriRec* __restrict__ tris, uint32_t T, uns
     int x = mn[0] + (int)(k / (ez * ey));
     float d = cell_distance<SIGN>(center(g, x, y, z), a, b, c, kind);
     if (isnan(d)) nan = true;
-    if (update_min<SIGN>(&keys[cell_index(g, x, y, z)], pack(d, t), &nan)) ++updates;
+    if (update_min<SIGN>(&keys[g.cell_off + local_index(g, x, y, z)], pack(d, t), &nan)) ++updates;
   }
   if (nan) atomicOr(status, bit(M2S_ERR_NAN_DISTANCE));
   for (int o = 16; o; o >>= 1) updates += __shfl_xor_sync(0xFFFFFFFFu, updates, o);
   if (lane == 0 && updates) atomicAdd(&st->seeds, (unsigned long long)updates);
 }
 
-// Distance bucket of a state.  Buckets are a quarter cell wide for the first
-// kLinearBuckets (8 cells) and widen in proportion to the distance beyond, so
-// the far field, where many triangles are nearly equidistant, takes few rounds.
+// Distance bucket of a state, in its own grid's cell units.  Buckets are a
+// quarter cell wide for the first kLinearBuckets (8 cells) and widen in
+// proportion to the distance beyond, so the far field, where many triangles
+// are nearly equidistant, takes few rounds.  Finite distances stay below a few
+// thousand; a NaN distance (already an error) lands in bucket 0.
 constexpr float kLinearBuckets = 32.0f;
-__device__ __forceinline__ unsigned long long bucket_of(const GridK& g, float d) {
-  float u = fabsf(d) * g.inv_delta;
+__device__ __forceinline__ uint32_t bucket_of(float inv_delta, float d) {
+  float u = fabsf(d) * inv_delta;
   if (u > kLinearBuckets) u = kLinearBuckets * (1.0f + logf(u / kLinearBuckets));
-  return sat_u64(floorf(u));
-}
-
-// Lowest bucket among the seeded cells.
-__global__ void k_min_bucket(GridK g, const unsigned long long* keys, PropState* st) {
-  unsigned long long best = ULLONG_MAX;
-  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < g.ncell;
-       i += (unsigned long long)gridDim.x * blockDim.x) {
-    unsigned long long k = keys[i];
-    if (k != KEY_EMPTY && key_tri(k) != NO_TRI) best = min(best, bucket_of(g, key_dist(k)));
-  }
-  for (int o = 16; o; o >>= 1) best = min(best, __shfl_xor_sync(0xFFFFFFFFu, best, o));
-  if ((threadIdx.x & 31) == 0 && best != ULLONG_MAX) atomicMin(&st->min_bucket, best);
+  if (isnan(u)) return 0;
+  if (!(u < 2147483520.0f)) return 0x7FFFFF00u;
+  return (uint32_t)u;  // floor, u >= 0
 }
 
 __global__ void k_state_init(PropState* st) {
-  // Lists 0..kRing-1 hold buckets b..b+kRing-1, list kRing is the relax list.
-  st->b = st->min_bucket == ULLONG_MAX ? 0 : st->min_bucket;
+  st->b = 0;
+  st->B = 0;
   for (int k = 0; k < kRing; ++k) st->slot[k] = k;
-  st->cur = kRing;
-  for (int k = 0; k <= kRing; ++k) st->count[k] = 0;
-  st->touched = 0;
-  st->done = 0;
-  st->overflow = 0;
+  st->cur = kCur0;
+  st->fp = 0;
+  st->far_min[0] = st->far_min[1] = kNoBucket;
 }
 
-// Appends (cell, triangle) to the list of its distance bucket.  Lanes of a warp
-// that target the same list share one atomicAdd.  Must be called by all 32
-// lanes; `act` says whether this lane pushes.
-__device__ __forceinline__ void push_entry_warp(const GridK& g, PropState* st, unsigned long long b,
-                                                const uint32_t* slots, uint2* lists, uint32_t cap, bool act,
-                                                unsigned long long cell, uint32_t tri, float d) {
+// Appends (cell, triangle) of bucket nb: inside the window to its bucket's list
+// (buckets at or below the current one to the list relaxed next), beyond it to
+// the far list fp.  Lanes of a warp that target the same list share one
+// atomicAdd.  Must be called by all 32 lanes; `act` says whether this lane pushes.
+__device__ __forceinline__ void push_entry_warp(PropState* st, uint32_t b, uint32_t B, const uint32_t* slots,
+                                                uint32_t fp, uint2* lists, uint32_t cap, bool act, uint32_t cell,
+                                                uint32_t tri, uint32_t nb) {
   const int lane = threadIdx.x & 31;
+  const bool far = act && nb >= B + kRing;
   uint32_t slot = 0xFFFFFFFFu;
-  if (act) {
-    unsigned long long nb = bucket_of(g, d);
-    unsigned long long rel = nb > b ? nb - b : 0;
-    slot = slots[rel >= kRing ? kRing - 1 : rel];
+  if (act) slot = far ? (uint32_t)kFar0 + fp : slots[nb > b ? nb - b : 0];
+  const uint32_t farmask = __ballot_sync(0xFFFFFFFFu, far);
+  if (farmask) {
+    const uint32_t m = __reduce_min_sync(0xFFFFFFFFu, far ? nb : kNoBucket);
+    if (lane == __ffs(farmask) - 1) atomicMin(&st->far_min[fp], m);
   }
   const uint32_t group = __match_any_sync(0xFFFFFFFFu, slot);
   if (!act) return;
@@ -276,50 +355,35 @@ __device__ __forceinline__ void push_entry_warp(const GridK& g, PropState* st, u
   base = __shfl_sync(group, base, leader);
   const uint32_t pos = base + __popc(group & ((1u << lane) - 1u));
   if (pos < cap)
-    lists[(unsigned long long)slot * cap + pos] = make_uint2((uint32_t)cell, tri);
+    lists[(unsigned long long)slot * cap + pos] = make_uint2(cell, tri);
   else
-    atomicOr(&st->overflow, 1u);  // the propagation is redone with larger lists
+    atomicOr(&st->overflow, 1u);  // the job is rerun with larger lists
 }
 
-__global__ void k_collect(GridK g, const unsigned long long* keys, PropState* st, uint2* lists, uint32_t cap) {
+// Initial states: every seeded cell with its seed triangle (window 0..15).
+template <bool MULTI>
+__global__ void k_collect(const __grid_constant__ GridSet gs, const unsigned long long* keys, PropState* st,
+                          uint2* lists, uint32_t cap) {
+  SegCursor<uint32_t> sc;
   const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
-  for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < g.ncell; base += stride) {
+  for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < gs.ncell; base += stride) {
     const unsigned long long i = base + threadIdx.x;  // warp-uniform loop, lanes mask out past the end
-    unsigned long long k = i < g.ncell ? keys[i] : KEY_EMPTY;
-    bool act = k != KEY_EMPTY && key_tri(k) != NO_TRI;
-    push_entry_warp(g, st, st->b, st->slot, lists, cap, act, i, key_tri(k), key_dist(k));
-  }
-}
-
-// Picks the next list to relax: the lowest non-empty bucket.
-__global__ void k_advance(PropState* st, uint32_t cap) {
-  if (st->done) return;
-  if (st->overflow) {  // this attempt is void; the host restarts it with larger lists
-    st->done = 1;
-    return;
-  }
-  st->count[st->cur] = 0;
-  st->touched = 0;
-  for (int it = 0; it <= kRing; ++it) {
-    uint32_t s0 = st->slot[0];
-    if (st->count[s0] > 0) {
-      st->slot[0] = st->cur;
-      st->cur = s0;
-      st->round += 1;
-      return;
+    const unsigned long long k = i < gs.ncell ? keys[i] : KEY_EMPTY;
+    const bool act = key_tri(k) != NO_TRI;
+    uint32_t nb = 0;
+    if (act) {
+      const float inv = MULTI ? gs.table[sc.at(gs.cell_off, gs.ngrids, (uint32_t)i)].inv_delta : gs.g0.inv_delta;
+      nb = bucket_of(inv, key_dist(k));
     }
-    st->b += 1;
-    for (int k = 0; k + 1 < kRing; ++k) st->slot[k] = st->slot[k + 1];
-    st->slot[kRing - 1] = s0;
+    push_entry_warp(st, 0, 0, st->slot, 0, lists, cap, act, (uint32_t)i, key_tri(k), nb);
   }
-  st->done = 1;
 }
 
-// ---- 2. relaxation rounds (persistent) -------------------------------------
-// ---- persistent propagation ---------------------------------------------------
-// All rounds in one cooperative launch.  Every block keeps an identical copy of
-// the bucket schedule in shared memory and advances it from the global list
-// counts after the round's second barrier, so no block waits for a scheduler.
+// ---- 2. relaxation (one persistent cooperative launch) -------------------------
+// Every block keeps an identical copy of the bucket schedule in shared memory
+// and advances it from the global list counts after each grid barrier, so no
+// block waits for a scheduler.
+//
 // Two-level arrival counters (groups of kBarrierFan blocks, then the group
 // leaders) keep the atomics of a barrier from queueing on one address.  Each
 // counter lives in its own 128-byte line.
@@ -387,49 +451,119 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* bar, unsigned int nblo
 constexpr int kTouchStage = 2048;  // touched cells staged per block and round
 
 struct Sched {
-  unsigned long long b;
+  uint32_t b, B;
   uint32_t slot[kRing];
-  uint32_t cur;
-  uint32_t round;
-  uint32_t done;
+  uint32_t cur, fp, round;
+  int action;
 };
+enum { kRelax = 0, kRedistribute = 1, kDone = 2, kLimit = 3 };
 
-template <int SIGN>
-__global__ void __launch_bounds__(256) k_propagate(GridK g, const TriRec* __restrict__ tris,
+// Next step of the schedule, computed by thread 0 of every block from the
+// global list counts (final at this point: the last grid barrier ordered every
+// push before it).  Block 0 also empties the list relaxed last round, which no
+// block reads here and which receives pushes only after the next barrier.
+__device__ __forceinline__ int next_step(Sched& sh, PropState* st, bool leader) {
+  if (*(volatile uint32_t*)&st->overflow) return kDone;
+  const uint32_t consumed = sh.cur;
+  for (int q = 0; q < kRing; ++q) {
+    const uint32_t s0 = sh.slot[0];
+    if (*(volatile uint32_t*)&st->count[s0] > 0) {
+      sh.slot[0] = consumed;  // becomes the list of states re-queued at bucket b
+      sh.cur = s0;
+      sh.round += 1;
+      if (leader) st->count[consumed] = 0;
+      return kRelax;
+    }
+    if (sh.b + 1 >= sh.B + kRing) break;  // window exhausted
+    sh.b += 1;
+    for (int w = 0; w + 1 < kRing; ++w) sh.slot[w] = sh.slot[w + 1];
+    sh.slot[kRing - 1] = s0;
+  }
+  // Every window list is empty.  Far states all lie at or beyond B + kRing, so
+  // the new window starts at the lowest of them.
+  if (*(volatile uint32_t*)&st->count[kFar0 + sh.fp] == 0) return kDone;
+  sh.B = sh.b = *(volatile uint32_t*)&st->far_min[sh.fp];
+  return kRedistribute;
+}
+
+template <int SIGN, bool MULTI>
+__global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ GridSet gs, const TriRec* __restrict__ tris,
                                                    unsigned long long* snap_keys, unsigned long long* work_keys,
                                                    uint2* lists, uint32_t cap, uint32_t* touched_lists,
-                                                   PropState* st, GridBarrier* bar, uint32_t max_rounds,
+                                                   PropState* st, GridBarrier* bar, uint32_t max_steps,
                                                    uint32_t* status) {
   __shared__ Sched sh;
   __shared__ uint32_t s_touch[kTouchStage];
   __shared__ uint32_t s_ntouch, s_touch_base;
   const unsigned int nblocks = gridDim.x;
   const int lane = threadIdx.x & 31;
+  const bool lead_block = blockIdx.x == 0;
   if (threadIdx.x == 0) {
     s_ntouch = 0;
     sh.b = st->b;
+    sh.B = st->B;
     for (int k = 0; k < kRing; ++k) sh.slot[k] = st->slot[k];
     sh.cur = st->cur;
-    sh.round = st->round;
-    sh.done = st->done;
+    sh.fp = st->fp;
+    sh.round = 0;
   }
-  __syncthreads();
   bool nan = false;
   unsigned long long evals = 0;
-  uint32_t prev_cur = 0xFFFFFFFFu;
+  uint32_t far_phases = 0;
   bool aborted = false;
-  for (uint32_t it = 0; !sh.done; ++it) {
-    if (it >= max_rounds) {
-      if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(status, bit(M2S_ERR_LIMIT));
+  for (uint32_t it = 0;; ++it) {
+    if (threadIdx.x == 0) sh.action = it >= max_steps ? kLimit : next_step(sh, st, lead_block);
+    __syncthreads();
+    const int action = sh.action;
+    if (action == kDone) break;
+    if (action == kLimit) {
+      if (lead_block && threadIdx.x == 0) atomicOr(status, bit(M2S_ERR_LIMIT));
       break;
+    }
+    if (action == kRedistribute) {
+      // ---- move every far state to its bucket's list, or to the other far
+      // list when it lies beyond the new window.  The bucket is recomputed
+      // from the state's cell and triangle, the same arithmetic that produced
+      // it, so it is exactly the bucket the state was filed under.
+      const uint32_t F = kFar0 + sh.fp;
+      const uint32_t nf = min(*(volatile uint32_t*)&st->count[F], cap);
+      const uint2* far = lists + (unsigned long long)F * cap;
+      for (uint32_t base = blockIdx.x * blockDim.x; base < nf; base += gridDim.x * blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        const bool act = i < nf;
+        uint2 ent = make_uint2(0, 0);
+        uint32_t nb = 0;
+        if (act) {
+          ent = __ldcg(&far[i]);
+          const GridK& g = grid_of_tri<MULTI>(gs, ent.y);
+          int x, y, z;
+          cell_coords(g, ent.x - g.cell_off, &x, &y, &z);
+          const TriRec r = tris[ent.y];
+          const float d = cell_distance<SIGN>(center(g, x, y, z), p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
+          nb = bucket_of(g.inv_delta, d);
+        }
+        push_entry_warp(st, sh.b, sh.B, sh.slot, sh.fp ^ 1u, lists, cap, act, ent.x, ent.y, nb);
+      }
+      if (!grid_barrier(bar, nblocks)) {
+        aborted = true;
+        break;
+      }
+      if (threadIdx.x == 0) {
+        if (lead_block) {  // the drained list is next written by the next redistribution
+          st->count[F] = 0;
+          st->far_min[sh.fp] = kNoBucket;
+        }
+        sh.fp ^= 1u;
+        ++far_phases;
+      }
+      continue;
     }
     const uint32_t parity = sh.round & 1u;
     uint32_t* touched_list = touched_lists + (unsigned long long)parity * cap;
     // ---- propose: every state of the bucket evaluates its triangle at the 27
-    // cells of its 3x3x3 block (one lane per cell); a proposal that beats the
-    // cell's value at the start of the round enters the working value (atomic
-    // minimum) and the first such proposal lists the cell as touched.
-    if (blockIdx.x == 0 && threadIdx.x == 0 && prev_cur != 0xFFFFFFFFu) st->count[prev_cur] = 0;
+    // cells of its 3x3x3 block; a proposal that beats the cell's value at the
+    // start of the round enters the working value (atomic minimum) and the
+    // first such proposal lists the cell as touched.
     const uint32_t n = min(*(volatile uint32_t*)&st->count[sh.cur], cap);
     const uint2* list = lists + (unsigned long long)sh.cur * cap;
     // One thread per (state, neighbour) proposal; consecutive threads share a
@@ -443,7 +577,7 @@ __global__ void __launch_bounds__(256) k_propagate(GridK g, const TriRec* __rest
     uint32_t e = t0 / 27u, k = t0 % 27u;
     while (e < n) {
       bool first[2] = {false, false};
-      unsigned long long jj[2] = {0, 0};
+      uint32_t jj[2] = {0, 0};
 #pragma unroll
       for (int u = 0; u < 2; ++u) {
         const uint32_t eu = e, ku = k;
@@ -454,14 +588,15 @@ __global__ void __launch_bounds__(256) k_propagate(GridK g, const TriRec* __rest
           ++e;
         }
         if (eu >= n) continue;
-        const uint2 ent = __ldcg(&list[eu]);  // written by other blocks last round
+        const uint2 ent = __ldcg(&list[eu]);  // written by other blocks in earlier rounds
         const uint32_t tri = ent.y;
+        const GridK& g = grid_of_tri<MULTI>(gs, tri);
         int x, y, z;
-        cell_coords(g, ent.x, &x, &y, &z);
+        cell_coords(g, ent.x - g.cell_off, &x, &y, &z);
         // iproduct!(-1..=1, -1..=1, -1..=1) order (grid.rs:512): x outermost.
         const int X = x + (int)(ku / 9u) - 1, Y = y + (int)((ku / 3u) % 3u) - 1, Z = z + (int)(ku % 3u) - 1;
         if (X < 0 || Y < 0 || Z < 0 || X >= g.n[0] || Y >= g.n[1] || Z >= g.n[2]) continue;
-        const uint32_t j = (uint32_t)Z + (uint32_t)Y * (uint32_t)g.n[2] + (uint32_t)X * ((uint32_t)g.n[1] * (uint32_t)g.n[2]);
+        const uint32_t j = g.cell_off + local_index(g, X, Y, Z);
         const unsigned long long snap = __ldcg(&snap_keys[j]);
         const TriRec r = tris[tri];
         const float d = cell_distance<SIGN>(center(g, X, Y, Z), p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
@@ -475,14 +610,13 @@ __global__ void __launch_bounds__(256) k_propagate(GridK g, const TriRec* __rest
       }
 #pragma unroll
       for (int u = 0; u < 2; ++u) {
-        const unsigned long long j = jj[u];
         if (first[u]) {
           const uint32_t q = atomicAdd(&s_ntouch, 1u);
           if (q < kTouchStage) {
-            s_touch[q] = (uint32_t)j;
+            s_touch[q] = jj[u];
           } else {
             const uint32_t pos = atomicAdd(&st->touched2[parity], 1u);
-            if (pos < cap) touched_list[pos] = (uint32_t)j;
+            if (pos < cap) touched_list[pos] = jj[u];
             else atomicOr(&st->overflow, 1u);
           }
         }
@@ -503,72 +637,45 @@ __global__ void __launch_bounds__(256) k_propagate(GridK g, const TriRec* __rest
         else atomicOr(&st->overflow, 1u);
       }
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&st->entries, (unsigned long long)n);
+    if (lead_block && threadIdx.x == 0) atomicAdd(&st->entries, (unsigned long long)n);
     if (!grid_barrier(bar, nblocks)) {
       aborted = true;
       break;
     }
     // ---- commit: each touched cell publishes its round winner to the snapshot
-    // and queues (cell, winning triangle) in the winner's distance bucket.
-    if (blockIdx.x == 0 && threadIdx.x == 0) st->touched2[parity ^ 1u] = 0;
+    // and queues (cell, winning triangle) under the winner's distance bucket.
+    if (lead_block && threadIdx.x == 0) st->touched2[parity ^ 1u] = 0;
     const uint32_t nt = min(*(volatile uint32_t*)&st->touched2[parity], cap);
     for (uint32_t base = blockIdx.x * blockDim.x; base < nt; base += gridDim.x * blockDim.x) {
       const uint32_t i = base + threadIdx.x;
       const bool act = i < nt;
-      unsigned long long j = 0, w = KEY_EMPTY;
+      uint32_t j = 0, nb = 0;
+      unsigned long long w = KEY_EMPTY;
       if (act) {
         j = __ldcg(&touched_list[i]);
         w = __ldcg(&work_keys[j]);
         snap_keys[j] = w;
+        nb = bucket_of(grid_of_tri<MULTI>(gs, key_tri(w)).inv_delta, key_dist(w));
       }
-      push_entry_warp(g, st, sh.b, sh.slot, lists, cap, act, j, key_tri(w), key_dist(w));
+      push_entry_warp(st, sh.b, sh.B, sh.slot, sh.fp, lists, cap, act, j, key_tri(w), nb);
     }
     if (!grid_barrier(bar, nblocks)) {
       aborted = true;
       break;
     }
-    // ---- advance (every block, identically)
-    if (threadIdx.x == 0) {
-      const uint32_t consumed = sh.cur;
-      if (*(volatile uint32_t*)&st->overflow) {
-        sh.done = 1;
-      } else {
-        bool found = false;
-        for (int k = 0; k <= kRing && !found; ++k) {
-          uint32_t s0 = sh.slot[0];
-          if (*(volatile uint32_t*)&st->count[s0] > 0) {
-            sh.slot[0] = consumed;
-            sh.cur = s0;
-            sh.round += 1;
-            found = true;
-          } else {
-            sh.b += 1;
-            for (int q = 0; q + 1 < kRing; ++q) sh.slot[q] = sh.slot[q + 1];
-            sh.slot[kRing - 1] = s0;
-          }
-        }
-        if (!found) sh.done = 1;
-      }
-    }
-    __syncthreads();
-    prev_cur = sh.slot[0];  // the consumed list now sits in slot 0 (or the schedule is done)
   }
   if (nan) atomicOr(status, bit(M2S_ERR_NAN_DISTANCE));
   for (int o = 16; o; o >>= 1) evals += __shfl_xor_sync(0xFFFFFFFFu, evals, o);
   if (lane == 0 && evals) atomicAdd(&st->evals, evals);
-  if (aborted && blockIdx.x == 0 && threadIdx.x == 0) atomicOr(status, bit(M2S_ERR_LIMIT));
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (aborted && lead_block && threadIdx.x == 0) atomicOr(status, bit(M2S_ERR_LIMIT));
+  if (lead_block && threadIdx.x == 0) {
     st->round = sh.round;
+    st->far_phases = far_phases;
     st->done = 1;
   }
 }
 
 // ---- 3. rays -------------------------------------------------------------------
-struct RayK {
-  uint32_t* bits[3];  // per axis: column-major toggles, words[col * W + w]
-  uint32_t words[3];  // W per axis
-};
-
 __device__ __forceinline__ unsigned long long column_of(const GridK& g, int axis, int x, int y, int z) {
   if (axis == 0) return (unsigned long long)y * g.n[2] + z;
   if (axis == 1) return (unsigned long long)x * g.n[2] + z;
@@ -591,12 +698,14 @@ __device__ __forceinline__ void lattice_range(const GridK& g, int d, float lo, f
   if (fb_ < 0.0f || fa_ > (float)(g.n[d] - 1)) *b = *a - 1;  // no lattice point in range
 }
 
-template <int AXIS>
-__global__ void k_rays(GridK g, const TriRec* __restrict__ tris, uint32_t T, RayK rk, PropState* st) {
+template <int AXIS, bool MULTI>
+__global__ void k_rays(const __grid_constant__ GridSet gs, const TriRec* __restrict__ tris, uint32_t T, uint32_t* bits,
+                       PropState* st) {
   constexpr int IY = (AXIS + 1) % 3, IZ = (AXIS + 2) % 3;
   const uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (t >= T) return;
+  const GridK& g = grid_of_tri<MULTI>(gs, t);
   TriRec r = tris[t];
   P3 a = p3(r.a), b = p3(r.b), c = p3(r.c);
   P3 lo, hi;
@@ -607,8 +716,8 @@ __global__ void k_rays(GridK g, const TriRec* __restrict__ tris, uint32_t T, Ray
   if (j1 < j0 || k1 < k0) return;
   const int nj = j1 - j0 + 1, nk = k1 - k0 + 1;
   const long long total = (long long)nj * nk;
-  uint32_t* bitsA = rk.bits[AXIS];
-  const uint32_t W = rk.words[AXIS];
+  uint32_t* bitsA = bits + g.bits_off[AXIS];
+  const uint32_t W = g.words[AXIS];
   uint32_t hits = 0;
   for (long long q = lane; q < total; q += 32) {
     int c3[3];
@@ -632,11 +741,16 @@ __global__ void k_rays(GridK g, const TriRec* __restrict__ tris, uint32_t T, Ray
 
 // Toggle bits -> suffix parity: bit i becomes the XOR of toggles i..n-1, i.e.
 // the parity of the hits whose cell range 0..=k covers cell i.
-__global__ void k_suffix(uint32_t* bits, unsigned long long ncols, uint32_t W) {
+template <bool MULTI>
+__global__ void k_suffix(const __grid_constant__ GridSet gs, int axis, uint32_t* bits) {
+  SegCursor<unsigned long long> sc;
+  const unsigned long long ncols = gs.ncols[axis];
   for (unsigned long long col = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; col < ncols;
        col += (unsigned long long)gridDim.x * blockDim.x) {
+    const GridK& g = MULTI ? gs.table[sc.at(gs.col_off[axis], gs.ngrids, col)] : gs.g0;
+    const uint32_t W = g.words[axis];
+    uint32_t* w = bits + g.bits_off[axis] + (col - g.col_off[axis]) * W;
     uint32_t carry = 0;
-    uint32_t* w = bits + col * W;
     for (int i = (int)W - 1; i >= 0; --i) {
       uint32_t s = w[i];
       s ^= s >> 1;
@@ -651,18 +765,20 @@ __global__ void k_suffix(uint32_t* bits, unsigned long long ncols, uint32_t W) {
   }
 }
 
-template <int SIGN>
-__global__ void k_finalize(GridK g, const unsigned long long* __restrict__ keys, RayK rk, float* __restrict__ out) {
-  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < g.ncell;
+template <int SIGN, bool MULTI>
+__global__ void k_finalize(const __grid_constant__ GridSet gs, const unsigned long long* __restrict__ keys,
+                           const uint32_t* __restrict__ bits, float* __restrict__ out) {
+  SegCursor<uint32_t> sc;
+  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < gs.ncell;
        i += (unsigned long long)gridDim.x * blockDim.x) {
     float d = key_dist(keys[i]);
     if (SIGN == M2S_SIGN_RAYCAST) {
-      int z = (int)(i % g.n[2]);
-      int y = (int)((i / g.n[2]) % g.n[1]);
-      int x = (int)(i / ((unsigned long long)g.n[1] * g.n[2]));
-      uint32_t px = (rk.bits[0][column_of(g, 0, x, y, z) * rk.words[0] + (x >> 5)] >> (x & 31)) & 1u;
-      uint32_t py = (rk.bits[1][column_of(g, 1, x, y, z) * rk.words[1] + (y >> 5)] >> (y & 31)) & 1u;
-      uint32_t pz = (rk.bits[2][column_of(g, 2, x, y, z) * rk.words[2] + (z >> 5)] >> (z & 31)) & 1u;
+      const GridK& g = MULTI ? gs.table[sc.at(gs.cell_off, gs.ngrids, (uint32_t)i)] : gs.g0;
+      int x, y, z;
+      cell_coords(g, (uint32_t)i - g.cell_off, &x, &y, &z);
+      uint32_t px = (bits[g.bits_off[0] + column_of(g, 0, x, y, z) * g.words[0] + (x >> 5)] >> (x & 31)) & 1u;
+      uint32_t py = (bits[g.bits_off[1] + column_of(g, 1, x, y, z) * g.words[1] + (y >> 5)] >> (y & 31)) & 1u;
+      uint32_t pz = (bits[g.bits_off[2] + column_of(g, 2, x, y, z) * g.words[2] + (z >> 5)] >> (z & 31)) & 1u;
       if (px + py + pz >= 2) d = -d;
     }
     out[i] = d;
@@ -674,34 +790,315 @@ unsigned blocks_for(unsigned long long n, int threads, unsigned cap = 148u * 16u
   return (unsigned)std::max<unsigned long long>(1, std::min<unsigned long long>(b, cap));
 }
 
+// Pinned host copy of the propagation state, one per host thread.
+struct HostState {
+  PropState* p = nullptr;
+  ~HostState() {
+    if (p) cudaFreeHost(p);
+  }
+};
+PropState* host_state() {
+  thread_local HostState h;
+  if (!h.p && cudaHostAlloc((void**)&h.p, sizeof(PropState), cudaHostAllocPortable) != cudaSuccess) {
+    cudaGetLastError();
+    h.p = nullptr;
+  }
+  return h.p;
+}
+
+template <int SIGN>
+const void* propagate_kernel(bool multi) {
+  return multi ? (const void*)k_propagate<SIGN, true> : (const void*)k_propagate<SIGN, false>;
+}
+
 }  // namespace
 
-int grid_sdf(const MeshView& m, const GridDesc& gd, int sign, float* d_out, uint32_t* d_status, cudaStream_t s,
-             uint64_t stats[kGridStats], float phase_ms[4]) {
-  const unsigned long long N = gd.cells();
-  if (N == 0) return M2S_OK;
-  for (int d = 0; d < 3; ++d)
-    if (gd.n[d] > 0x7FFFFFFFull) return M2S_ERR_INVALID_ARGUMENT;
-  if (N > 0xFFFFFFFFull) return M2S_ERR_INVALID_ARGUMENT;  // cells are addressed with 32-bit entries
-  GridK g;
-  for (int d = 0; d < 3; ++d) {
-    g.f[d] = gd.first[d];
-    g.s[d] = gd.size[d];
-    g.n[d] = (int)gd.n[d];
-  }
-  g.ncell = N;
-  g.div_z = make_fastdiv((uint32_t)g.n[2]);
-  g.div_y = make_fastdiv((uint32_t)g.n[1]);
-  float minsize = std::min(std::fabs(g.s[0]), std::min(std::fabs(g.s[1]), std::fabs(g.s[2])));
-  float delta = 0.25f * minsize;
-  g.inv_delta = (delta > 0.0f && std::isfinite(delta)) ? 1.0f / delta : 1.0f;
-
-  const uint32_t T = m.n_tris;
+struct GridJob::Impl {
+  std::vector<GridK> grids;
+  GridSet gs{};
+  bool multi = false;
+  int sign = 0;
+  uint32_t T = 0;
+  const TriRec* tris = nullptr;
+  float* d_out = nullptr;
+  uint32_t* d_status = nullptr;
+  uint32_t cap = 0;
+  unsigned coop_blocks = 0;
+  unsigned coop_max = 0;
+  unsigned long long ray_words = 0;
   uint64_t launches = 0;
-  // Phase events (seeding, propagation, rays, finalize) when asked for.
+  DevBuf<TriRec> comb_tris;
+  DevBuf<const TriRec*> src_tris;
+  DevBuf<uint32_t> tri_grid, tri_off, cell_off;
+  DevBuf<unsigned long long> col_off[3];
+  DevBuf<GridK> table;
+  DevBuf<unsigned long long> snap, work;
+  DevBuf<PropState> state;
+  DevBuf<GridBarrier> bar;
+  DevBuf<uint32_t> bits;
+  DevBuf<uint2> lists;
+  DevBuf<uint32_t> touched;
+};
+
+GridJob::GridJob() : p(new Impl) {}
+GridJob::~GridJob() { delete p; }
+uint32_t GridJob::capacity() const { return p->cap; }
+void GridJob::set_capacity(uint32_t cap) { p->cap = cap; }
+uint64_t GridJob::cells() const { return p->gs.ncell; }
+unsigned GridJob::cooperative_blocks() const { return p->coop_blocks; }
+unsigned GridJob::max_cooperative_blocks() const { return p->coop_max; }
+void GridJob::set_cooperative_blocks(unsigned blocks) { p->coop_blocks = std::max(1u, std::min(blocks, p->coop_max)); }
+int GridJob::sign() const { return p->sign; }
+uint32_t GridJob::grids() const { return p->gs.ngrids; }
+uint64_t GridJob::device_bytes() const {
+  const Impl& J = *p;
+  return J.comb_tris.n * sizeof(TriRec) + J.tri_grid.n * 4 + (J.snap.n + J.work.n) * 8 + J.bits.n * 4 +
+         (uint64_t)kLists * J.cap * 8 + 2ull * J.cap * 4 + J.table.n * sizeof(GridK);
+}
+
+int check_grid(const GridDesc& g) {
+  for (int d = 0; d < 3; ++d)
+    if (g.n[d] == 0 || g.n[d] > 0x7FFFFFFFull) return M2S_ERR_INVALID_ARGUMENT;
+  if (g.cells() >= 0xFFFFFFFFull) return M2S_ERR_INVALID_ARGUMENT;  // cells are addressed with 32-bit indices
+  return M2S_OK;
+}
+
+int GridJob::prepare(const MeshView* meshes, uint32_t n, const GridDesc* gds, int sign, float* d_out,
+                     uint32_t* d_status, cudaStream_t s, const GridTuning& tune) {
+  Impl& J = *p;
+  if (n == 0) return M2S_ERR_INVALID_ARGUMENT;
+  J.sign = sign;
+  J.d_out = d_out;
+  J.d_status = d_status;
+  J.multi = n > 1;
+  J.grids.assign(n, GridK{});
+  unsigned long long cells = 0, tris = 0, cols[3] = {0, 0, 0}, words[3] = {0, 0, 0};
+  std::vector<uint32_t> h_cell_off(n + 1), h_tri_off(n + 1);
+  std::vector<unsigned long long> h_col_off[3];
+  std::vector<const TriRec*> h_src(n);
+  for (int a = 0; a < 3; ++a) h_col_off[a].assign(n + 1, 0);
+  int st;
+  for (uint32_t k = 0; k < n; ++k) {
+    const GridDesc& gd = gds[k];
+    if ((st = check_grid(gd))) return st;
+    GridK& g = J.grids[k];
+    for (int d = 0; d < 3; ++d) {
+      g.f[d] = gd.first[d];
+      g.s[d] = gd.size[d];
+      g.n[d] = (int)gd.n[d];
+    }
+    const unsigned long long nk = gd.cells();
+    if (cells + nk >= 0xFFFFFFFFull) return M2S_ERR_INVALID_ARGUMENT;  // 32-bit cell indices across the job
+    g.ncell = (uint32_t)nk;
+    g.cell_off = (uint32_t)cells;
+    h_cell_off[k] = (uint32_t)cells;
+    cells += nk;
+    g.div_z = make_fastdiv((uint32_t)g.n[2]);
+    g.div_y = make_fastdiv((uint32_t)g.n[1]);
+    const float minsize = std::min(std::fabs(g.s[0]), std::min(std::fabs(g.s[1]), std::fabs(g.s[2])));
+    const float delta = 0.25f * minsize;
+    g.inv_delta = (delta > 0.0f && std::isfinite(delta)) ? 1.0f / delta : 1.0f;
+    for (int a = 0; a < 3; ++a) {
+      const unsigned long long nc = nk / gd.n[a];
+      g.words[a] = (uint32_t)((gd.n[a] + 31) / 32);
+      g.col_off[a] = cols[a];
+      h_col_off[a][k] = cols[a];
+      g.bits_off[a] = words[a];
+      cols[a] += nc;
+      words[a] += nc * g.words[a];
+    }
+    h_tri_off[k] = (uint32_t)tris;
+    h_src[k] = meshes[k].tris;
+    tris += meshes[k].n_tris;
+    if (tris > 0x7FFFFFFFull) return M2S_ERR_INVALID_ARGUMENT;
+  }
+  h_cell_off[n] = (uint32_t)cells;
+  h_tri_off[n] = (uint32_t)tris;
+  // The three axes share one bit array, axis after axis.
+  unsigned long long woff = 0;
+  for (int a = 0; a < 3; ++a) {
+    h_col_off[a][n] = cols[a];
+    for (auto& g : J.grids) g.bits_off[a] += woff;
+    woff += words[a];
+    J.gs.ncols[a] = cols[a];
+  }
+  J.ray_words = woff;
+  J.T = (uint32_t)tris;
+  J.gs.g0 = J.grids[0];
+  J.gs.ngrids = n;
+  J.gs.ncell = (uint32_t)cells;
+  if (J.multi) {
+    if ((st = J.table.alloc(n, s)) || (st = J.cell_off.alloc(n + 1, s)) || (st = J.tri_off.alloc(n + 1, s)) ||
+        (st = J.src_tris.alloc(n, s)) || (st = J.comb_tris.alloc(tris, s)) || (st = J.tri_grid.alloc(tris, s)))
+      return st;
+    for (int a = 0; a < 3; ++a)
+      if ((st = J.col_off[a].alloc(n + 1, s))) return st;
+    // Pageable sources: each copy has read its source when the call returns.
+    M2S_CUDA(cudaMemcpyAsync(J.table.p, J.grids.data(), n * sizeof(GridK), cudaMemcpyHostToDevice, s));
+    M2S_CUDA(cudaMemcpyAsync(J.cell_off.p, h_cell_off.data(), (n + 1) * 4ull, cudaMemcpyHostToDevice, s));
+    M2S_CUDA(cudaMemcpyAsync(J.tri_off.p, h_tri_off.data(), (n + 1) * 4ull, cudaMemcpyHostToDevice, s));
+    M2S_CUDA(cudaMemcpyAsync(J.src_tris.p, h_src.data(), n * sizeof(TriRec*), cudaMemcpyHostToDevice, s));
+    for (int a = 0; a < 3; ++a)
+      M2S_CUDA(cudaMemcpyAsync(J.col_off[a].p, h_col_off[a].data(), (n + 1) * 8ull, cudaMemcpyHostToDevice, s));
+    if (tris) {
+      k_gather_tris<<<blocks_for(tris, 256), 256, 0, s>>>(J.src_tris.p, J.tri_off.p, n, (uint32_t)tris, J.comb_tris.p,
+                                                          J.tri_grid.p);
+      M2S_CUDA(cudaGetLastError());
+    }
+    J.tris = J.comb_tris.p;
+    J.gs.table = J.table.p;
+    J.gs.tri_grid = J.tri_grid.p;
+    J.gs.cell_off = J.cell_off.p;
+    for (int a = 0; a < 3; ++a) J.gs.col_off[a] = J.col_off[a].p;
+  } else {
+    J.tris = meshes[0].tris;
+  }
+  const unsigned long long N = cells;
+  if ((st = J.snap.alloc(N, s)) || (st = J.work.alloc(N, s)) || (st = J.state.alloc(1, s)) ||
+      (st = J.bar.alloc(1, s)))
+    return st;
+  if (sign == M2S_SIGN_RAYCAST && (st = J.bits.alloc(woff, s))) return st;
+  J.cap = tune.list_capacity
+              ? tune.list_capacity
+              : (uint32_t)std::min<unsigned long long>(std::max<unsigned long long>(N / 2, std::min(N + 1024, 1ull << 20)),
+                                                       0x40000000ull);
+  // Cooperative grid: co-resident blocks, fewer for small jobs (a barrier
+  // over fewer blocks is faster and a small bucket does not fill many).
+  const void* kern = sign == M2S_SIGN_RAYCAST ? propagate_kernel<M2S_SIGN_RAYCAST>(J.multi)
+                                              : propagate_kernel<M2S_SIGN_NORMAL>(J.multi);
+  int dev = 0, sms = 0, per_sm = 0;
+  M2S_CUDA(cudaGetDevice(&dev));
+  M2S_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  M2S_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0));
+  if (per_sm < 1) {
+    set_error("grid propagation kernel cannot be resident");
+    return M2S_ERR_CUDA;
+  }
+  J.coop_max = (unsigned)std::min<unsigned long long>((unsigned long long)sms * per_sm,
+                                                     (unsigned long long)kBarrierFan * kBarrierGroups);
+  if (tune.blocks_per_sm > 0) per_sm = std::min(per_sm, tune.blocks_per_sm);
+  const unsigned long long cpb = std::max<uint32_t>(tune.cells_per_block, 1);
+  const unsigned long long want = std::max<unsigned long long>(8, (N + cpb - 1) / cpb);
+  J.coop_blocks = (unsigned)std::min<unsigned long long>(
+      want, std::min<unsigned long long>((unsigned long long)sms * per_sm, J.coop_max));
+  return M2S_OK;
+}
+
+int GridJob::alloc_lists(cudaStream_t s) {
+  Impl& J = *p;
+  int st;
+  if ((st = J.lists.alloc((unsigned long long)kLists * J.cap, s)) || (st = J.touched.alloc(2ull * J.cap, s))) return st;
+  return M2S_OK;
+}
+
+int GridJob::enqueue(cudaStream_t s, cudaEvent_t* ev) {
+  Impl& J = *p;
+  const unsigned long long N = J.gs.ncell;
+  const bool raycast = J.sign == M2S_SIGN_RAYCAST;
+  const bool multi = J.multi;
+  J.launches = 0;
+  auto mark = [&](int i) -> int {
+    if (ev) M2S_CUDA(cudaEventRecord(ev[i], s));
+    return M2S_OK;
+  };
+  int st;
+  if ((st = mark(0))) return st;
+  M2S_CUDA(cudaMemsetAsync(J.state.p, 0, sizeof(PropState), s));
+  k_state_init<<<1, 1, 0, s>>>(J.state.p);
+  k_fill_u64<<<blocks_for(N, 256), 256, 0, s>>>(J.snap.p, N, KEY_EMPTY);
+  J.launches += 2;
+  if (J.T > 0) {
+    const unsigned sb = (unsigned)((J.T * 32ull + 255) / 256);
+    if (raycast) {
+      if (multi) k_seed<M2S_SIGN_RAYCAST, true><<<sb, 256, 0, s>>>(J.gs, J.tris, J.T, J.snap.p, J.d_status, J.state.p);
+      else k_seed<M2S_SIGN_RAYCAST, false><<<sb, 256, 0, s>>>(J.gs, J.tris, J.T, J.snap.p, J.d_status, J.state.p);
+    } else {
+      if (multi) k_seed<M2S_SIGN_NORMAL, true><<<sb, 256, 0, s>>>(J.gs, J.tris, J.T, J.snap.p, J.d_status, J.state.p);
+      else k_seed<M2S_SIGN_NORMAL, false><<<sb, 256, 0, s>>>(J.gs, J.tris, J.T, J.snap.p, J.d_status, J.state.p);
+    }
+    ++J.launches;
+  }
+  M2S_CUDA(cudaGetLastError());
+  if ((st = mark(1))) return st;
+  if (J.T > 0) {
+    M2S_CUDA(cudaMemsetAsync(J.bar.p, 0, sizeof(GridBarrier), s));
+    M2S_CUDA(cudaMemcpyAsync(J.work.p, J.snap.p, N * 8, cudaMemcpyDeviceToDevice, s));
+    if (multi) k_collect<true><<<blocks_for(N, 256), 256, 0, s>>>(J.gs, J.snap.p, J.state.p, J.lists.p, J.cap);
+    else k_collect<false><<<blocks_for(N, 256), 256, 0, s>>>(J.gs, J.snap.p, J.state.p, J.lists.p, J.cap);
+    M2S_CUDA(cudaGetLastError());
+    const void* kern = raycast ? propagate_kernel<M2S_SIGN_RAYCAST>(multi) : propagate_kernel<M2S_SIGN_NORMAL>(multi);
+    uint32_t max_steps = kMaxSteps;
+    const TriRec* tris = J.tris;
+    void* args[] = {&J.gs,        &tris,      &J.snap.p, &J.work.p,  &J.lists.p,   &J.cap,
+                    &J.touched.p, &J.state.p, &J.bar.p,  &max_steps, &J.d_status};
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(J.coop_blocks);
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    M2S_CUDA(cudaLaunchKernelExC(&cfg, kern, args));
+    J.launches += 2;
+  }
+  if ((st = mark(2))) return st;
+  const unsigned fb = blocks_for(N, 256, 148u * 32u);
+  if (raycast) {
+    M2S_CUDA(cudaMemsetAsync(J.bits.p, 0, J.ray_words * 4, s));
+    if (J.T > 0) {
+      const unsigned rb = (unsigned)((J.T * 32ull + 255) / 256);
+      if (multi) {
+        k_rays<0, true><<<rb, 256, 0, s>>>(J.gs, J.tris, J.T, J.bits.p, J.state.p);
+        k_rays<1, true><<<rb, 256, 0, s>>>(J.gs, J.tris, J.T, J.bits.p, J.state.p);
+        k_rays<2, true><<<rb, 256, 0, s>>>(J.gs, J.tris, J.T, J.bits.p, J.state.p);
+      } else {
+        k_rays<0, false><<<rb, 256, 0, s>>>(J.gs, J.tris, J.T, J.bits.p, J.state.p);
+        k_rays<1, false><<<rb, 256, 0, s>>>(J.gs, J.tris, J.T, J.bits.p, J.state.p);
+        k_rays<2, false><<<rb, 256, 0, s>>>(J.gs, J.tris, J.T, J.bits.p, J.state.p);
+      }
+      J.launches += 3;
+    }
+    for (int a = 0; a < 3; ++a) {
+      if (multi) k_suffix<true><<<blocks_for(J.gs.ncols[a], 256), 256, 0, s>>>(J.gs, a, J.bits.p);
+      else k_suffix<false><<<blocks_for(J.gs.ncols[a], 256), 256, 0, s>>>(J.gs, a, J.bits.p);
+    }
+    J.launches += 3;
+    M2S_CUDA(cudaGetLastError());
+    if ((st = mark(3))) return st;
+    if (multi) k_finalize<M2S_SIGN_RAYCAST, true><<<fb, 256, 0, s>>>(J.gs, J.snap.p, J.bits.p, J.d_out);
+    else k_finalize<M2S_SIGN_RAYCAST, false><<<fb, 256, 0, s>>>(J.gs, J.snap.p, J.bits.p, J.d_out);
+  } else {
+    if ((st = mark(3))) return st;
+    if (multi) k_finalize<M2S_SIGN_NORMAL, true><<<fb, 256, 0, s>>>(J.gs, J.snap.p, nullptr, J.d_out);
+    else k_finalize<M2S_SIGN_NORMAL, false><<<fb, 256, 0, s>>>(J.gs, J.snap.p, nullptr, J.d_out);
+  }
+  M2S_CUDA(cudaGetLastError());
+  ++J.launches;
+  return mark(4);
+}
+
+int GridJob::read_state(cudaStream_t s, GridRunInfo* info) {
+  Impl& J = *p;
+  PropState* h = host_state();
+  if (!h) return M2S_ERR_OUT_OF_MEMORY;
+  M2S_CUDA(cudaMemcpyAsync(h, J.state.p, sizeof(PropState), cudaMemcpyDeviceToHost, s));
+  M2S_CUDA(cudaStreamSynchronize(s));
+  info->overflow = h->overflow != 0;
+  info->seeds = h->seeds;
+  info->rounds = h->round;
+  info->entries = h->entries;
+  info->evals = h->evals;
+  info->ray_hits = h->ray_hits;
+  info->far_phases = h->far_phases;
+  info->launches = J.launches;
+  return M2S_OK;
+}
+
+int run_grid_job(GridJob& job, cudaStream_t s, uint64_t stats[kGridStats], float phase_ms[4]) {
   cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
-  if (phase_ms)
-    for (auto& e : ev) M2S_CUDA(cudaEventCreate(&e));
   struct EvFree {
     cudaEvent_t* e;
     ~EvFree() {
@@ -709,150 +1106,52 @@ int grid_sdf(const MeshView& m, const GridDesc& gd, int sign, float* d_out, uint
         if (e[i]) cudaEventDestroy(e[i]);
     }
   } evf{ev};
-  auto mark = [&](int i) {
-    if (phase_ms) cudaEventRecord(ev[i], s);
-  };
-  mark(0);
-  DevBuf<unsigned long long> snap_keys, work_keys;
-  DevBuf<PropState> state;
+  if (phase_ms)
+    for (auto& e : ev) M2S_CUDA(cudaEventCreate(&e));
+  GridRunInfo info;
+  uint32_t restarts = 0;
   int st;
-  if ((st = snap_keys.alloc(N, s)) || (st = state.alloc(1, s))) return st;
-  M2S_CUDA(cudaMemsetAsync(state.p, 0, sizeof(PropState), s));
-  k_fill_u64<<<blocks_for(N, 256), 256, 0, s>>>(snap_keys.p, N, KEY_EMPTY);
-  M2S_CUDA(cudaGetLastError());
-  ++launches;
-
-  if (T > 0) {
-    unsigned sb = (unsigned)((T * 32ull + 255) / 256);
-    uint32_t cap = (uint32_t)std::min<unsigned long long>(std::max<unsigned long long>(N / 2, 1ull << 20),
-                                                          0x7FFFFFFFull);
-    PropState* hst = nullptr;
-    M2S_CUDA(cudaMallocHost(&hst, sizeof(PropState)));
-    struct HostFree {
-      PropState* p;
-      ~HostFree() { cudaFreeHost(p); }
-    } hf{hst};
-    if ((st = work_keys.alloc(N, s))) return st;
-    uint32_t rounds_launched = 0, attempts = 0;
-    for (;; ++attempts) {
-      // ---- seeding (redone on a restart so every attempt starts from the same state)
-      if (attempts > 0) {
-        k_fill_u64<<<blocks_for(N, 256), 256, 0, s>>>(snap_keys.p, N, KEY_EMPTY);
-        M2S_CUDA(cudaMemsetAsync(state.p, 0, sizeof(PropState), s));
-        ++launches;
-      }
-      if (sign == M2S_SIGN_RAYCAST)
-        k_seed<M2S_SIGN_RAYCAST><<<sb, 256, 0, s>>>(g, m.tris, T, snap_keys.p, d_status, state.p);
-      else
-        k_seed<M2S_SIGN_NORMAL><<<sb, 256, 0, s>>>(g, m.tris, T, snap_keys.p, d_status, state.p);
-      M2S_CUDA(cudaGetLastError());
-      ++launches;
-      if (attempts == 0) mark(1);
-
-      // ---- propagation: one cooperative launch runs every round
-      DevBuf<uint2> lists;
-      DevBuf<uint32_t> touched;
-      DevBuf<GridBarrier> bar;
-      if ((st = lists.alloc((kRing + 1ull) * cap, s)) || (st = touched.alloc(2ull * cap, s)) ||
-          (st = bar.alloc(1, s)))
-        return st;
-      M2S_CUDA(cudaMemsetAsync(bar.p, 0, sizeof(GridBarrier), s));
-      M2S_CUDA(cudaMemcpyAsync(work_keys.p, snap_keys.p, N * 8, cudaMemcpyDeviceToDevice, s));
-      unsigned long long ull_max = ULLONG_MAX;
-      M2S_CUDA(cudaMemcpyAsync(&state.p->min_bucket, &ull_max, 8, cudaMemcpyHostToDevice, s));
-      k_min_bucket<<<blocks_for(N, 256), 256, 0, s>>>(g, snap_keys.p, state.p);
-      k_state_init<<<1, 1, 0, s>>>(state.p);
-      k_collect<<<blocks_for(N, 256), 256, 0, s>>>(g, snap_keys.p, state.p, lists.p, cap);
-      k_advance<<<1, 1, 0, s>>>(state.p, cap);
-      M2S_CUDA(cudaGetLastError());
-      launches += 4;
-      {
-        void* kern = sign == M2S_SIGN_RAYCAST ? (void*)k_propagate<M2S_SIGN_RAYCAST> : (void*)k_propagate<M2S_SIGN_NORMAL>;
-        int dev = 0, sms = 0, per_sm = 0;
-        M2S_CUDA(cudaGetDevice(&dev));
-        M2S_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        M2S_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0));
-        if (per_sm < 1) return M2S_ERR_CUDA;
-        if (sms * per_sm > kBarrierFan * kBarrierGroups) per_sm = (kBarrierFan * kBarrierGroups) / sms;
-        dim3 grid_dim((unsigned)(sms * per_sm)), block_dim(256);
-        const TriRec* tris_p = m.tris;
-        unsigned long long* snap_p = snap_keys.p;
-        unsigned long long* work_p = work_keys.p;
-        uint2* lists_p = lists.p;
-        uint32_t* touched_p = touched.p;
-        PropState* st_p = state.p;
-        GridBarrier* bar_p = bar.p;
-        uint32_t max_rounds = kMaxRounds;
-        void* args[] = {&g, &tris_p, &snap_p, &work_p, &lists_p, &cap, &touched_p, &st_p, &bar_p, &max_rounds,
-                        &d_status};
-        M2S_CUDA(cudaLaunchCooperativeKernel(kern, grid_dim, block_dim, args, 0, s));
-        ++launches;
-      }
-      M2S_CUDA(cudaMemcpyAsync(hst, state.p, sizeof(PropState), cudaMemcpyDeviceToHost, s));
-      M2S_CUDA(cudaStreamSynchronize(s));
-      rounds_launched += hst->round;
-      if (!hst->overflow) break;
-      if (attempts >= 6 || cap >= 0x40000000u) return M2S_ERR_LIMIT;
-      cap *= 2;
+  for (;; ++restarts) {
+    if ((st = job.alloc_lists(s))) return st;
+    if ((st = job.enqueue(s, phase_ms ? ev : nullptr))) return st;
+    if ((st = job.read_state(s, &info))) return st;
+    if (!info.overflow) break;
+    if (restarts >= 6 || job.capacity() >= 0x40000000u) {
+      set_error("grid propagation lists overflowed at the largest capacity");
+      return M2S_ERR_LIMIT;
     }
-    if (stats) {
-      stats[0] = hst->seeds;
-      stats[1] = hst->round;
-      stats[2] = hst->entries;
-      stats[3] = hst->evals;
-      stats[5] = attempts;
-      stats[7] = rounds_launched;
-    }
-  } else {
-    mark(1);
+    job.set_capacity(job.capacity() * 2);  // the rerun starts over from an empty grid
   }
-  mark(2);
-
-  // ---- sign: rays + finalize
-  RayK rk{};
-  DevBuf<uint32_t> rbits[3];
-  if (sign == M2S_SIGN_RAYCAST) {
-    for (int a = 0; a < 3; ++a) {
-      unsigned long long ncols = N / gd.n[a];
-      rk.words[a] = (uint32_t)((gd.n[a] + 31) / 32);
-      if ((st = rbits[a].alloc(ncols * rk.words[a], s))) return st;
-      M2S_CUDA(cudaMemsetAsync(rbits[a].p, 0, ncols * rk.words[a] * 4, s));
-      rk.bits[a] = rbits[a].p;
-    }
-    if (T > 0) {
-      unsigned rb = (unsigned)((T * 32ull + 255) / 256);
-      k_rays<0><<<rb, 256, 0, s>>>(g, m.tris, T, rk, state.p);
-      k_rays<1><<<rb, 256, 0, s>>>(g, m.tris, T, rk, state.p);
-      k_rays<2><<<rb, 256, 0, s>>>(g, m.tris, T, rk, state.p);
-      M2S_CUDA(cudaGetLastError());
-      launches += 3;
-    }
-    for (int a = 0; a < 3; ++a) {
-      unsigned long long ncols = N / gd.n[a];
-      k_suffix<<<blocks_for(ncols, 256), 256, 0, s>>>(rk.bits[a], ncols, rk.words[a]);
-    }
-    launches += 3;
-    mark(3);
-    k_finalize<M2S_SIGN_RAYCAST><<<blocks_for(N, 256, 148u * 32u), 256, 0, s>>>(g, snap_keys.p, rk, d_out);
-    if (stats) {
-      unsigned long long h = 0;
-      M2S_CUDA(cudaMemcpyAsync(&h, &state.p->ray_hits, 8, cudaMemcpyDeviceToHost, s));
-      M2S_CUDA(cudaStreamSynchronize(s));
-      stats[4] = h;
-    }
-  } else {
-    mark(3);
-    k_finalize<M2S_SIGN_NORMAL><<<blocks_for(N, 256, 148u * 32u), 256, 0, s>>>(g, snap_keys.p, rk, d_out);
+  if (stats) {
+    stats[0] = info.seeds;
+    stats[1] = info.rounds;
+    stats[2] = info.entries;
+    stats[3] = info.evals;
+    stats[4] = info.ray_hits;
+    stats[5] = restarts;
+    stats[6] = info.launches;
+    stats[7] = info.far_phases;
   }
-  M2S_CUDA(cudaGetLastError());
-  ++launches;
-  mark(4);
-  if (stats) stats[6] = launches;
-  if (phase_ms) {
-    M2S_CUDA(cudaEventSynchronize(ev[4]));
-    for (int i = 0; i < 4; ++i) cudaEventElapsedTime(&phase_ms[i], ev[i], ev[i + 1]);
-  }
+  if (phase_ms)
+    for (int i = 0; i < 4; ++i) M2S_CUDA(cudaEventElapsedTime(&phase_ms[i], ev[i], ev[i + 1]));
   return M2S_OK;
+}
+
+int grid_sdf_batch(const MeshView* meshes, uint32_t n, const GridDesc* gds, int sign, float* d_out, uint32_t* d_status,
+                   cudaStream_t s, uint64_t stats[kGridStats], float phase_ms[4], const GridTuning& tune) {
+  if (n == 0) return M2S_OK;
+  GridJob job;
+  int st = job.prepare(meshes, n, gds, sign, d_out, d_status, s, tune);
+  if (st) return st;
+  return run_grid_job(job, s, stats, phase_ms);
+}
+
+GridTuning g_grid_tuning;
+
+int grid_sdf(const MeshView& m, const GridDesc& gd, int sign, float* d_out, uint32_t* d_status, cudaStream_t s,
+             uint64_t stats[kGridStats], float phase_ms[4]) {
+  if (gd.cells() == 0) return M2S_OK;
+  return grid_sdf_batch(&m, 1, &gd, sign, d_out, d_status, s, stats, phase_ms, g_grid_tuning);
 }
 
 }  // namespace m2s

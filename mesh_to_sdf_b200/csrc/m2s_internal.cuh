@@ -134,14 +134,102 @@ struct GridDesc {
   float first[3];
   float size[3];
   uint64_t n[3];
-  uint64_t cells() const { return n[0] * n[1] * n[2]; }
+  // Cell count, saturated at UINT64_MAX when the product overflows.
+  uint64_t cells() const {
+    unsigned __int128 c = (unsigned __int128)n[0] * n[1];
+    if (c > UINT64_MAX) return UINT64_MAX;
+    c *= n[2];
+    return c > UINT64_MAX ? UINT64_MAX : (uint64_t)c;
+  }
 };
 
-// stats: [seed updates, rounds, states relaxed, neighbour evaluations, ray hits,
-// overflow recoveries, kernel launches, relax rounds launched].  phase_ms (may be
-// NULL) receives device time of [seeding, propagation, rays, finalize].
+// stats: [seed updates, relax rounds, states relaxed, neighbour evaluations,
+// ray hits, overflow restarts, kernel launches, far-list redistributions].
+// phase_ms (may be NULL) receives device time of [seeding, propagation, rays,
+// finalize].
 constexpr int kGridStats = 8;
 int grid_sdf(const MeshView& m, const GridDesc& g, int sign, float* d_out, uint32_t* d_status, cudaStream_t s,
              uint64_t stats[kGridStats], float phase_ms[4]);
+
+// Knobs that change speed, never results.
+struct GridTuning {
+  int blocks_per_sm = 0;             // cooperative blocks per SM (0: occupancy limit)
+  uint32_t cells_per_block = 2048;   // cooperative grid = ceil(cells / this) blocks, at least 8
+  uint32_t list_capacity = 0;        // entries per bucket list (0: derived from the cell count)
+};
+
+struct GridRunInfo {
+  bool overflow = false;
+  uint64_t seeds = 0, rounds = 0, entries = 0, evals = 0, ray_hits = 0, far_phases = 0, launches = 0;
+};
+
+// A set of (mesh, grid) pairs computed together: one cell index space (grid k
+// starts at the sum of the cells of grids 0..k-1, which is also where its
+// output starts in d_out) and one triangle array.  prepare() allocates and
+// uploads everything; enqueue() queues the whole pipeline on a stream with no
+// host synchronisation, so it can be captured into a CUDA graph; read_state()
+// waits for the stream and reports whether the bucket lists overflowed, in
+// which case the caller raises the capacity and runs enqueue() again (the
+// rerun starts from scratch, so results never depend on the capacity).
+class GridJob {
+ public:
+  GridJob();
+  ~GridJob();
+  GridJob(const GridJob&) = delete;
+  GridJob& operator=(const GridJob&) = delete;
+  int prepare(const MeshView* meshes, uint32_t n, const GridDesc* grids, int sign, float* d_out, uint32_t* d_status,
+              cudaStream_t s, const GridTuning& tune);
+  int alloc_lists(cudaStream_t s);
+  int enqueue(cudaStream_t s, cudaEvent_t* ev5);
+  int read_state(cudaStream_t s, GridRunInfo* info);
+  uint32_t capacity() const;
+  void set_capacity(uint32_t cap);
+  uint64_t cells() const;
+  uint64_t device_bytes() const;  // workspace held by the job (lists included)
+  unsigned cooperative_blocks() const;
+  unsigned max_cooperative_blocks() const;
+  void set_cooperative_blocks(unsigned blocks);  // clamped to [1, max_cooperative_blocks()]
+  int sign() const;
+  uint32_t grids() const;
+
+ private:
+  struct Impl;
+  Impl* p;
+};
+
+// Runs a job to completion (restarting with larger lists on overflow).
+int run_grid_job(GridJob& job, cudaStream_t s, uint64_t stats[kGridStats], float phase_ms[4]);
+
+// n (mesh, grid) pairs in one job; results concatenated in d_out.
+int grid_sdf_batch(const MeshView* meshes, uint32_t n, const GridDesc* grids, int sign, float* d_out,
+                   uint32_t* d_status, cudaStream_t s, uint64_t stats[kGridStats], float phase_ms[4],
+                   const GridTuning& tune);
+
+// Validates a grid description for the device path (32-bit cell indices).
+int check_grid(const GridDesc& g);
+
+// Process-wide grid knobs (m2s_set_grid_tuning).
+extern GridTuning g_grid_tuning;
+
+// ---- host API helpers (m2s_api.cu) -------------------------------------------
+
+// M2S_OK when the current device is compute capability 10.x.
+int require_device();
+// Records the counters / phase times of the last grid call of this thread.
+void record_grid_stats(const uint64_t stats[kGridStats]);
+float* grid_phase_slot();  // NULL unless profiling is on
+int status_from_bits(uint32_t bits);
+
+}  // namespace m2s
+
+// Resident mesh behind the m2s_mesh handle.
+struct m2s_mesh {
+  int device = 0;
+  int accel = 0;
+  int sign = 0;
+  m2s::DeviceMesh mesh;
+};
+
+namespace m2s {
 
 }  // namespace m2s

@@ -17,6 +17,8 @@ same bytes.  Shapes:
 """
 from __future__ import annotations
 
+import functools
+
 import numpy as np
 
 _ICO_V = None
@@ -32,8 +34,21 @@ def _icosahedron():
     return v / np.linalg.norm(v, axis=1, keepdims=True), f
 
 
+@functools.lru_cache(maxsize=8)
+def _icosphere_f64_cached(subdiv: int):
+    v, f = _icosphere_build(subdiv)
+    v.setflags(write=False)
+    f.setflags(write=False)
+    return v, f
+
+
 def icosphere_f64(subdiv: int):
     """Unit icosphere in float64: (vertices (V,3), faces (T,3) int64)."""
+    v, f = _icosphere_f64_cached(subdiv)
+    return v.copy(), f.copy()
+
+
+def _icosphere_build(subdiv: int):
     v, f = _icosahedron()
     for _ in range(subdiv):
         e = np.concatenate([f[:, [0, 1]], f[:, [1, 2]], f[:, [2, 0]]])
@@ -165,3 +180,28 @@ def mixed_points(vertices, indices, n, seed, frac_uniform=0.8, sigma=0.02, pad=0
     out = np.concatenate([u, s])
     rng = np.random.default_rng(seed + 2)
     return out[rng.permutation(n)]
+
+
+BATCH_SUBDIVS = (2, 3, 4, 5, 6)
+BATCH_EDGES = (32, 64, 96, 128, 192)
+
+
+def batch_meshes(n: int = 256, seed: int = 0, subdivs=BATCH_SUBDIVS, edges=BATCH_EDGES):
+    """The batched-grid workload: n displaced icospheres (subdivision uniform
+    over `subdivs`, so log-uniform in triangle count), each scaled by U[0.5, 2]
+    and turned by a uniform random rotation, with a cubic grid of edge drawn
+    from `edges` over its bounding box padded 10 %.  Returns a list of
+    (vertices f32 (V,3), u32 list indices, grid lo, grid hi, edge)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        s = int(rng.choice(subdivs))
+        scale = rng.uniform(0.5, 2.0)
+        rot = random_rotation(rng)
+        edge = int(rng.choice(edges))
+        u, f = icosphere_f64(s)
+        r = star_radius(u, seed * 100003 + k)
+        v = ((u * r[:, None]) @ rot.T * scale).astype(np.float32)
+        lo, hi = padded_bbox(v)
+        out.append((v, f.astype(np.uint32).reshape(-1), lo, hi, edge))
+    return out

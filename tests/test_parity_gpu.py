@@ -336,3 +336,13 @@ def test_grid_negative_and_anisotropic_sizes(orc):
     gpu, ref1, ref8, nn = grid_report(orc, v, idx, grid, S.Raycast)
     assert np.array_equal(np.signbit(gpu), np.signbit(ref1))
     assert np.all(np.abs(gpu) >= nn)
+
+
+def test_grid_coarse_mesh_far_states(orc):
+    # a coarse sphere in a fine grid: seeds lie many buckets from the surface and
+    # wait in the far list; the result keeps the same envelope as the others
+    v, idx = synth.icosphere(1)
+    grid = m2s.Grid.from_bounding_box([-1.3] * 3, [1.3] * 3, [40, 40, 40])
+    gpu, ref1, ref8, nn = grid_report(orc, v, idx, grid, S.Raycast)
+    assert m2s.last_grid_stats()["far_phases"] > 0
+    check_grid(gpu, ref1, ref8, nn, float(np.linalg.norm(grid.cell_size)), S.Raycast, "coarse")
