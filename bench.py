@@ -462,6 +462,20 @@ def batch_workload(args):
         for m, g, o in zip(meshes, grids, views):
             m.grid_device(g, S.Raycast, o, status)
 
+    def plain_by_edge():
+        """Device time of the single-grid calls, summed per grid edge."""
+        per = {}
+        for m, g, o, it in zip(meshes, grids, views, items):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            m.grid_device(g, S.Raycast, o, status)
+            b.record()
+            b.synchronize()
+            e = it[4]
+            n_, t_ = per.get(e, (0, 0.0))
+            per[e] = (n_ + 1, t_ + a.elapsed_time(b))
+        return {str(e): {"grids": n_, "ms": round(t_, 2)} for e, (n_, t_) in sorted(per.items())}
+
     def timed(fn, steps):
         ms = []
         for _ in range(steps):
@@ -476,6 +490,7 @@ def batch_workload(args):
 
     plain_pass()
     plain_ms = timed(plain_pass, max(1, min(args.steps, 3)))
+    per_edge = plain_by_edge()
     batched = torch.empty(N, dtype=torch.float32, device="cuda")
     plan = m2s.GridPlan(meshes, grids, S.Raycast, batched, status)
     blocks0 = plan.blocks
@@ -486,12 +501,16 @@ def batch_workload(args):
     plan.run()
     stats = m2s.last_grid_stats()
     batch_ms = timed(plan.run, max(3, args.steps))
-    same = bool(torch.equal(plain.view(torch.int32), batched.view(torch.int32)))
+    diff = plain.view(torch.int32) != batched.view(torch.int32)
+    ndiff = int(diff.sum().item())
+    same = ndiff == 0
+    bad_grids = [k for k in range(len(grids)) if bool(diff[int(off[k]):int(off[k + 1])].any().item())] if ndiff else []
     assert int(status.item()) == 0, int(status.item())
     line = {"workload": "c4_batch", "grids": len(grids), "cells": N, "triangles": tris,
             "plain_ms": plain_ms, "plain_cells_per_s": N / (plain_ms / 1e3),
             "batched_ms": batch_ms, "batched_cells_per_s": N / (batch_ms / 1e3),
-            "speedup": plain_ms / batch_ms, "bit_identical": same,
+            "speedup": plain_ms / batch_ms, "bit_identical": same, "cells_differing": ndiff,
+            "grids_differing": bad_grids[:16], "waves": plan.waves, "plain_ms_by_edge": per_edge,
             "blocks_default": blocks0, "blocks_autotuned": chosen, "autotune_s": tune_s,
             "plan_device_gb": plan.device_bytes / 1e9, "grid_stats": stats}
     plan.close()

@@ -150,14 +150,16 @@ int m2s_grid_plan_create(const m2s_mesh* const* meshes, uint32_t n_grids,
                          uint32_t* d_status, void* stream, m2s_grid_plan** out_plan);
 /* Replays the plan on `stream`; returns once d_out is written. */
 int m2s_grid_plan_run(m2s_grid_plan* plan, void* stream);
-/* Times the plan at several cooperative grid sizes (results are identical at
- * every size), keeps the fastest for this plan and for later plans of the
- * same class (device, sign, batch or single, log2 of the cell count).
- * *out_blocks (may be NULL) receives the chosen block count. */
+/* Times the plan's waves at several cooperative grid sizes (results are
+ * identical at every size) and keeps the fastest per class of wave (device,
+ * sign, one grid or several, log2 of the cell count), for this plan and for
+ * later plans.  *out_blocks (may be NULL) receives the first wave's choice. */
 int m2s_grid_plan_autotune(m2s_grid_plan* plan, void* stream, uint32_t* out_blocks);
 uint64_t m2s_grid_plan_cells(const m2s_grid_plan* plan);
 uint64_t m2s_grid_plan_device_bytes(const m2s_grid_plan* plan);
 uint32_t m2s_grid_plan_blocks(const m2s_grid_plan* plan);
+/* Number of jobs ("waves") the plan's batch was split into (see below). */
+uint32_t m2s_grid_plan_waves(const m2s_grid_plan* plan);
 void m2s_grid_plan_free(m2s_grid_plan* plan);
 /* Forgets every autotuned choice. */
 void m2s_clear_grid_autotune(void);
@@ -165,8 +167,10 @@ void m2s_clear_grid_autotune(void);
 /* Process-wide grid knobs; they change speed, never results.  blocks_per_sm:
  * cooperative propagation blocks per SM (0 = occupancy limit);
  * cells_per_block: the propagation launch uses ceil(cells / this) blocks, at
- * least 8 (0 = 2048). */
-void m2s_set_grid_tuning(int blocks_per_sm, uint32_t cells_per_block);
+ * least 8 (0 = 2048); wave_cells: a batch runs as jobs of at most this many
+ * cells, largest grids first (a larger grid alone), so each job's working set
+ * stays near L2 size (0 = 4M). */
+void m2s_set_grid_tuning(int blocks_per_sm, uint32_t cells_per_block, uint64_t wave_cells);
 
 /* generate_sdf with AccelerationMethod::None for callers that cannot allocate
  * device memory.  No counterpart in the reference: the crate allocates freely.

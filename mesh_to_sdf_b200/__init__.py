@@ -452,6 +452,10 @@ class GridPlan:
     def blocks(self):
         return int(_lib.lib().m2s_grid_plan_blocks(self._h))
 
+    @property
+    def waves(self):
+        return int(_lib.lib().m2s_grid_plan_waves(self._h))
+
     def close(self):
         if self._h and self._h.value:
             _lib.lib().m2s_grid_plan_free(self._h)
@@ -464,9 +468,10 @@ class GridPlan:
             pass
 
 
-def set_grid_tuning(blocks_per_sm: int = 0, cells_per_block: int = 2048):
-    """Process-wide grid propagation knobs (speed only)."""
-    _lib.lib().m2s_set_grid_tuning(int(blocks_per_sm), int(cells_per_block))
+def set_grid_tuning(blocks_per_sm: int = 0, cells_per_block: int = 2048, wave_cells: int = 4 << 20):
+    """Process-wide grid propagation knobs (speed only): cooperative blocks per
+    SM, cells per cooperative block, and the most cells a batch job holds."""
+    _lib.lib().m2s_set_grid_tuning(int(blocks_per_sm), int(cells_per_block), int(wave_cells))
 
 
 def clear_grid_autotune():

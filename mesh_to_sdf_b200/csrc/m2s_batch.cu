@@ -4,26 +4,34 @@
 // one persistent propagation launch instead of paying its fixed cost —
 // rounds that each end in a grid-wide barrier — once per grid.
 //
-// A batch is one GridJob over all its grids.  Every grid's states are relaxed
-// in the rounds of their own distance buckets whatever else is in the job, so
-// each grid's output is bit-identical to computing it alone; the batch takes
-// as many rounds as its slowest grid.
+// A job (GridJob) computes several grids in one set of launches.  Every
+// grid's states are relaxed in the rounds of their own distance buckets
+// whatever else is in the job, so each grid's output is bit-identical to
+// computing it alone; a job takes as many rounds as its slowest grid.
 //
-// A plan captures a job's whole pipeline (memsets, seeding, collection, the
-// cooperative propagation kernel, rays, finalisation) into a CUDA graph once
-// and replays it.  Its workspace is allocated on a stream the plan owns and
-// kept until the plan is freed.
+// A batch runs as waves: jobs of at most wave_cells cells (4M by default; a
+// larger grid alone), packed largest grid first.  A job's keys (16 bytes per
+// cell) then stay near the size of L2, where the random neighbour accesses of
+// propagation hit; one job over every grid of a large batch would send them
+// all to HBM.  Small grids share a job, so their short rounds share barriers.
+//
+// A plan captures every wave's whole pipeline (memsets, seeding, collection,
+// the cooperative propagation kernel, rays, finalisation) into one CUDA graph
+// once and replays it.  Its workspace is allocated on a stream the plan owns
+// and kept until the plan is freed.
 //
 // The autotuner times a plan at several cooperative grid sizes — the one knob
 // that moves propagation time most: more blocks relax big buckets faster, but
 // every round ends in a barrier whose cost grows with the block count — and
-// keeps the fastest.  The choice is cached per (device, sign, batch or not,
-// log2 of the cell count) and reused by later plans of that class.
+// keeps the fastest, timing one wave per class of waves (device, sign, one
+// grid or several, log2 of the cell count).  The choice is cached per class
+// and reused by later plans.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <vector>
 
@@ -84,7 +92,7 @@ uint64_t tune_key(const GridJob& job) {
 struct m2s_grid_plan {
   int device = 0;
   cudaStream_t own = nullptr;  // allocation and capture stream
-  GridJob job;
+  std::vector<std::unique_ptr<GridJob>> jobs;  // one per wave
   cudaGraphExec_t exec = nullptr;
   uint64_t stats[kGridStats] = {};
   uint32_t restarts = 0;
@@ -93,11 +101,13 @@ struct m2s_grid_plan {
     if (exec) cudaGraphExecDestroy(exec);
     exec = nullptr;
   }
-  // Records the job's pipeline into a fresh executable graph.
+  // Records every job's pipeline, one after the other, into one executable graph.
   int capture() {
     drop_graph();
     M2S_CUDA(cudaStreamBeginCapture(own, cudaStreamCaptureModeThreadLocal));
-    const int st = job.enqueue(own, nullptr);
+    int st = M2S_OK;
+    for (auto& j : jobs)
+      if ((st = j->enqueue(own, nullptr))) break;
     cudaGraph_t g = nullptr;
     const cudaError_t e = cudaStreamEndCapture(own, &g);
     if (st) {
@@ -113,35 +123,43 @@ struct m2s_grid_plan {
     }
     return M2S_OK;
   }
-  // Launches the graph; on a list overflow doubles the lists, re-captures and
-  // launches again (the job starts from scratch, so results are unaffected).
+  // Launches the graph; if a job's lists overflowed, doubles them, re-captures
+  // and launches again (every job starts from scratch, so results are unaffected).
   int run(cudaStream_t s) {
     int st;
-    GridRunInfo info;
     for (uint32_t attempt = 0;; ++attempt) {
       if (!exec && (st = capture())) return st;
       M2S_CUDA(cudaGraphLaunch(exec, s));
-      if ((st = job.read_state(s, &info))) return st;
-      if (!info.overflow) break;
-      if (attempt >= 6 || job.capacity() >= 0x40000000u) {
-        set_error("grid propagation lists overflowed at the largest capacity");
-        return M2S_ERR_LIMIT;
+      uint64_t sum[kGridStats] = {};
+      bool again = false;
+      for (auto& j : jobs) {
+        GridRunInfo info;
+        if ((st = j->read_state(s, &info))) return st;
+        sum[0] += info.seeds;
+        sum[1] += info.rounds;
+        sum[2] += info.entries;
+        sum[3] += info.evals;
+        sum[4] += info.ray_hits;
+        sum[6] += info.launches;
+        sum[7] += info.far_phases;
+        if (!info.overflow) continue;
+        if (attempt >= 6 || j->capacity() >= 0x40000000u) {
+          set_error("grid propagation lists overflowed at the largest capacity");
+          return M2S_ERR_LIMIT;
+        }
+        j->set_capacity(j->capacity() * 2);
+        if ((st = j->alloc_lists(own))) return st;
+        again = true;
       }
-      drop_graph();
-      job.set_capacity(job.capacity() * 2);
-      if ((st = job.alloc_lists(own))) return st;
+      if (!again) {
+        sum[5] = restarts;
+        for (int i = 0; i < kGridStats; ++i) stats[i] = sum[i];
+        return M2S_OK;
+      }
       M2S_CUDA(cudaStreamSynchronize(own));
+      drop_graph();
       ++restarts;
     }
-    stats[0] = info.seeds;
-    stats[1] = info.rounds;
-    stats[2] = info.entries;
-    stats[3] = info.evals;
-    stats[4] = info.ray_hits;
-    stats[5] = restarts;
-    stats[6] = info.launches;
-    stats[7] = info.far_phases;
-    return M2S_OK;
   }
   ~m2s_grid_plan() {
     drop_graph();
@@ -204,13 +222,14 @@ int m2s_grid_plan_create(const m2s_mesh* const* meshes, uint32_t n_grids, const 
     cudaStreamDestroy(own);
     return code;
   };
-  if ((st = P->job.prepare(views.data(), n_grids, grids.data(), sign, d_out, d_status, P->own, g_grid_tuning)))
+  if ((st = prepare_waves(views.data(), n_grids, grids.data(), sign, d_out, d_status, P->own, g_grid_tuning,
+                          &P->jobs)))
     return fail(st);
-  if ((st = P->job.alloc_lists(P->own))) return fail(st);
-  {
+  for (auto& j : P->jobs) {
+    if ((st = j->alloc_lists(P->own))) return fail(st);
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    auto it = g_tuned_blocks.find(tune_key(P->job));
-    if (it != g_tuned_blocks.end()) P->job.set_cooperative_blocks(it->second);
+    auto it = g_tuned_blocks.find(tune_key(*j));
+    if (it != g_tuned_blocks.end()) j->set_cooperative_blocks(it->second);
   }
   e = cudaStreamSynchronize(P->own);
   if (e != cudaSuccess) return fail(cuda_fail(e, "cudaStreamSynchronize"));
@@ -233,15 +252,10 @@ int m2s_grid_plan_autotune(m2s_grid_plan* plan, void* stream, uint32_t* out_bloc
   int st;
   if ((st = require_device())) return st;
   cudaStream_t s = (cudaStream_t)stream;
-  GridJob& job = plan->job;
-  const unsigned most = job.max_cooperative_blocks();
+  if ((st = plan->run(s))) return st;  // settles every job's list capacity
   int dev = 0, sms = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  std::vector<unsigned> cand = {job.cooperative_blocks(), 16, 32, 64, (unsigned)sms / 2, (unsigned)sms,
-                                2u * sms, 3u * sms, most};
-  std::sort(cand.begin(), cand.end());
-  cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
   cudaEvent_t e0, e1;
   M2S_CUDA(cudaEventCreate(&e0));
   M2S_CUDA(cudaEventCreate(&e1));
@@ -252,41 +266,65 @@ int m2s_grid_plan_autotune(m2s_grid_plan* plan, void* stream, uint32_t* out_bloc
       cudaEventDestroy(b);
     }
   } evf{e0, e1};
-  float best_ms = INFINITY;
-  unsigned best = job.cooperative_blocks();
-  for (unsigned c : cand) {
-    if (c < 1 || c > most) continue;
-    job.set_cooperative_blocks(c);
-    plan->drop_graph();
-    if ((st = plan->run(s))) return st;  // warm-up (and settles the list capacity)
-    float ms = 0.0f;
-    for (int rep = 0; rep < 2; ++rep) {
+  // One job per class is timed (launched directly, not from the graph); the
+  // choice applies to every job of the class and to later plans.
+  std::map<uint64_t, unsigned> chosen;
+  for (auto& jp : plan->jobs) {
+    GridJob& job = *jp;
+    const uint64_t key = tune_key(job);
+    if (chosen.count(key)) continue;
+    const unsigned most = job.max_cooperative_blocks();
+    std::vector<unsigned> cand = {job.cooperative_blocks(), 16, 32, 64, (unsigned)sms / 2, (unsigned)sms,
+                                  2u * sms, 3u * sms, most};
+    std::sort(cand.begin(), cand.end());
+    cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+    float best_ms = INFINITY;
+    unsigned best = job.cooperative_blocks();
+    for (unsigned c : cand) {
+      if (c < 1 || c > most) continue;
+      job.set_cooperative_blocks(c);
+      if ((st = job.enqueue(s, nullptr))) return st;  // warm-up
       M2S_CUDA(cudaEventRecord(e0, s));
-      M2S_CUDA(cudaGraphLaunch(plan->exec, s));
+      for (int rep = 0; rep < 2; ++rep)
+        if ((st = job.enqueue(s, nullptr))) return st;
       M2S_CUDA(cudaEventRecord(e1, s));
       M2S_CUDA(cudaEventSynchronize(e1));
-      float t = 0.0f;
-      M2S_CUDA(cudaEventElapsedTime(&t, e0, e1));
-      ms += t;
+      float ms = 0.0f;
+      M2S_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = c;
+      }
     }
-    if (ms < best_ms) {
-      best_ms = ms;
-      best = c;
-    }
+    chosen[key] = best;
   }
-  job.set_cooperative_blocks(best);
-  if ((st = plan->capture())) return st;
+  for (auto& jp : plan->jobs) jp->set_cooperative_blocks(chosen[tune_key(*jp)]);
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tuned_blocks[tune_key(job)] = best;
+    for (auto& kv : chosen) g_tuned_blocks[kv.first] = kv.second;
   }
-  if (out_blocks) *out_blocks = best;
+  plan->drop_graph();
+  if ((st = plan->run(s))) return st;  // re-captures with the chosen shapes
+  if (out_blocks) *out_blocks = plan->jobs.front()->cooperative_blocks();
   return M2S_OK;
 }
 
-uint64_t m2s_grid_plan_cells(const m2s_grid_plan* plan) { return plan ? plan->job.cells() : 0; }
-uint64_t m2s_grid_plan_device_bytes(const m2s_grid_plan* plan) { return plan ? plan->job.device_bytes() : 0; }
-uint32_t m2s_grid_plan_blocks(const m2s_grid_plan* plan) { return plan ? plan->job.cooperative_blocks() : 0; }
+uint64_t m2s_grid_plan_cells(const m2s_grid_plan* plan) {
+  uint64_t n = 0;
+  if (plan)
+    for (auto& j : plan->jobs) n += j->cells();
+  return n;
+}
+uint64_t m2s_grid_plan_device_bytes(const m2s_grid_plan* plan) {
+  uint64_t n = 0;
+  if (plan)
+    for (auto& j : plan->jobs) n += j->device_bytes();
+  return n;
+}
+uint32_t m2s_grid_plan_blocks(const m2s_grid_plan* plan) {
+  return plan && !plan->jobs.empty() ? plan->jobs.front()->cooperative_blocks() : 0;
+}
+uint32_t m2s_grid_plan_waves(const m2s_grid_plan* plan) { return plan ? (uint32_t)plan->jobs.size() : 0; }
 
 void m2s_grid_plan_free(m2s_grid_plan* plan) {
   if (!plan) return;
@@ -300,9 +338,10 @@ void m2s_grid_plan_free(m2s_grid_plan* plan) {
   cudaSetDevice(prev);
 }
 
-void m2s_set_grid_tuning(int blocks_per_sm, uint32_t cells_per_block) {
+void m2s_set_grid_tuning(int blocks_per_sm, uint32_t cells_per_block, uint64_t wave_cells) {
   g_grid_tuning.blocks_per_sm = blocks_per_sm > 0 ? blocks_per_sm : 0;
   g_grid_tuning.cells_per_block = cells_per_block ? cells_per_block : 2048;
+  g_grid_tuning.wave_cells = wave_cells ? wave_cells : (4ull << 20);
 }
 
 void m2s_clear_grid_autotune(void) {

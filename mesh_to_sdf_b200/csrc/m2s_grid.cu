@@ -41,6 +41,7 @@
 #include <climits>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <vector>
 
 #include "m2s_internal.cuh"
@@ -91,6 +92,7 @@ struct GridK {
   uint32_t words[3];  // 32-bit words per ray column, per axis
   unsigned long long bits_off[3];  // its first ray word, per axis
   unsigned long long col_off[3];   // its first ray column, per axis
+  unsigned long long out_off;      // its first value in the caller's output
 };
 
 // Kernel view of a job.
@@ -308,18 +310,22 @@ __global__ void k_seed(const __grid_constant__ GridSet gs, const TriRec* __restr
   if (lane == 0 && updates) atomicAdd(&st->seeds, (unsigned long long)updates);
 }
 
-// Distance bucket of a state, in its own grid's cell units.  Buckets are a
-// quarter cell wide for the first kLinearBuckets (8 cells) and widen in
-// proportion to the distance beyond, so the far field, where many triangles
-// are nearly equidistant, takes few rounds.  Finite distances stay below a few
-// thousand; a NaN distance (already an error) lands in bucket 0.
+// Distance bucket of a state, in its own grid's cell units: u = |d| / (a
+// quarter of the smallest cell size).  Buckets are one unit wide up to u = 32
+// (8 cells) and beyond grow with the distance — kLogBuckets per doubling of u,
+// from the piecewise-linear log2 that the f32 bit pattern gives (exponent,
+// then mantissa) — so the far field, where many triangles are nearly
+// equidistant, takes few rounds.  Everything after the one rounded product is
+// integer arithmetic, so every kernel files a state under the same bucket.
 constexpr float kLinearBuckets = 32.0f;
+constexpr uint64_t kLogBuckets = 22;
 __device__ __forceinline__ uint32_t bucket_of(float inv_delta, float d) {
-  float u = fabsf(d) * inv_delta;
-  if (u > kLinearBuckets) u = kLinearBuckets * (1.0f + logf(u / kLinearBuckets));
-  if (isnan(u)) return 0;
-  if (!(u < 2147483520.0f)) return 0x7FFFFF00u;
-  return (uint32_t)u;  // floor, u >= 0
+  const float u = __fmul_rn(fabsf(d), inv_delta);
+  if (isnan(u)) return 0;  // a NaN distance is already an error
+  if (u <= kLinearBuckets) return (uint32_t)u;  // floor, u >= 0
+  const uint32_t b = __float_as_uint(u);   // u > 32: exponent >= 5; +inf has exponent 128
+  const uint64_t lin = ((uint64_t)((b >> 23) - 127 - 5) << 23) | (b & 0x7FFFFFu);
+  return 32u + (uint32_t)((kLogBuckets * lin) >> 23);
 }
 
 __global__ void k_state_init(PropState* st) {
@@ -494,7 +500,7 @@ __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ GridS
                                                    uint32_t* status) {
   __shared__ Sched sh;
   __shared__ uint32_t s_touch[kTouchStage];
-  __shared__ uint32_t s_ntouch, s_touch_base;
+  __shared__ uint32_t s_ntouch, s_nloc, s_touch_base;
   const unsigned int nblocks = gridDim.x;
   const int lane = threadIdx.x & 31;
   const bool lead_block = blockIdx.x == 0;
@@ -622,15 +628,20 @@ __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ GridS
         }
       }
     }
-    // flush this block's staged touched cells with one global atomic
+    // flush this block's staged touched cells with one global atomic.  Thread
+    // 0 alone reads and resets the stage count and publishes it: a thread that
+    // read s_ntouch after the reset would skip its share of the stage and leave
+    // unwritten words in the touched list.
     __syncthreads();
     {
-      const uint32_t nloc = min(s_ntouch, (uint32_t)kTouchStage);
       if (threadIdx.x == 0) {
-        s_touch_base = nloc ? atomicAdd(&st->touched2[parity], nloc) : 0;
+        const uint32_t nl = min(s_ntouch, (uint32_t)kTouchStage);
+        s_nloc = nl;
+        s_touch_base = nl ? atomicAdd(&st->touched2[parity], nl) : 0;
         s_ntouch = 0;
       }
       __syncthreads();
+      const uint32_t nloc = s_nloc;
       for (uint32_t i = threadIdx.x; i < nloc; i += blockDim.x) {
         const uint32_t pos = s_touch_base + i;
         if (pos < cap) touched_list[pos] = s_touch[i];
@@ -780,8 +791,11 @@ __global__ void k_finalize(const __grid_constant__ GridSet gs, const unsigned lo
       uint32_t py = (bits[g.bits_off[1] + column_of(g, 1, x, y, z) * g.words[1] + (y >> 5)] >> (y & 31)) & 1u;
       uint32_t pz = (bits[g.bits_off[2] + column_of(g, 2, x, y, z) * g.words[2] + (z >> 5)] >> (z & 31)) & 1u;
       if (px + py + pz >= 2) d = -d;
+      out[g.out_off + ((uint32_t)i - g.cell_off)] = d;
+    } else {
+      const GridK& g = MULTI ? gs.table[sc.at(gs.cell_off, gs.ngrids, (uint32_t)i)] : gs.g0;
+      out[g.out_off + ((uint32_t)i - g.cell_off)] = d;
     }
-    out[i] = d;
   }
 }
 
@@ -864,7 +878,7 @@ int check_grid(const GridDesc& g) {
 }
 
 int GridJob::prepare(const MeshView* meshes, uint32_t n, const GridDesc* gds, int sign, float* d_out,
-                     uint32_t* d_status, cudaStream_t s, const GridTuning& tune) {
+                     uint32_t* d_status, cudaStream_t s, const GridTuning& tune, const uint64_t* out_offsets) {
   Impl& J = *p;
   if (n == 0) return M2S_ERR_INVALID_ARGUMENT;
   J.sign = sign;
@@ -891,6 +905,7 @@ int GridJob::prepare(const MeshView* meshes, uint32_t n, const GridDesc* gds, in
     if (cells + nk >= 0xFFFFFFFFull) return M2S_ERR_INVALID_ARGUMENT;  // 32-bit cell indices across the job
     g.ncell = (uint32_t)nk;
     g.cell_off = (uint32_t)cells;
+    g.out_off = out_offsets ? out_offsets[k] : cells;
     h_cell_off[k] = (uint32_t)cells;
     cells += nk;
     g.div_z = make_fastdiv((uint32_t)g.n[2]);
@@ -1137,13 +1152,92 @@ int run_grid_job(GridJob& job, cudaStream_t s, uint64_t stats[kGridStats], float
   return M2S_OK;
 }
 
+std::vector<std::vector<uint32_t>> plan_waves(const GridDesc* gds, uint32_t n, uint64_t wave_cells) {
+  std::vector<uint32_t> order(n);
+  for (uint32_t k = 0; k < n; ++k) order[k] = k;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](uint32_t a, uint32_t b) { return gds[a].cells() > gds[b].cells(); });
+  std::vector<std::vector<uint32_t>> waves;
+  std::vector<uint64_t> fill;
+  for (uint32_t k : order) {  // first fit, largest grids first
+    const uint64_t c = gds[k].cells();
+    size_t w = 0;
+    while (w < waves.size() && fill[w] + c > wave_cells) ++w;
+    if (w == waves.size()) {
+      waves.emplace_back();
+      fill.push_back(0);
+    }
+    waves[w].push_back(k);
+    fill[w] += c;
+  }
+  for (auto& w : waves) std::sort(w.begin(), w.end());  // keep triangle/grid order inside a wave
+  return waves;
+}
+
+int prepare_waves(const MeshView* meshes, uint32_t n, const GridDesc* gds, int sign, float* d_out, uint32_t* d_status,
+                  cudaStream_t s, const GridTuning& tune, std::vector<std::unique_ptr<GridJob>>* jobs) {
+  std::vector<uint64_t> out_off(n);
+  uint64_t acc = 0;
+  for (uint32_t k = 0; k < n; ++k) {
+    out_off[k] = acc;
+    acc += gds[k].cells();
+  }
+  const uint64_t wave = tune.wave_cells ? tune.wave_cells : ~0ull;
+  for (const auto& w : plan_waves(gds, n, wave)) {
+    std::vector<MeshView> m;
+    std::vector<GridDesc> g;
+    std::vector<uint64_t> o;
+    for (uint32_t k : w) {
+      m.push_back(meshes[k]);
+      g.push_back(gds[k]);
+      o.push_back(out_off[k]);
+    }
+    jobs->emplace_back(new GridJob());
+    int st = jobs->back()->prepare(m.data(), (uint32_t)w.size(), g.data(), sign, d_out, d_status, s, tune, o.data());
+    if (st) return st;
+  }
+  return M2S_OK;
+}
+
 int grid_sdf_batch(const MeshView* meshes, uint32_t n, const GridDesc* gds, int sign, float* d_out, uint32_t* d_status,
                    cudaStream_t s, uint64_t stats[kGridStats], float phase_ms[4], const GridTuning& tune) {
   if (n == 0) return M2S_OK;
-  GridJob job;
-  int st = job.prepare(meshes, n, gds, sign, d_out, d_status, s, tune);
-  if (st) return st;
-  return run_grid_job(job, s, stats, phase_ms);
+  for (uint32_t k = 0; k < n; ++k) {
+    int st = check_grid(gds[k]);
+    if (st) return st;
+  }
+  std::vector<uint64_t> out_off(n);
+  uint64_t acc = 0;
+  for (uint32_t k = 0; k < n; ++k) {
+    out_off[k] = acc;
+    acc += gds[k].cells();
+  }
+  uint64_t total[kGridStats] = {};
+  float ms[4] = {0, 0, 0, 0};
+  // One job at a time, so only one workspace is alive.
+  for (const auto& w : plan_waves(gds, n, tune.wave_cells ? tune.wave_cells : ~0ull)) {
+    std::vector<MeshView> m;
+    std::vector<GridDesc> g;
+    std::vector<uint64_t> o;
+    for (uint32_t k : w) {
+      m.push_back(meshes[k]);
+      g.push_back(gds[k]);
+      o.push_back(out_off[k]);
+    }
+    GridJob job;
+    int st = job.prepare(m.data(), (uint32_t)w.size(), g.data(), sign, d_out, d_status, s, tune, o.data());
+    if (st) return st;
+    uint64_t one[kGridStats] = {};
+    float pm[4] = {0, 0, 0, 0};
+    if ((st = run_grid_job(job, s, one, phase_ms ? pm : nullptr))) return st;
+    for (int i = 0; i < kGridStats; ++i) total[i] += one[i];
+    for (int i = 0; i < 4; ++i) ms[i] += pm[i];
+  }
+  if (stats)
+    for (int i = 0; i < kGridStats; ++i) stats[i] = total[i];
+  if (phase_ms)
+    for (int i = 0; i < 4; ++i) phase_ms[i] = ms[i];
+  return M2S_OK;
 }
 
 GridTuning g_grid_tuning;

@@ -4,7 +4,9 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
 #include <string>
+#include <vector>
 
 #include "../../include/m2s.h"
 #include "m2s_geo.cuh"
@@ -156,6 +158,9 @@ struct GridTuning {
   int blocks_per_sm = 0;             // cooperative blocks per SM (0: occupancy limit)
   uint32_t cells_per_block = 2048;   // cooperative grid = ceil(cells / this) blocks, at least 8
   uint32_t list_capacity = 0;        // entries per bucket list (0: derived from the cell count)
+  // A batch runs as jobs ("waves") of at most this many cells each (a larger
+  // grid alone), so a job's 16 bytes of keys per cell stay near L2 size.
+  uint64_t wave_cells = 4ull << 20;
 };
 
 struct GridRunInfo {
@@ -177,8 +182,9 @@ class GridJob {
   ~GridJob();
   GridJob(const GridJob&) = delete;
   GridJob& operator=(const GridJob&) = delete;
+  // out_offsets[k] (NULL: back to back from 0) is where grid k's values start in d_out.
   int prepare(const MeshView* meshes, uint32_t n, const GridDesc* grids, int sign, float* d_out, uint32_t* d_status,
-              cudaStream_t s, const GridTuning& tune);
+              cudaStream_t s, const GridTuning& tune, const uint64_t* out_offsets = nullptr);
   int alloc_lists(cudaStream_t s);
   int enqueue(cudaStream_t s, cudaEvent_t* ev5);
   int read_state(cudaStream_t s, GridRunInfo* info);
@@ -200,7 +206,17 @@ class GridJob {
 // Runs a job to completion (restarting with larger lists on overflow).
 int run_grid_job(GridJob& job, cudaStream_t s, uint64_t stats[kGridStats], float phase_ms[4]);
 
-// n (mesh, grid) pairs in one job; results concatenated in d_out.
+// Waves of a batch: grid indices per job, largest grids first, first fit into
+// jobs of at most wave_cells cells (a larger grid alone).
+std::vector<std::vector<uint32_t>> plan_waves(const GridDesc* grids, uint32_t n, uint64_t wave_cells);
+
+// One prepared job per wave of a batch (outputs back to back in d_out, in the
+// order of `grids`).
+int prepare_waves(const MeshView* meshes, uint32_t n, const GridDesc* grids, int sign, float* d_out,
+                  uint32_t* d_status, cudaStream_t s, const GridTuning& tune,
+                  std::vector<std::unique_ptr<GridJob>>* jobs);
+
+// n (mesh, grid) pairs, wave by wave; results back to back in d_out.
 int grid_sdf_batch(const MeshView* meshes, uint32_t n, const GridDesc* grids, int sign, float* d_out,
                    uint32_t* d_status, cudaStream_t s, uint64_t stats[kGridStats], float phase_ms[4],
                    const GridTuning& tune);

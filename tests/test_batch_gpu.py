@@ -100,8 +100,11 @@ def test_plan_replays_and_autotune_keep_results():
     ref, off, _ = _batch(meshes, grids, sign)
     out = torch.full((int(off[-1]),), float("nan"), dtype=torch.float32, device="cuda")
     st = torch.zeros(1, dtype=torch.int32, device="cuda")
+    m2s.set_grid_tuning(wave_cells=30000)  # several waves in one graph
     plan = m2s.GridPlan(meshes, grids, sign, out, st)
+    m2s.set_grid_tuning()
     try:
+        assert plan.waves > 1
         assert plan.cells == int(off[-1])
         assert plan.device_bytes > 0
         for _ in range(3):
@@ -126,12 +129,14 @@ def test_launch_shape_never_changes_results():
     meshes, grids = _workload(sign, seed=7)
     ref, _, _ = _batch(meshes, grids, sign)
     try:
-        for bps, cpb in [(1, 2048), (0, 64), (2, 1 << 20)]:
-            m2s.set_grid_tuning(bps, cpb)
+        # blocks per SM, cells per block, and wave size (1 cell: every grid in
+        # a job of its own; 1 << 30: the whole batch in one job)
+        for bps, cpb, wave in [(1, 2048, 4 << 20), (0, 64, 1), (2, 1 << 20, 1 << 30), (0, 2048, 20000)]:
+            m2s.set_grid_tuning(bps, cpb, wave)
             got, _, _ = _batch(meshes, grids, sign)
-            assert np.array_equal(bits(got), bits(ref)), (bps, cpb)
+            assert np.array_equal(bits(got), bits(ref)), (bps, cpb, wave)
     finally:
-        m2s.set_grid_tuning(0, 2048)
+        m2s.set_grid_tuning()
 
 
 def test_batch_with_empty_mesh():
