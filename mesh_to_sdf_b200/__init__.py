@@ -277,12 +277,12 @@ def generate_grid_sdf(vertices, indices: Topology, grid: Grid, sign_method: Sign
 
 
 GRID_STATS = ("seed_updates", "rounds", "states_relaxed", "neighbour_evals", "ray_hits", "restarts",
-              "kernel_launches", "far_phases")
+              "kernel_launches", "far_phases", "same_triangle_proposals", "max_list")
 
 
 def last_grid_stats():
     """Counters of the last grid call on this thread (names in GRID_STATS)."""
-    a = np.zeros(8, np.uint64)
+    a = np.zeros(len(GRID_STATS), np.uint64)
     _lib.lib().m2s_last_grid_stats(_vp(a))
     return dict(zip(GRID_STATS, (int(x) for x in a)))
 

@@ -223,7 +223,7 @@ int m2s_device_available(void) { return require_device() == M2S_OK ? 1 : 0; }
 void m2s_set_query_budget(uint32_t node_visits) { g_query_budget = node_visits; }
 uint32_t m2s_query_budget(void) { return g_query_budget; }
 
-int m2s_last_grid_stats(uint64_t out[8]) {
+int m2s_last_grid_stats(uint64_t out[10]) {
   if (!out) return M2S_ERR_INVALID_ARGUMENT;
   for (int i = 0; i < kGridStats; ++i) out[i] = t_grid_stats[i];
   return M2S_OK;

@@ -163,7 +163,8 @@ struct PropState {
   uint32_t overflow;
   uint32_t round;
   uint32_t far_phases;
-  unsigned long long entries, evals, seeds, ray_hits;
+  uint32_t max_list;      // largest bucket list relaxed in one round
+  unsigned long long entries, evals, seeds, ray_hits, skips;
 };
 
 __device__ __forceinline__ P3 center(const GridK& g, int x, int y, int z) {
@@ -477,7 +478,10 @@ __device__ __forceinline__ int next_step(Sched& sh, PropState* st, bool leader) 
       sh.slot[0] = consumed;  // becomes the list of states re-queued at bucket b
       sh.cur = s0;
       sh.round += 1;
-      if (leader) st->count[consumed] = 0;
+      if (leader) {
+        st->count[consumed] = 0;
+        st->max_list = max(st->max_list, *(volatile uint32_t*)&st->count[s0]);
+      }
       return kRelax;
     }
     if (sh.b + 1 >= sh.B + kRing) break;  // window exhausted
@@ -514,7 +518,7 @@ __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ GridS
     sh.round = 0;
   }
   bool nan = false;
-  unsigned long long evals = 0;
+  unsigned long long evals = 0, skips = 0;
   uint32_t far_phases = 0;
   bool aborted = false;
   for (uint32_t it = 0;; ++it) {
@@ -604,6 +608,9 @@ __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ GridS
         if (X < 0 || Y < 0 || Z < 0 || X >= g.n[0] || Y >= g.n[1] || Z >= g.n[2]) continue;
         const uint32_t j = g.cell_off + local_index(g, X, Y, Z);
         const unsigned long long snap = __ldcg(&snap_keys[j]);
+        // Counted only: such a proposal recomputes the distance the cell holds
+        // and cannot win, but skipping it leaves its lanes idle in the warp.
+        if (key_tri(snap) == tri) ++skips;
         const TriRec r = tris[tri];
         const float d = cell_distance<SIGN>(center(g, X, Y, Z), p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
         ++evals;
@@ -678,6 +685,8 @@ __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ GridS
   if (nan) atomicOr(status, bit(M2S_ERR_NAN_DISTANCE));
   for (int o = 16; o; o >>= 1) evals += __shfl_xor_sync(0xFFFFFFFFu, evals, o);
   if (lane == 0 && evals) atomicAdd(&st->evals, evals);
+  for (int o = 16; o; o >>= 1) skips += __shfl_xor_sync(0xFFFFFFFFu, skips, o);
+  if (lane == 0 && skips) atomicAdd(&st->skips, skips);
   if (aborted && lead_block && threadIdx.x == 0) atomicOr(status, bit(M2S_ERR_LIMIT));
   if (lead_block && threadIdx.x == 0) {
     st->round = sh.round;
@@ -1108,6 +1117,8 @@ int GridJob::read_state(cudaStream_t s, GridRunInfo* info) {
   info->evals = h->evals;
   info->ray_hits = h->ray_hits;
   info->far_phases = h->far_phases;
+  info->skips = h->skips;
+  info->max_list = h->max_list;
   info->launches = J.launches;
   return M2S_OK;
 }
@@ -1146,6 +1157,8 @@ int run_grid_job(GridJob& job, cudaStream_t s, uint64_t stats[kGridStats], float
     stats[5] = restarts;
     stats[6] = info.launches;
     stats[7] = info.far_phases;
+    stats[8] = info.skips;
+    stats[9] = info.max_list;
   }
   if (phase_ms)
     for (int i = 0; i < 4; ++i) M2S_CUDA(cudaEventElapsedTime(&phase_ms[i], ev[i], ev[i + 1]));
@@ -1230,7 +1243,7 @@ int grid_sdf_batch(const MeshView* meshes, uint32_t n, const GridDesc* gds, int 
     uint64_t one[kGridStats] = {};
     float pm[4] = {0, 0, 0, 0};
     if ((st = run_grid_job(job, s, one, phase_ms ? pm : nullptr))) return st;
-    for (int i = 0; i < kGridStats; ++i) total[i] += one[i];
+    for (int i = 0; i < kGridStats; ++i) total[i] = i == 9 ? std::max(total[i], one[i]) : total[i] + one[i];
     for (int i = 0; i < 4; ++i) ms[i] += pm[i];
   }
   if (stats)
