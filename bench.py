@@ -183,9 +183,12 @@ def main():
     ap.add_argument("--small", action="store_true",
                     help="one short pass for profilers: one grid, 100k Rtree / RtreeBvh points, 8k brute-force points")
     ap.add_argument("--grid", type=int, default=128, help="grid edge of the --small pass")
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4"],
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
                     help="c2 (default): the headline line; c1 / c3: the small and the terrain configurations; "
-                         "c4: 256 grids batched in one plan against 256 single-grid calls")
+                         "c4: 256 grids batched in one plan against 256 single-grid calls; "
+                         "c5: the serving loop under Poisson arrivals at swept rates")
+    ap.add_argument("--rates", default="50,100,200,400", help="c5 arrival rates, requests/s")
+    ap.add_argument("--requests", type=int, default=200, help="c5 requests per rate")
     ap.add_argument("--batch", type=int, default=256, help="meshes of the c4 batch")
     ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()
@@ -193,6 +196,8 @@ def main():
         return small_case(args.grid)
     if args.workload == "c4":
         return batch_workload(args)
+    if args.workload == "c5":
+        return serving_workload(args)
     if args.workload != "c2":
         return other_workload(args)
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
@@ -517,6 +522,108 @@ def batch_workload(args):
     print(json.dumps(line), flush=True)
     if not same:
         raise SystemExit("batched grids differ from single-grid calls")
+
+
+def serving_workload(args):
+    """c5: a server with a 120 GB device-memory budget and 64 resident meshes
+    of the batched-grid kind (RtreeBvh), fed Poisson arrivals at each rate of
+    `--rates`: 5 % uploads of new meshes (built on the GPU), 60 % point
+    requests (Q log-uniform in [1e3, 1e6], uniform in the mesh's padded box),
+    40 % Raycast grid requests (edge log-uniform in [64, 256] over the padded
+    box).  Host buffers are pinned.  Latency is submission to completion as the
+    server records it; one JSON line with p50/p99 per rate."""
+    import torch
+
+    import mesh_to_sdf_b200 as m2s
+    from mesh_to_sdf_b200 import synth
+
+    A, S = m2s.AccelerationMethod, m2s.SignMethod
+    srv = m2s.Server(120 * 10**9, point_streams=4)
+    resident = synth.batch_meshes(64, seed=SEED + 5)
+    fresh = synth.batch_meshes(32, seed=SEED + 6)
+    ids = []
+    for v, i, *_ in resident:
+        mid, t = srv.submit_upload(v, m2s.Topology.TriangleList(i), A.rtree_bvh())
+        ids.append((mid, t))
+    for mid, t in ids:
+        assert srv.wait(t)[0] == 0
+    boxes = [(lo, hi) for _, _, lo, hi, _ in resident]
+    ids = [mid for mid, _ in ids]
+    rng = np.random.default_rng(SEED + 7)
+    unit = torch.from_numpy(rng.random((1_000_000, 3), dtype=np.float32)).pin_memory()
+    rates = [float(r) for r in args.rates.split(",") if r]
+    n_req = args.requests
+    lines = []
+    fresh_next = 0
+    for rate in rates:
+        # the stream: kinds, sizes, arrival times
+        kinds = rng.choice(3, size=n_req, p=[0.05, 0.60, 0.40])
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
+        reqs, out_elems = [], 0
+        for k in kinds:
+            j = int(rng.integers(len(ids)))
+            if k == 1:
+                q = int(10 ** rng.uniform(3, 6))
+                reqs.append(("points", j, q, out_elems))
+                out_elems += q
+            elif k == 2:
+                e = int(round(2 ** rng.uniform(6, 8)))
+                reqs.append(("grid", j, e, out_elems))
+                out_elems += e ** 3
+            else:
+                reqs.append(("upload", j, 0, out_elems))
+        out = torch.empty(out_elems, dtype=torch.float32).pin_memory()
+        outn = out.numpy()
+        # per-request query arrays: the pinned unit cube scaled into the mesh's box
+        qbufs = {}
+        for r_, (kind, j, n, o) in enumerate(reqs):
+            if kind == "points":
+                lo, hi = boxes[j]
+                qbufs[r_] = (unit[:n] * torch.from_numpy(hi - lo) + torch.from_numpy(lo)).pin_memory().numpy()
+        tickets = []
+        t0 = time.perf_counter()
+        for r_, (kind, j, n, o) in enumerate(reqs):
+            wait = t0 + arrivals[r_] - time.perf_counter()
+            if wait > 0:
+                time.sleep(wait)
+            if kind == "points":
+                tickets.append((kind, n, srv.submit_points(ids[j], qbufs[r_], outn[o:o + n])))
+            elif kind == "grid":
+                lo, hi = boxes[j]
+                g = m2s.Grid.from_bounding_box(lo, hi, [n, n, n])
+                tickets.append((kind, n ** 3, srv.submit_grid(ids[j], g, S.Raycast, outn[o:o + n ** 3])))
+            else:
+                v, i = fresh[fresh_next % len(fresh)][:2]
+                fresh_next += 1
+                mid, t = srv.submit_upload(v, m2s.Topology.TriangleList(i), A.rtree_bvh())
+                tickets.append((kind, len(i) // 3, t))
+        lat = {"points": [], "grid": [], "upload": []}
+        work = {"points": 0, "grid": 0, "upload": 0}
+        for kind, n, t in tickets:
+            st, l = srv.wait(t)
+            assert st == 0, (kind, st)
+            lat[kind].append(l)
+            work[kind] += n
+        span = time.perf_counter() - t0
+        allv = np.array(sum(lat.values(), []))
+
+        def pct(a, p):
+            return round(float(np.percentile(a, p)) * 1e3, 3) if len(a) else None
+
+        lines.append({"rate_rps": rate, "requests": n_req, "span_s": round(span, 3),
+                      "achieved_rps": round(n_req / span, 1),
+                      "p50_ms": pct(allv, 50), "p99_ms": pct(allv, 99),
+                      "points": {"n": len(lat["points"]), "p50_ms": pct(lat["points"], 50),
+                                 "p99_ms": pct(lat["points"], 99), "points_per_s": work["points"] / span},
+                      "grid": {"n": len(lat["grid"]), "p50_ms": pct(lat["grid"], 50),
+                               "p99_ms": pct(lat["grid"], 99), "cells_per_s": work["grid"] / span},
+                      "upload": {"n": len(lat["upload"]), "p50_ms": pct(lat["upload"], 50),
+                                 "p99_ms": pct(lat["upload"], 99)}})
+    stats = srv.stats()
+    srv.close()
+    print(json.dumps({"workload": "c5_serving", "budget_bytes": 120 * 10**9, "resident_meshes": 64,
+                      "mix": {"upload": 0.05, "points": 0.60, "grid": 0.40}, "sweep": lines,
+                      "server_stats": stats}), flush=True)
 
 
 def small_case(edge=128):

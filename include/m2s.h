@@ -192,6 +192,50 @@ int m2s_generate_sdf_none_noalloc(const float* d_vertices, uint64_t n_vertices,
                                   int topology, const float* d_query_points, uint64_t n_queries,
                                   int sign, float* d_out, void* stream);
 
+/* ---- serving loop (no counterpart in the reference) ----------------------- */
+
+/* The crate's resident API (build_sdf_acceleration / query_sdf, lib.rs:410-485)
+ * answers one call at a time on the caller's thread.  A server owns resident
+ * meshes and three worker threads (uploads, point requests, grid requests)
+ * and admits requests against a device-memory budget: each reserves an
+ * estimate of what it will hold and waits, in arrival order per kind, until
+ * that fits.  Point requests on different meshes overlap on a pool of
+ * `point_streams` streams (0 = 4); grid requests that wait together are
+ * computed as one batch.  Every result equals the one the single-request
+ * calls give (m2s_query_sdf with the mesh's method; m2s_grid_sdf_device).
+ * Submissions return a ticket at once; the caller's host buffers (queries,
+ * outputs) must stay valid until m2s_server_wait returns for that ticket.
+ * Pinned host buffers let copies overlap kernels.  Free the server only
+ * after every ticket was waited for. */
+typedef struct m2s_server m2s_server;
+int m2s_server_create(uint64_t hbm_budget_bytes, uint32_t point_streams, m2s_server** out);
+void m2s_server_free(m2s_server* server);
+/* Copies the mesh now; its triangle records and LBVH are built by the server.
+ * *mesh_id is valid at once: requests on it wait until the build is done.
+ * An upload that does not fit first evicts idle meshes (no queued or running
+ * request), least recently used first. */
+int m2s_server_submit_upload(m2s_server* server, const float* vertices, uint64_t n_vertices,
+                             const void* indices, uint64_t n_indices, int index_bits, int topology,
+                             int accel, int sign, uint32_t* mesh_id, uint64_t* ticket);
+/* query_sdf on a resident mesh: out receives n_queries floats. */
+int m2s_server_submit_points(m2s_server* server, uint32_t mesh_id, const float* query_points,
+                             uint64_t n_queries, float* out, uint64_t* ticket);
+/* generate_grid_sdf on a resident mesh: out receives the grid's cells. */
+int m2s_server_submit_grid(m2s_server* server, uint32_t mesh_id, const float first_cell[3],
+                           const float cell_size[3], const uint64_t cell_count[3], int sign,
+                           float* out, uint64_t* ticket);
+/* Waits for a ticket (timeout_s < 0: no limit; M2S_ERR_LIMIT if it is still
+ * pending at the timeout, the ticket staying valid); *status receives the
+ * request's status and *latency_s the time from submission to completion. */
+int m2s_server_wait(m2s_server* server, uint64_t ticket, double timeout_s, int* status,
+                    double* latency_s);
+/* Frees a resident mesh that no queued or running request uses. */
+int m2s_server_remove_mesh(m2s_server* server, uint32_t mesh_id);
+/* [uploads, point requests, grid requests completed; failed; grid batches;
+ *  grid requests batched; largest batch; reserved bytes; peak reserved bytes;
+ *  resident meshes; queued requests; evicted meshes]. */
+int m2s_server_stats(m2s_server* server, uint64_t out[12]);
+
 /* ---- utilities ----------------------------------------------------------- */
 
 /* Stable LSD radix sort of (uint32 key, uint32 value) pairs on the device, the

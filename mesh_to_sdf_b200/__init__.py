@@ -26,7 +26,7 @@ __all__ = [
     "SignMethod", "AccelerationMethod", "Topology", "Grid", "SnapResult", "SdfAccelerationMesh", "M2SError",
     "generate_sdf", "generate_grid_sdf", "build_sdf_acceleration", "query_sdf",
     "query_vector_to_closest_point_rtree_bvh", "ALL_SDF_ACCELERATION_METHODS", "device_available",
-    "grid_sdf_batch_device", "GridPlan", "grid_offsets", "set_grid_tuning", "clear_grid_autotune",
+    "grid_sdf_batch_device", "GridPlan", "grid_offsets", "set_grid_tuning", "clear_grid_autotune", "Server",
 ]
 
 F32 = np.float32
@@ -476,6 +476,98 @@ def set_grid_tuning(blocks_per_sm: int = 0, cells_per_block: int = 2048, wave_ce
 
 def clear_grid_autotune():
     _lib.lib().m2s_clear_grid_autotune()
+
+
+# ---- serving loop (no counterpart in the crate) -----------------------------
+
+SERVER_STATS = ("uploads", "point_requests", "grid_requests", "failed", "grid_batches", "grid_requests_batched",
+                "largest_batch", "reserved_bytes", "peak_reserved_bytes", "resident_meshes", "queued", "evictions")
+
+
+def _host_ptr(a):
+    """Pointer of a C-contiguous numpy array or CPU torch tensor (pinned or not)."""
+    if hasattr(a, "data_ptr"):
+        if a.is_cuda or not a.is_contiguous():
+            raise ValueError("server buffers are contiguous host memory")
+        return ctypes.c_void_p(a.data_ptr())
+    if not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("server buffers are contiguous host memory")
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class Server:
+    """Resident meshes, device-memory admission and batched requests on one GPU
+    (m2s_server_*).  submit_* return a ticket at once; the buffers passed stay
+    referenced here until wait() returns for that ticket.  Results equal the
+    single-request calls: query_sdf for points, SdfAccelerationMesh.grid_device
+    for grids."""
+
+    def __init__(self, hbm_budget_bytes: int, point_streams: int = 4):
+        h = ctypes.c_void_p(None)
+        _check(_lib.lib().m2s_server_create(int(hbm_budget_bytes), int(point_streams), ctypes.byref(h)),
+               "server_create")
+        self._h = h
+        self._keep = {}
+
+    def submit_upload(self, vertices, indices: Topology, acceleration_method: AccelerationMethod = None):
+        """Returns (mesh_id, ticket)."""
+        am = acceleration_method or AccelerationMethod.default()
+        v = _points(vertices)
+        idx, ni, bits, topo = indices._ffi()
+        mid, t = ctypes.c_uint32(0), ctypes.c_uint64(0)
+        _check(_lib.lib().m2s_server_submit_upload(self._h, _vp(v), len(v), _vp(idx), ni, bits, topo, am.kind,
+                                                   int(am.sign), ctypes.byref(mid), ctypes.byref(t)),
+               "server_submit_upload")
+        return int(mid.value), int(t.value)
+
+    def submit_points(self, mesh_id: int, queries, out):
+        """queries: (n,3) float32 host array; out: n float32 host array."""
+        t = ctypes.c_uint64(0)
+        n = int(queries.shape[0])
+        _check(_lib.lib().m2s_server_submit_points(self._h, int(mesh_id), _host_ptr(queries), n, _host_ptr(out),
+                                                   ctypes.byref(t)), "server_submit_points")
+        self._keep[t.value] = (queries, out)
+        return int(t.value)
+
+    def submit_grid(self, mesh_id: int, grid: Grid, sign_method: SignMethod, out):
+        """out: grid.get_total_cell_count() float32 host array."""
+        first = np.ascontiguousarray(grid.first_cell, F32)
+        size = np.ascontiguousarray(grid.cell_size, F32)
+        count = np.ascontiguousarray(np.array(grid.cell_count, np.uint64))
+        t = ctypes.c_uint64(0)
+        _check(_lib.lib().m2s_server_submit_grid(self._h, int(mesh_id), _vp(first), _vp(size), _vp(count),
+                                                 int(sign_method), _host_ptr(out), ctypes.byref(t)),
+               "server_submit_grid")
+        self._keep[t.value] = (out,)
+        return int(t.value)
+
+    def wait(self, ticket: int, timeout_s: float = -1.0):
+        """(status, latency_s) of a ticket; status 0 is success."""
+        st, lat = ctypes.c_int(0), ctypes.c_double(0.0)
+        _check(_lib.lib().m2s_server_wait(self._h, int(ticket), float(timeout_s), ctypes.byref(st),
+                                          ctypes.byref(lat)), "server_wait")
+        self._keep.pop(int(ticket), None)
+        return int(st.value), float(lat.value)
+
+    def remove_mesh(self, mesh_id: int):
+        _check(_lib.lib().m2s_server_remove_mesh(self._h, int(mesh_id)), "server_remove_mesh")
+
+    def stats(self):
+        a = np.zeros(len(SERVER_STATS), np.uint64)
+        _check(_lib.lib().m2s_server_stats(self._h, _vp(a)), "server_stats")
+        return dict(zip(SERVER_STATS, (int(x) for x in a)))
+
+    def close(self):
+        if self._h and self._h.value:
+            _lib.lib().m2s_server_free(self._h)
+            self._h = ctypes.c_void_p(None)
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def radix_sort_pairs_device(keys, values, key_bits=32, stream=None):

@@ -38,6 +38,14 @@ SIGNATURES = {
     "m2s_set_grid_tuning": (None, [I, ctypes.c_uint32, U64]),
     "m2s_grid_plan_waves": (ctypes.c_uint32, [P]),
     "m2s_radix_sort_pairs_device": (I, [P, P, U64, I, P]),
+    "m2s_server_create": (I, [U64, ctypes.c_uint32, P]),
+    "m2s_server_free": (None, [P]),
+    "m2s_server_submit_upload": (I, [P, P, U64, P, U64, I, I, I, I, P, P]),
+    "m2s_server_submit_points": (I, [P, ctypes.c_uint32, P, U64, P, P]),
+    "m2s_server_submit_grid": (I, [P, ctypes.c_uint32, P, P, P, I, P, P]),
+    "m2s_server_wait": (I, [P, U64, ctypes.c_double, P, P]),
+    "m2s_server_remove_mesh": (I, [P, ctypes.c_uint32]),
+    "m2s_server_stats": (I, [P, P]),
     "m2s_generate_sdf_none_noalloc": (I, [P, U64, P, U64, I, I, P, U64, I, P, P]),
     "m2s_last_grid_stats": (I, [P]),
     "m2s_set_profiling": (None, [I]),

@@ -879,6 +879,17 @@ uint64_t GridJob::device_bytes() const {
          (uint64_t)kLists * J.cap * 8 + 2ull * J.cap * 4 + J.table.n * sizeof(GridK);
 }
 
+uint32_t default_list_capacity(uint64_t cells) {
+  return (uint32_t)std::min<uint64_t>(std::max<uint64_t>(cells / 2, std::min<uint64_t>(cells + 1024, 1ull << 20)),
+                                      0x40000000ull);
+}
+
+uint64_t grid_job_bytes(uint64_t cells) {
+  const uint64_t cap = default_list_capacity(cells);
+  const uint64_t ray_words = 3 * (cells / 32 + 3 * std::cbrt((double)cells) * std::cbrt((double)cells));
+  return 16 * cells + (uint64_t)kLists * 8 * cap + 8 * cap + 4 * ray_words + (1u << 20);
+}
+
 int check_grid(const GridDesc& g) {
   for (int d = 0; d < 3; ++d)
     if (g.n[d] == 0 || g.n[d] > 0x7FFFFFFFull) return M2S_ERR_INVALID_ARGUMENT;
@@ -982,10 +993,7 @@ int GridJob::prepare(const MeshView* meshes, uint32_t n, const GridDesc* gds, in
       (st = J.bar.alloc(1, s)))
     return st;
   if (sign == M2S_SIGN_RAYCAST && (st = J.bits.alloc(woff, s))) return st;
-  J.cap = tune.list_capacity
-              ? tune.list_capacity
-              : (uint32_t)std::min<unsigned long long>(std::max<unsigned long long>(N / 2, std::min(N + 1024, 1ull << 20)),
-                                                       0x40000000ull);
+  J.cap = tune.list_capacity ? tune.list_capacity : default_list_capacity(N);
   // Cooperative grid: co-resident blocks, fewer for small jobs (a barrier
   // over fewer blocks is faster and a small bucket does not fill many).
   const void* kern = sign == M2S_SIGN_RAYCAST ? propagate_kernel<M2S_SIGN_RAYCAST>(J.multi)

@@ -226,6 +226,11 @@ int grid_sdf_batch(const MeshView* meshes, uint32_t n, const GridDesc* grids, in
 // Validates a grid description for the device path (32-bit cell indices).
 int check_grid(const GridDesc& g);
 
+// Entries per bucket list of a job of `cells` cells (before any overflow
+// restart), and the device bytes of such a job's workspace.
+uint32_t default_list_capacity(uint64_t cells);
+uint64_t grid_job_bytes(uint64_t cells);
+
 // Process-wide grid knobs (m2s_set_grid_tuning).
 extern GridTuning g_grid_tuning;
 
