@@ -557,7 +557,7 @@ def serving_workload(args):
     fresh_next = 0
     for rate in rates:
         # the stream: kinds, sizes, arrival times
-        kinds = rng.choice(3, size=n_req, p=[0.05, 0.60, 0.40])
+        kinds = rng.choice(3, size=n_req, p=[0.05, 0.95 * 0.60, 0.95 * 0.40])
         arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
         reqs, out_elems = [], 0
         for k in kinds:
@@ -622,7 +622,7 @@ def serving_workload(args):
     stats = srv.stats()
     srv.close()
     print(json.dumps({"workload": "c5_serving", "budget_bytes": 120 * 10**9, "resident_meshes": 64,
-                      "mix": {"upload": 0.05, "points": 0.60, "grid": 0.40}, "sweep": lines,
+                      "mix": {"upload": 0.05, "points": 0.57, "grid": 0.38}, "sweep": lines,
                       "server_stats": stats}), flush=True)
 
 
