@@ -418,16 +418,19 @@ __device__ __forceinline__ void st_release(unsigned int* p, unsigned int v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Sense-reversing barrier over the co-resident blocks of a cooperative launch.
-// The wait is bounded: after kBarrierPolls polls it raises `abort`, which makes
-// every block leave the kernel at its next barrier.
+// Barrier over the co-resident blocks of a cooperative launch.  Every block
+// passes the same sequence of barriers, so each keeps the generation count in
+// shared memory and waits for the global one to reach its next value: an
+// arrival costs the group atomic, the top atomic for the last of a group, and
+// the wait.  The wait is bounded: after kBarrierPolls polls it raises `abort`,
+// which makes every block leave the kernel at its next barrier.
 constexpr uint32_t kBarrierPolls = 1u << 22;  // about a second of polling
 
-__device__ __forceinline__ bool grid_barrier(GridBarrier* bar, unsigned int nblocks) {
+__device__ __forceinline__ bool grid_barrier(GridBarrier* bar, unsigned int nblocks, unsigned int* gen) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    const unsigned int g0 = ld_acquire(&bar->gen);
+    const unsigned int target = *gen + 1;
     const unsigned int grp = blockIdx.x / kBarrierFan;
     const unsigned int ngroups = (nblocks + kBarrierFan - 1) / kBarrierFan;
     const unsigned int in_grp = min((unsigned)kBarrierFan, nblocks - grp * kBarrierFan);
@@ -438,10 +441,10 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* bar, unsigned int nblo
     }
     if (last) {
       bar->top[0] = 0;
-      st_release(&bar->gen, g0 + 1);
+      st_release(&bar->gen, target);
     } else {
       uint32_t polls = 0;
-      while (ld_acquire(&bar->gen) == g0) {
+      while (ld_acquire(&bar->gen) != target) {
         if (ld_acquire(&bar->abort)) break;
         if (++polls > kBarrierPolls) {
           atomicExch(&bar->abort, 1u);
@@ -449,67 +452,83 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* bar, unsigned int nblo
         }
       }
     }
+    *gen = target;
     ok = ld_acquire(&bar->abort) ? 0 : 1;
   }
   __syncthreads();
   return ok != 0;
 }
 
-constexpr int kTouchStage = 2048;  // touched cells staged per block and round
+// Touched cells staged per block and round in shared memory; a block commits
+// the cells it touched itself, so only a block whose stage fills up writes to
+// the global spill list.
+constexpr int kTouchStage = 6144;
+constexpr int kUnroll = 4;  // proposals per thread in flight
 
 struct Sched {
   uint32_t b, B;
   uint32_t slot[kRing];
-  uint32_t cur, fp, round;
+  uint32_t cur, fp, round, n;
   int action;
 };
 enum { kRelax = 0, kRedistribute = 1, kDone = 2, kLimit = 3 };
 
 // Next step of the schedule, computed by thread 0 of every block from the
 // global list counts (final at this point: the last grid barrier ordered every
-// push before it).  Block 0 also empties the list relaxed last round, which no
-// block reads here and which receives pushes only after the next barrier.
+// push before it).  All counts it may need are loaded together, one round trip.
+// Block 0 also empties the list relaxed last round, which no block reads here
+// and which receives pushes only after the next barrier.
 __device__ __forceinline__ int next_step(Sched& sh, PropState* st, bool leader) {
-  if (*(volatile uint32_t*)&st->overflow) return kDone;
-  const uint32_t consumed = sh.cur;
-  for (int q = 0; q < kRing; ++q) {
-    const uint32_t s0 = sh.slot[0];
-    if (*(volatile uint32_t*)&st->count[s0] > 0) {
-      sh.slot[0] = consumed;  // becomes the list of states re-queued at bucket b
-      sh.cur = s0;
-      sh.round += 1;
-      if (leader) {
-        st->count[consumed] = 0;
-        st->max_list = max(st->max_list, *(volatile uint32_t*)&st->count[s0]);
-      }
-      return kRelax;
+  uint32_t c[kRing];
+#pragma unroll
+  for (int k = 0; k < kRing; ++k) c[k] = *(volatile uint32_t*)&st->count[sh.slot[k]];
+  const uint32_t overflow = *(volatile uint32_t*)&st->overflow;
+  const uint32_t far_n = *(volatile uint32_t*)&st->count[kFar0 + sh.fp];
+  const uint32_t far_b = *(volatile uint32_t*)&st->far_min[sh.fp];
+  if (overflow) return kDone;
+  // slot[q] holds bucket b + q; the window ends at bucket B + kRing - 1.
+  int q = 0;
+  while (q < kRing && sh.b + q < sh.B + kRing && c[q] == 0) ++q;
+  if (q < kRing && sh.b + q < sh.B + kRing) {
+    uint32_t rot[kRing];
+#pragma unroll
+    for (int k = 0; k < kRing; ++k) rot[k] = sh.slot[(k + q) % kRing];  // advance b by q
+    const uint32_t consumed = sh.cur;
+    sh.cur = rot[0];
+    rot[0] = consumed;  // becomes the list of states re-queued at bucket b
+#pragma unroll
+    for (int k = 0; k < kRing; ++k) sh.slot[k] = rot[k];
+    sh.b += q;
+    sh.n = c[q];
+    sh.round += 1;
+    if (leader) {
+      st->count[consumed] = 0;
+      st->max_list = max(st->max_list, c[q]);
     }
-    if (sh.b + 1 >= sh.B + kRing) break;  // window exhausted
-    sh.b += 1;
-    for (int w = 0; w + 1 < kRing; ++w) sh.slot[w] = sh.slot[w + 1];
-    sh.slot[kRing - 1] = s0;
+    return kRelax;
   }
   // Every window list is empty.  Far states all lie at or beyond B + kRing, so
   // the new window starts at the lowest of them.
-  if (*(volatile uint32_t*)&st->count[kFar0 + sh.fp] == 0) return kDone;
-  sh.B = sh.b = *(volatile uint32_t*)&st->far_min[sh.fp];
+  if (far_n == 0) return kDone;
+  sh.B = sh.b = far_b;
   return kRedistribute;
 }
 
 template <int SIGN, bool MULTI>
 __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ GridSet gs, const TriRec* __restrict__ tris,
                                                    unsigned long long* snap_keys, unsigned long long* work_keys,
-                                                   uint2* lists, uint32_t cap, uint32_t* touched_lists,
+                                                   uint2* lists, uint32_t cap, uint32_t* spill_lists,
                                                    PropState* st, GridBarrier* bar, uint32_t max_steps,
                                                    uint32_t* status) {
   __shared__ Sched sh;
   __shared__ uint32_t s_touch[kTouchStage];
-  __shared__ uint32_t s_ntouch, s_nloc, s_touch_base;
+  __shared__ uint32_t s_ntouch, s_gen;
   const unsigned int nblocks = gridDim.x;
   const int lane = threadIdx.x & 31;
   const bool lead_block = blockIdx.x == 0;
   if (threadIdx.x == 0) {
     s_ntouch = 0;
+    s_gen = 0;
     sh.b = st->b;
     sh.B = st->B;
     for (int k = 0; k < kRing; ++k) sh.slot[k] = st->slot[k];
@@ -522,7 +541,10 @@ __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ GridS
   uint32_t far_phases = 0;
   bool aborted = false;
   for (uint32_t it = 0;; ++it) {
-    if (threadIdx.x == 0) sh.action = it >= max_steps ? kLimit : next_step(sh, st, lead_block);
+    if (threadIdx.x == 0) {
+      s_ntouch = 0;  // every thread read it in the last commit, before the last barrier
+      sh.action = it >= max_steps ? kLimit : next_step(sh, st, lead_block);
+    }
     __syncthreads();
     const int action = sh.action;
     if (action == kDone) break;
@@ -554,7 +576,7 @@ __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ GridS
         }
         push_entry_warp(st, sh.b, sh.B, sh.slot, sh.fp ^ 1u, lists, cap, act, ent.x, ent.y, nb);
       }
-      if (!grid_barrier(bar, nblocks)) {
+      if (!grid_barrier(bar, nblocks, &s_gen)) {
         aborted = true;
         break;
       }
@@ -569,27 +591,29 @@ __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ GridS
       continue;
     }
     const uint32_t parity = sh.round & 1u;
-    uint32_t* touched_list = touched_lists + (unsigned long long)parity * cap;
+    uint32_t* spill = spill_lists + (unsigned long long)parity * cap;
     // ---- propose: every state of the bucket evaluates its triangle at the 27
     // cells of its 3x3x3 block; a proposal that beats the cell's value at the
     // start of the round enters the working value (atomic minimum) and the
-    // first such proposal lists the cell as touched.
-    const uint32_t n = min(*(volatile uint32_t*)&st->count[sh.cur], cap);
+    // first such proposal stages the cell as touched by this block.
+    const uint32_t n = min(sh.n, cap);
     const uint2* list = lists + (unsigned long long)sh.cur * cap;
     // One thread per (state, neighbour) proposal; consecutive threads share a
-    // state, so its entry and triangle loads are warp broadcasts.  Two
-    // independent proposals per iteration keep two load chains in flight.
-    // Thread t takes proposals t, t + T, t + 2T, ... as (state e, neighbour k)
-    // pairs advanced without division: T = 27 * dE + dK.
+    // state, so its entry and triangle loads are warp broadcasts.  kUnroll
+    // independent proposals per iteration keep that many load chains in
+    // flight.  Thread t takes proposals t, t + T, t + 2T, ... as (state e,
+    // neighbour k) pairs advanced without division: T = 27 * dE + dK.
     const uint32_t T = gridDim.x * blockDim.x;
     const uint32_t dE = T / 27u, dK = T % 27u;
     const uint32_t t0 = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t e = t0 / 27u, k = t0 % 27u;
     while (e < n) {
-      bool first[2] = {false, false};
-      uint32_t jj[2] = {0, 0};
+      bool first[kUnroll];
+      uint32_t jj[kUnroll];
 #pragma unroll
-      for (int u = 0; u < 2; ++u) {
+      for (int u = 0; u < kUnroll; ++u) {
+        first[u] = false;
+        jj[u] = 0;
         const uint32_t eu = e, ku = k;
         k += dK;
         e += dE;
@@ -622,62 +646,57 @@ __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ GridS
         }
       }
 #pragma unroll
-      for (int u = 0; u < 2; ++u) {
+      for (int u = 0; u < kUnroll; ++u) {
         if (first[u]) {
           const uint32_t q = atomicAdd(&s_ntouch, 1u);
           if (q < kTouchStage) {
             s_touch[q] = jj[u];
           } else {
             const uint32_t pos = atomicAdd(&st->touched2[parity], 1u);
-            if (pos < cap) touched_list[pos] = jj[u];
+            if (pos < cap) spill[pos] = jj[u];
             else atomicOr(&st->overflow, 1u);
           }
         }
       }
     }
-    // flush this block's staged touched cells with one global atomic.  Thread
-    // 0 alone reads and resets the stage count and publishes it: a thread that
-    // read s_ntouch after the reset would skip its share of the stage and leave
-    // unwritten words in the touched list.
-    __syncthreads();
-    {
-      if (threadIdx.x == 0) {
-        const uint32_t nl = min(s_ntouch, (uint32_t)kTouchStage);
-        s_nloc = nl;
-        s_touch_base = nl ? atomicAdd(&st->touched2[parity], nl) : 0;
-        s_ntouch = 0;
-      }
-      __syncthreads();
-      const uint32_t nloc = s_nloc;
-      for (uint32_t i = threadIdx.x; i < nloc; i += blockDim.x) {
-        const uint32_t pos = s_touch_base + i;
-        if (pos < cap) touched_list[pos] = s_touch[i];
-        else atomicOr(&st->overflow, 1u);
-      }
-    }
     if (lead_block && threadIdx.x == 0) atomicAdd(&st->entries, (unsigned long long)n);
-    if (!grid_barrier(bar, nblocks)) {
+    if (!grid_barrier(bar, nblocks, &s_gen)) {
       aborted = true;
       break;
     }
     // ---- commit: each touched cell publishes its round winner to the snapshot
     // and queues (cell, winning triangle) under the winner's distance bucket.
+    // A block commits the cells it staged; all blocks share the spill list.
     if (lead_block && threadIdx.x == 0) st->touched2[parity ^ 1u] = 0;
-    const uint32_t nt = min(*(volatile uint32_t*)&st->touched2[parity], cap);
-    for (uint32_t base = blockIdx.x * blockDim.x; base < nt; base += gridDim.x * blockDim.x) {
+    const uint32_t nspill = min(*(volatile uint32_t*)&st->touched2[parity], cap);
+    const uint32_t nloc = min(s_ntouch, (uint32_t)kTouchStage);
+    for (uint32_t base = 0; base < nloc; base += blockDim.x) {
       const uint32_t i = base + threadIdx.x;
-      const bool act = i < nt;
+      const bool act = i < nloc;
       uint32_t j = 0, nb = 0;
       unsigned long long w = KEY_EMPTY;
       if (act) {
-        j = __ldcg(&touched_list[i]);
+        j = s_touch[i];
         w = __ldcg(&work_keys[j]);
         snap_keys[j] = w;
         nb = bucket_of(grid_of_tri<MULTI>(gs, key_tri(w)).inv_delta, key_dist(w));
       }
       push_entry_warp(st, sh.b, sh.B, sh.slot, sh.fp, lists, cap, act, j, key_tri(w), nb);
     }
-    if (!grid_barrier(bar, nblocks)) {
+    for (uint32_t base = blockIdx.x * blockDim.x; base < nspill; base += gridDim.x * blockDim.x) {
+      const uint32_t i = base + threadIdx.x;
+      const bool act = i < nspill;
+      uint32_t j = 0, nb = 0;
+      unsigned long long w = KEY_EMPTY;
+      if (act) {
+        j = __ldcg(&spill[i]);
+        w = __ldcg(&work_keys[j]);
+        snap_keys[j] = w;
+        nb = bucket_of(grid_of_tri<MULTI>(gs, key_tri(w)).inv_delta, key_dist(w));
+      }
+      push_entry_warp(st, sh.b, sh.B, sh.slot, sh.fp, lists, cap, act, j, key_tri(w), nb);
+    }
+    if (!grid_barrier(bar, nblocks, &s_gen)) {
       aborted = true;
       break;
     }
