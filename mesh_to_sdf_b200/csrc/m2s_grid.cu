@@ -160,7 +160,8 @@ struct PropState {
   uint32_t far_min[2];   // lowest bucket in each far list
   uint32_t touched2[2];  // touched cells per round parity
   uint32_t done;
-  uint32_t overflow;
+  uint32_t overflow;      // a list push did not fit (collection, commit, redistribution)
+  uint32_t overflow2[2];  // a spill did not fit, per round parity (propose)
   uint32_t round;
   uint32_t far_phases;
   uint32_t max_list;      // largest bucket list relaxed in one round
@@ -482,7 +483,11 @@ __device__ __forceinline__ int next_step(Sched& sh, PropState* st, bool leader) 
   uint32_t c[kRing];
 #pragma unroll
   for (int k = 0; k < kRing; ++k) c[k] = *(volatile uint32_t*)&st->count[sh.slot[k]];
-  const uint32_t overflow = *(volatile uint32_t*)&st->overflow;
+  // Only values no block can change before every block has passed this step:
+  // list counts (pushes come after the next barrier), the push overflow flag
+  // and the spill overflow flag of the round just finished (the next propose
+  // phase writes the other parity).
+  const uint32_t overflow = *(volatile uint32_t*)&st->overflow | *(volatile uint32_t*)&st->overflow2[sh.round & 1u];
   const uint32_t far_n = *(volatile uint32_t*)&st->count[kFar0 + sh.fp];
   const uint32_t far_b = *(volatile uint32_t*)&st->far_min[sh.fp];
   if (overflow) return kDone;
@@ -556,7 +561,13 @@ __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ GridS
       // ---- move every far state to its bucket's list, or to the other far
       // list when it lies beyond the new window.  The bucket is recomputed
       // from the state's cell and triangle, the same arithmetic that produced
-      // it, so it is exactly the bucket the state was filed under.
+      // it, so it is exactly the bucket the state was filed under.  The
+      // barrier first lets every block finish the step that chose this phase:
+      // that step reads the list counts these pushes change.
+      if (!grid_barrier(bar, nblocks, &s_gen)) {
+        aborted = true;
+        break;
+      }
       const uint32_t F = kFar0 + sh.fp;
       const uint32_t nf = min(*(volatile uint32_t*)&st->count[F], cap);
       const uint2* far = lists + (unsigned long long)F * cap;
@@ -654,7 +665,7 @@ __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ GridS
           } else {
             const uint32_t pos = atomicAdd(&st->touched2[parity], 1u);
             if (pos < cap) spill[pos] = jj[u];
-            else atomicOr(&st->overflow, 1u);
+            else atomicOr(&st->overflow2[parity], 1u);
           }
         }
       }
@@ -1137,7 +1148,7 @@ int GridJob::read_state(cudaStream_t s, GridRunInfo* info) {
   if (!h) return M2S_ERR_OUT_OF_MEMORY;
   M2S_CUDA(cudaMemcpyAsync(h, J.state.p, sizeof(PropState), cudaMemcpyDeviceToHost, s));
   M2S_CUDA(cudaStreamSynchronize(s));
-  info->overflow = h->overflow != 0;
+  info->overflow = (h->overflow | h->overflow2[0] | h->overflow2[1]) != 0;
   info->seeds = h->seeds;
   info->rounds = h->round;
   info->entries = h->entries;
