@@ -464,7 +464,7 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* bar, unsigned int nblo
 // the cells it touched itself, so only a block whose stage fills up writes to
 // the global spill list.
 constexpr int kTouchStage = 6144;
-constexpr int kUnroll = 4;  // proposals per thread in flight
+constexpr int kUnroll = 2;  // proposals per thread in flight
 
 struct Sched {
   uint32_t b, B;
