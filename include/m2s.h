@@ -44,7 +44,8 @@ enum m2s_status {
   M2S_ERR_CUDA = 7,
   M2S_ERR_OUT_OF_MEMORY = 8,
   M2S_ERR_LIMIT = 9, /* a bounded device loop (stack, worklist, rounds) hit its limit */
-  M2S_ERR_NO_DEVICE = 10
+  M2S_ERR_NO_DEVICE = 10,
+  M2S_ERR_FORMAT = 11 /* serde.rs: SerdeError::DeserializationFailed */
 };
 
 enum { M2S_TOPOLOGY_TRIANGLE_LIST = 0, M2S_TOPOLOGY_TRIANGLE_STRIP = 1 }; /* lib.rs:156-171 */
@@ -235,6 +236,32 @@ int m2s_server_remove_mesh(m2s_server* server, uint32_t mesh_id);
  *  grid requests batched; largest batch; reserved bytes; peak reserved bytes;
  *  resident meshes; queued requests; evicted meshes]. */
 int m2s_server_stats(m2s_server* server, uint64_t out[12]);
+
+/* ---- results for the viewer and on disk ----------------------------------- */
+
+/* The voxel viewer's index buffer (mesh_to_sdf_client/src/sdf.rs:63-71): the
+ * indices 0..n-1 stably sorted by f32::total_cmp of the distances, and the
+ * (min, max) of the distances as its iso limits.  Device arrays, asynchronous
+ * on `stream`; d_minmax (2 floats) may be NULL.  n < 2^32. */
+int m2s_sort_cells_by_distance_device(const float* d_sdf, uint64_t n, uint32_t* d_order, float* d_minmax,
+                                      void* stream);
+/* The same from and into host memory (returns when done). */
+int m2s_sort_cells_by_distance(const float* sdf, uint64_t n, uint32_t* order, float minmax[2], void* stream);
+
+/* The crate's on-disk format V1 (serde.rs:106-221, rmp-serde encoding):
+ * save_to_file writes these bytes, read_from_file reads them.  Host memory
+ * only, no device needed.  With out = NULL, *out_len receives the size. */
+int m2s_serialize_generic(const float* query_points, uint64_t n_points, const float* distances,
+                          uint64_t n_distances, uint8_t* out, uint64_t capacity, uint64_t* out_len);
+int m2s_serialize_grid(const float first_cell[3], const float cell_size[3], const uint64_t cell_count[3],
+                       const float* distances, uint64_t n_distances, uint8_t* out, uint64_t capacity,
+                       uint64_t* out_len);
+/* *kind: 0 generic, 1 grid.  Call with NULL arrays to learn the counts, then
+ * again with arrays of 3 * n_points and n_distances floats.  Malformed data:
+ * M2S_ERR_FORMAT. */
+int m2s_deserialize(const uint8_t* data, uint64_t len, int* kind, uint64_t* n_points, uint64_t* n_distances,
+                    float* query_points, float* distances, float grid_first[3], float grid_size[3],
+                    uint64_t grid_count[3]);
 
 /* ---- utilities ----------------------------------------------------------- */
 

@@ -27,13 +27,14 @@ __all__ = [
     "generate_sdf", "generate_grid_sdf", "build_sdf_acceleration", "query_sdf",
     "query_vector_to_closest_point_rtree_bvh", "ALL_SDF_ACCELERATION_METHODS", "device_available",
     "grid_sdf_batch_device", "GridPlan", "grid_offsets", "set_grid_tuning", "clear_grid_autotune", "Server",
+    "sort_cells_by_distance", "sort_cells_by_distance_device",
 ]
 
 F32 = np.float32
 
 STATUS = {
     0: "OK", 1: "INVALID_ARGUMENT", 2: "NONFINITE_QUERY", 3: "INDEX_COUNT", 4: "INDEX_RANGE",
-    5: "NAN_DISTANCE", 6: "EMPTY_MESH", 7: "CUDA", 8: "OUT_OF_MEMORY", 9: "LIMIT", 10: "NO_DEVICE",
+    5: "NAN_DISTANCE", 6: "EMPTY_MESH", 7: "CUDA", 8: "OUT_OF_MEMORY", 9: "LIMIT", 10: "NO_DEVICE", 11: "FORMAT",
 }
 
 
@@ -476,6 +477,29 @@ def set_grid_tuning(blocks_per_sm: int = 0, cells_per_block: int = 2048, wave_ce
 
 def clear_grid_autotune():
     _lib.lib().m2s_clear_grid_autotune()
+
+
+# ---- results for the viewer -----------------------------------------------------
+
+def sort_cells_by_distance(distances):
+    """mesh_to_sdf_client/src/sdf.rs:63-71 on the GPU: (order, (min, max)) —
+    the cell indices stably sorted by f32::total_cmp of the distances (u32) and
+    the distances' extremes (the viewer's iso limits)."""
+    d = np.ascontiguousarray(distances, F32).reshape(-1)
+    order = np.empty(len(d), np.uint32)
+    mm = np.zeros(2, F32)
+    if len(d):
+        _check(_lib.lib().m2s_sort_cells_by_distance(_vp(d), len(d), _vp(order), _vp(mm), None),
+               "sort_cells_by_distance")
+    return order, (float(mm[0]), float(mm[1]))
+
+
+def sort_cells_by_distance_device(distances, order, minmax=None, stream=None):
+    """The same on device tensors (float32 in, uint32/int32 order out, optional 2-float minmax)."""
+    _check(_lib.lib().m2s_sort_cells_by_distance_device(
+        ctypes.c_void_p(distances.data_ptr()), distances.numel(), ctypes.c_void_p(order.data_ptr()),
+        None if minmax is None else ctypes.c_void_p(minmax.data_ptr()),
+        None if stream is None else ctypes.c_void_p(stream)), "sort_cells_by_distance_device")
 
 
 # ---- serving loop (no counterpart in the crate) -----------------------------

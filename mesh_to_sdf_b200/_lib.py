@@ -38,6 +38,11 @@ SIGNATURES = {
     "m2s_set_grid_tuning": (None, [I, ctypes.c_uint32, U64]),
     "m2s_grid_plan_waves": (ctypes.c_uint32, [P]),
     "m2s_radix_sort_pairs_device": (I, [P, P, U64, I, P]),
+    "m2s_sort_cells_by_distance_device": (I, [P, U64, P, P, P]),
+    "m2s_sort_cells_by_distance": (I, [P, U64, P, P, P]),
+    "m2s_serialize_generic": (I, [P, U64, P, U64, P, U64, P]),
+    "m2s_serialize_grid": (I, [P, P, P, P, U64, P, U64, P]),
+    "m2s_deserialize": (I, [P, U64, P, P, P, P, P, P, P, P]),
     "m2s_server_create": (I, [U64, ctypes.c_uint32, P]),
     "m2s_server_free": (None, [P]),
     "m2s_server_submit_upload": (I, [P, P, U64, P, U64, I, I, I, I, P, P]),

@@ -214,6 +214,7 @@ const char* m2s_status_string(int status) {
     case M2S_ERR_OUT_OF_MEMORY: return "out of device memory";
     case M2S_ERR_LIMIT: return "a bounded device loop hit its limit";
     case M2S_ERR_NO_DEVICE: return "no usable sm_100 CUDA device";
+    case M2S_ERR_FORMAT: return "malformed serialized signed distance field";
     default: return "unknown status";
   }
 }
