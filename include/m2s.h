@@ -263,6 +263,16 @@ int m2s_deserialize(const uint8_t* data, uint64_t len, int* kind, uint64_t* n_po
                     float* query_points, float* distances, float grid_first[3], float grid_size[3],
                     uint64_t grid_count[3]);
 
+/* check_mesh_triangle_list (generate/mesh_check.rs:24-81) on the device, by
+ * sorting (O(E log E); the crate's edge loop is O(E^2)), with the crate's
+ * verdict and the crate's first reported failure: *result 0 = Ok; 1 = the
+ * index count is not a multiple of 3; 2 = duplicate vertex (detail[0] = its
+ * index); 3 = duplicate face (detail[0] = its face index); 4 = duplicate edge
+ * detail[0] -> detail[1]; 5 = edge detail[0] -> detail[1] without a reverse
+ * edge.  Host arrays; returns when done. */
+int m2s_check_mesh_triangle_list(const float* vertices, uint64_t n_vertices, const uint32_t* faces,
+                                 uint64_t n_face_indices, int* result, uint64_t detail[2], void* stream);
+
 /* ---- utilities ----------------------------------------------------------- */
 
 /* Stable LSD radix sort of (uint32 key, uint32 value) pairs on the device, the

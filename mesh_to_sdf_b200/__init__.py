@@ -27,7 +27,7 @@ __all__ = [
     "generate_sdf", "generate_grid_sdf", "build_sdf_acceleration", "query_sdf",
     "query_vector_to_closest_point_rtree_bvh", "ALL_SDF_ACCELERATION_METHODS", "device_available",
     "grid_sdf_batch_device", "GridPlan", "grid_offsets", "set_grid_tuning", "clear_grid_autotune", "Server",
-    "sort_cells_by_distance", "sort_cells_by_distance_device",
+    "sort_cells_by_distance", "sort_cells_by_distance_device", "check_mesh_triangle_list",
 ]
 
 F32 = np.float32
@@ -500,6 +500,50 @@ def sort_cells_by_distance_device(distances, order, minmax=None, stream=None):
         ctypes.c_void_p(distances.data_ptr()), distances.numel(), ctypes.c_void_p(order.data_ptr()),
         None if minmax is None else ctypes.c_void_p(minmax.data_ptr()),
         None if stream is None else ctypes.c_void_p(stream)), "sort_cells_by_distance_device")
+
+
+# ---- mesh check ------------------------------------------------------------------
+
+def _rust_debug_f32(x) -> str:
+    """`{:?}` of an f32 as Rust prints it: shortest round-trip digits, decimal
+    with at least one fractional digit for 1e-4 <= |x| < 1e16 (and 0),
+    exponential otherwise."""
+    x = np.float32(x)
+    if np.isnan(x):
+        return "NaN"
+    if np.isinf(x):
+        return "inf" if x > 0 else "-inf"
+    a = np.abs(x)  # compared in f32, as Rust does
+    if a == 0 or np.float32(1e-4) <= a < np.float32(1e16):
+        return np.format_float_positional(x, unique=True, trim="0")
+    mant, exp = np.format_float_scientific(x, unique=True, trim="-").split("e")
+    return f"{mant}e{int(exp)}"
+
+
+def check_mesh_triangle_list(vertices, faces):
+    """generate/mesh_check.rs:24-81 on the GPU: None when the mesh is
+    watertight with no duplicate vertices or faces (the crate's Ok(())),
+    otherwise the crate's error message (its Err(String))."""
+    v = np.ascontiguousarray(np.asarray(vertices, F32).reshape(-1, 3))
+    f = np.ascontiguousarray(np.asarray(faces).reshape(-1).astype(np.uint32))
+    result = ctypes.c_int(0)
+    detail = np.zeros(2, np.uint64)
+    _check(_lib.lib().m2s_check_mesh_triangle_list(_vp(v) if len(v) else None, len(v), _vp(f) if len(f) else None,
+                                                   len(f), ctypes.byref(result), _vp(detail), None),
+           "check_mesh_triangle_list")
+    k, a, b = result.value, int(detail[0]), int(detail[1])
+    if k == 0:
+        return None
+    if k == 1:
+        return "Faces must be a multiple of 3"
+    if k == 2:
+        x, y, z = (_rust_debug_f32(c) for c in v[a])
+        return f"Duplicate vertex found at ({x}, {y}, {z})"
+    if k == 3:
+        return f"Duplicate face found: [{f[3 * a]}, {f[3 * a + 1]}, {f[3 * a + 2]}]"
+    if k == 4:
+        return f"Duplicate edge {a} -> {b} - do you have an inverted normal?"
+    return (f"Mesh is not waterproof - edge {a} -> {b} does not have a corresponding edge {b} -> {a}")
 
 
 # ---- serving loop (no counterpart in the crate) -----------------------------

@@ -43,6 +43,7 @@ SIGNATURES = {
     "m2s_serialize_generic": (I, [P, U64, P, U64, P, U64, P]),
     "m2s_serialize_grid": (I, [P, P, P, P, U64, P, U64, P]),
     "m2s_deserialize": (I, [P, U64, P, P, P, P, P, P, P, P]),
+    "m2s_check_mesh_triangle_list": (I, [P, U64, P, U64, P, P, P]),
     "m2s_server_create": (I, [U64, ctypes.c_uint32, P]),
     "m2s_server_free": (None, [P]),
     "m2s_server_submit_upload": (I, [P, P, U64, P, U64, I, I, I, I, P, P]),

@@ -55,6 +55,7 @@ def lib():
             L.orc_generate_grid_sdf.argtypes = [P, U64, P, U64, I, I, P, P, P, I, P, P, I, P]
             L.orc_generate_sdf_f64.argtypes = [P, U64, P, U64, I, I, P, U64, P, P, I]
             L.orc_grid_snap_point.restype = I
+            L.orc_check_mesh_triangle_list.argtypes = [P, U64, P, U64, P, P]
             _lib = L
     return _lib
 
@@ -245,3 +246,13 @@ def grid_snap_point(first_cell, cell_size, cell_count, p):
     c = np.ascontiguousarray(np.asarray(cell_count, dtype=np.uint64).reshape(3))
     inside = lib().orc_grid_snap_point(_ptr(f), _ptr(s), _ptr(c), _ptr(pp), _ptr(cell))
     return bool(inside), [int(x) for x in cell]
+
+
+def check_mesh_triangle_list(vertices, faces):
+    """(kind, (a, b)) of generate/mesh_check.rs:24-81 — see m2s_oracle.h for the kinds."""
+    v = np.ascontiguousarray(np.asarray(vertices, np.float32).reshape(-1, 3))
+    f = np.ascontiguousarray(np.asarray(faces, np.uint32).reshape(-1))
+    kind = ctypes.c_int(0)
+    detail = np.zeros(2, np.uint64)
+    lib().orc_check_mesh_triangle_list(_ptr(v), len(v), _ptr(f), len(f), ctypes.byref(kind), _ptr(detail))
+    return kind.value, (int(detail[0]), int(detail[1]))

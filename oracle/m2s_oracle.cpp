@@ -23,6 +23,8 @@
 #include <mutex>
 #include <queue>
 #include <thread>
+#include <array>
+#include <set>
 #include <vector>
 
 #include "geo_ref.hpp"
@@ -879,6 +881,79 @@ int orc_generate_sdf_f64(const float* v, uint64_t nv, const void* idx, uint64_t 
     }
     out_inside[i] = insides > 1 ? 1 : 0;
   }
+  return ST_OK;
+}
+
+// check_mesh_triangle_list (generate/mesh_check.rs:24-81), restated step by
+// step.  The crate compares vertices by their `{:?}` text, which is the same
+// as comparing the f32 bit patterns except that every NaN prints "NaN": the
+// key below merges the NaNs.  Faces compare as ordered index triples.  The
+// edge loop is the crate's: pop the last edge, fail if another copy remains
+// or if its reverse is missing, drop every copy of the reverse.
+// kind: 0 ok, 1 length not a multiple of 3, 2 duplicate vertex (detail[0] =
+// vertex index), 3 duplicate face (detail[0] = face index), 4 duplicate edge,
+// 5 edge without its reverse (detail = from, to).
+int orc_check_mesh_triangle_list(const float* vertices, uint64_t nv, const uint32_t* faces, uint64_t n_idx,
+                                 int* kind, uint64_t* detail) {
+  detail[0] = detail[1] = 0;
+  if (n_idx % 3 != 0) {
+    *kind = 1;
+    return ST_OK;
+  }
+  auto vkey = [&](uint64_t i, int d) {
+    float f = vertices[3 * i + d];
+    uint32_t b;
+    std::memcpy(&b, &f, 4);
+    return std::isnan(f) ? 0x7FC00000u : b;
+  };
+  {
+    std::set<std::array<uint32_t, 3>> seen;
+    for (uint64_t i = 0; i < nv; ++i) {
+      if (!seen.insert({vkey(i, 0), vkey(i, 1), vkey(i, 2)}).second) {
+        *kind = 2;
+        detail[0] = i;
+        return ST_OK;
+      }
+    }
+  }
+  const uint64_t F = n_idx / 3;
+  {
+    std::set<std::array<uint32_t, 3>> seen;
+    for (uint64_t f = 0; f < F; ++f) {
+      if (!seen.insert({faces[3 * f], faces[3 * f + 1], faces[3 * f + 2]}).second) {
+        *kind = 3;
+        detail[0] = f;
+        return ST_OK;
+      }
+    }
+  }
+  std::vector<std::pair<uint32_t, uint32_t>> edges;
+  edges.reserve(3 * F);
+  for (uint64_t f = 0; f < F; ++f) {
+    const uint32_t* t = faces + 3 * f;
+    edges.push_back({t[0], t[1]});
+    edges.push_back({t[1], t[2]});
+    edges.push_back({t[2], t[0]});
+  }
+  while (!edges.empty()) {
+    const auto e = edges.back();
+    edges.pop_back();
+    const std::pair<uint32_t, uint32_t> opp{e.second, e.first};
+    if (std::count(edges.begin(), edges.end(), e) > 0) {
+      *kind = 4;
+      detail[0] = e.first;
+      detail[1] = e.second;
+      return ST_OK;
+    }
+    if (std::find(edges.begin(), edges.end(), opp) == edges.end()) {
+      *kind = 5;
+      detail[0] = e.first;
+      detail[1] = e.second;
+      return ST_OK;
+    }
+    edges.erase(std::remove(edges.begin(), edges.end(), opp), edges.end());
+  }
+  *kind = 0;
   return ST_OK;
 }
 

@@ -85,6 +85,13 @@ void orc_grid_cell_center(const float* first_cell, const float* cell_size, const
 int orc_grid_snap_point(const float* first_cell, const float* cell_size,
                         const uint64_t* cell_count, const float* p, uint64_t* cell_out);
 
+/* check_mesh_triangle_list (generate/mesh_check.rs:24-81): kind 0 ok, 1 length
+ * not a multiple of 3, 2 duplicate vertex (detail[0]), 3 duplicate face
+ * (detail[0]), 4 duplicate edge, 5 edge without its reverse (detail[0] ->
+ * detail[1]). */
+int orc_check_mesh_triangle_list(const float* vertices, uint64_t n_vertices, const uint32_t* faces,
+                                 uint64_t n_face_indices, int* kind, uint64_t* detail);
+
 #ifdef __cplusplus
 }
 #endif
