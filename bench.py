@@ -359,6 +359,29 @@ def main():
             acc.close()
         assert int(status.item()) == 0
 
+    # ---- result-side rows on this grid and mesh: the viewer's distance-ordered
+    # cell list (device arrays) and the watertightness check (host arrays)
+    results = {}
+    if not args.no_points:
+        order = torch.empty(N, dtype=torch.int32, device=dev)
+        mm = torch.empty(2, dtype=torch.float32, device=dev)
+        m2s.sort_cells_by_distance_device(out, order, mm, stream)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        flush.fill_(3)
+        e0.record()
+        for _ in range(3):
+            m2s.sort_cells_by_distance_device(out, order, mm, stream)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 3
+        results["cell_order"] = {"cells": N, "ms": ms, "cells_per_s": N / (ms / 1e3)}
+        m2s.check_mesh_triangle_list(v, idx)
+        t0 = time.perf_counter()
+        verdict = m2s.check_mesh_triangle_list(v, idx)
+        results["mesh_check"] = {"faces": T, "ms_host_to_verdict": (time.perf_counter() - t0) * 1e3,
+                                 "watertight": verdict is None}
+
     # ---- CPU baseline (rank 0, N = 1 only): the oracle port on a bounded sample
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -377,7 +400,7 @@ def main():
                            "sign": "Raycast", "parallelism": f"replicas x{world}",
                            "l2": "flushed between steps (256 MiB write, untimed)"},
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": int(launches),
-                "clocks": clk.summary(), "points": points, "wall_s_timed": t_wall}
+                "clocks": clk.summary(), "points": points, "results": results, "wall_s_timed": t_wall}
         print(json.dumps(line), flush=True)
     mesh.close()
     if world > 1:
