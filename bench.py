@@ -34,6 +34,11 @@ N_BRUTE = 65_536
 SEED = 0
 
 
+# DRAM bytes (read + write) of one propagation launch of this workload, from
+# the ncu capture summarised in profiles/k_propagate_star_s6_grid256_dram.md.
+PROPAGATE_DRAM_BYTES = 331_320_000 + 446_240_000
+
+
 def workload():
     from mesh_to_sdf_b200 import synth
 
@@ -276,7 +281,9 @@ def main():
     prop_s = phases["propagation"] / 1e3
     achieved = relax_bytes / prop_s / 1e9 if prop_s > 0 else 0.0
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                "frac": achieved / hbm_peak, "traffic": None,
+                "frac": achieved / hbm_peak, "traffic": PROPAGATE_DRAM_BYTES,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one 256^3 launch "
+                                  "(profiles/k_propagate_star_s6_grid256_dram.md)",
                 "kernel": "k_relax (propagation rounds)", "peak_source": "measured" if peaks else "fallback",
                 "phase_ms": phases, "stats": stats}
 
