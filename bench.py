@@ -34,8 +34,8 @@ N_BRUTE = 65_536
 SEED = 0
 
 
-# DRAM bytes (read + write) of one propagation launch of this workload, from
-# the ncu capture summarised in profiles/k_propagate_star_s6_grid256_dram.md.
+# DRAM bytes (read + write) of one propagation launch of this workload, from an
+# ncu capture of dram__bytes_read.sum and dram__bytes_write.sum (one launch).
 PROPAGATE_DRAM_BYTES = 331_320_000 + 446_240_000
 
 
@@ -282,8 +282,7 @@ def main():
     achieved = relax_bytes / prop_s / 1e9 if prop_s > 0 else 0.0
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                 "frac": achieved / hbm_peak, "traffic": PROPAGATE_DRAM_BYTES,
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one 256^3 launch "
-                                  "(profiles/k_propagate_star_s6_grid256_dram.md)",
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one 256^3 launch",
                 "kernel": "k_relax (propagation rounds)", "peak_source": "measured" if peaks else "fallback",
                 "phase_ms": phases, "stats": stats}
 
