@@ -294,6 +294,12 @@ int m2s_last_grid_stats(uint64_t out[10]);
  * [seeding, propagation, rays, finalize] in milliseconds. */
 void m2s_set_profiling(int enable);
 int m2s_last_grid_phase_ms(float out[4]);
+/* With profiling on, the last grid call on this thread also records its
+ * propagation steps in order: the number of states of each relaxed bucket
+ * list, or (top bit set) the number of far states of each redistribution.
+ * Returns the number of steps recorded (at most 65,536), copying up to
+ * `capacity` of them to `out` (may be NULL). */
+uint32_t m2s_last_grid_round_log(uint32_t* out, uint32_t capacity);
 
 /* Point queries run one thread per query; a query that visits more than
  * `node_visits` LBVH nodes is continued by a whole warp (points deep inside a

@@ -288,6 +288,18 @@ def last_grid_stats():
     return dict(zip(GRID_STATS, (int(x) for x in a)))
 
 
+def last_grid_round_log():
+    """With profiling on: the last grid call's propagation steps in order, as
+    (kind, size) rows — kind 0 a relax round of `size` states, kind 1 a far-list
+    redistribution of `size` states."""
+    L = _lib.lib()
+    n = int(L.m2s_last_grid_round_log(None, 0))
+    a = np.zeros(n, np.uint32)
+    if n:
+        L.m2s_last_grid_round_log(_vp(a), n)
+    return np.stack([(a >> 31).astype(np.int64), (a & 0x7FFFFFFF).astype(np.int64)], 1)
+
+
 def set_profiling(enable: bool):
     """Time grid phases with CUDA events (per thread); see last_grid_phase_ms()."""
     _lib.lib().m2s_set_profiling(1 if enable else 0)

@@ -56,6 +56,7 @@ SIGNATURES = {
     "m2s_last_grid_stats": (I, [P]),
     "m2s_set_profiling": (None, [I]),
     "m2s_last_grid_phase_ms": (I, [P]),
+    "m2s_last_grid_round_log": (ctypes.c_uint32, [P, ctypes.c_uint32]),
     "m2s_set_query_budget": (None, [ctypes.c_uint32]),
     "m2s_query_budget": (ctypes.c_uint32, []),
     "m2s_status_string": (ctypes.c_char_p, [I]),

@@ -11,6 +11,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "m2s_internal.cuh"
 
@@ -21,6 +22,7 @@ thread_local std::string t_last_error;
 thread_local uint64_t t_grid_stats[kGridStats];
 thread_local float t_grid_phase_ms[4];
 thread_local bool t_profile = false;
+thread_local std::vector<uint32_t> t_round_log;
 
 std::mutex g_pool_mu;
 cudaMemPool_t g_pools[64];
@@ -161,6 +163,8 @@ void record_grid_stats(const uint64_t stats[kGridStats]) {
 
 float* grid_phase_slot() { return t_profile ? t_grid_phase_ms : nullptr; }
 
+void record_round_log(const std::vector<uint32_t>& log) { t_round_log = log; }
+
 int dev_alloc(void** p, size_t bytes, cudaStream_t s) {
   cudaMemPool_t pool;
   int st = current_pool(&pool);
@@ -231,6 +235,13 @@ int m2s_last_grid_stats(uint64_t out[10]) {
 }
 
 void m2s_set_profiling(int enable) { t_profile = enable != 0; }
+
+uint32_t m2s_last_grid_round_log(uint32_t* out, uint32_t capacity) {
+  const uint32_t n = (uint32_t)t_round_log.size();
+  if (out)
+    for (uint32_t i = 0; i < n && i < capacity; ++i) out[i] = t_round_log[i];
+  return n;
+}
 
 int m2s_last_grid_phase_ms(float out[4]) {
   if (!out) return M2S_ERR_INVALID_ARGUMENT;

@@ -165,6 +165,7 @@ struct PropState {
   uint32_t round;
   uint32_t far_phases;
   uint32_t max_list;      // largest bucket list relaxed in one round
+  uint32_t log_n;         // steps recorded in the round log
   unsigned long long entries, evals, seeds, ray_hits, skips;
 };
 
@@ -524,7 +525,7 @@ __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ GridS
                                                    unsigned long long* snap_keys, unsigned long long* work_keys,
                                                    uint2* lists, uint32_t cap, uint32_t* spill_lists,
                                                    PropState* st, GridBarrier* bar, uint32_t max_steps,
-                                                   uint32_t* status) {
+                                                   uint32_t* status, uint32_t* round_log, uint32_t log_cap) {
   __shared__ Sched sh;
   __shared__ uint32_t s_touch[kTouchStage];
   __shared__ uint32_t s_ntouch, s_gen;
@@ -543,12 +544,18 @@ __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ GridS
   }
   bool nan = false;
   unsigned long long evals = 0, skips = 0;
-  uint32_t far_phases = 0;
+  uint32_t far_phases = 0, logged = 0;
   bool aborted = false;
   for (uint32_t it = 0;; ++it) {
     if (threadIdx.x == 0) {
       s_ntouch = 0;  // every thread read it in the last commit, before the last barrier
       sh.action = it >= max_steps ? kLimit : next_step(sh, st, lead_block);
+      // Profiling: block 0 records each step, the size of the relaxed list or
+      // (top bit set) the size of the redistributed far list.
+      if (lead_block && round_log && logged < log_cap) {
+        if (sh.action == kRelax) round_log[logged++] = sh.n;
+        else if (sh.action == kRedistribute) round_log[logged++] = 0x80000000u | *(volatile uint32_t*)&st->count[kFar0 + sh.fp];
+      }
     }
     __syncthreads();
     const int action = sh.action;
@@ -721,6 +728,7 @@ __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ GridS
   if (lead_block && threadIdx.x == 0) {
     st->round = sh.round;
     st->far_phases = far_phases;
+    st->log_n = logged;
     st->done = 1;
   }
 }
@@ -891,11 +899,20 @@ struct GridJob::Impl {
   DevBuf<uint32_t> bits;
   DevBuf<uint2> lists;
   DevBuf<uint32_t> touched;
+  DevBuf<uint32_t> round_log;  // profiling only
 };
 
 GridJob::GridJob() : p(new Impl) {}
 GridJob::~GridJob() { delete p; }
 uint32_t GridJob::capacity() const { return p->cap; }
+int GridJob::enable_round_log(uint32_t cap, cudaStream_t s) { return p->round_log.alloc(cap, s); }
+int GridJob::read_round_log(std::vector<uint32_t>* out, uint32_t n, cudaStream_t s) {
+  n = std::min<uint32_t>(n, (uint32_t)p->round_log.n);
+  out->resize(n);
+  if (n) M2S_CUDA(cudaMemcpyAsync(out->data(), p->round_log.p, 4ull * n, cudaMemcpyDeviceToHost, s));
+  M2S_CUDA(cudaStreamSynchronize(s));
+  return M2S_OK;
+}
 void GridJob::set_capacity(uint32_t cap) { p->cap = cap; }
 uint64_t GridJob::cells() const { return p->gs.ncell; }
 unsigned GridJob::cooperative_blocks() const { return p->coop_blocks; }
@@ -1091,8 +1108,10 @@ int GridJob::enqueue(cudaStream_t s, cudaEvent_t* ev) {
     const void* kern = raycast ? propagate_kernel<M2S_SIGN_RAYCAST>(multi) : propagate_kernel<M2S_SIGN_NORMAL>(multi);
     uint32_t max_steps = kMaxSteps;
     const TriRec* tris = J.tris;
-    void* args[] = {&J.gs,        &tris,      &J.snap.p, &J.work.p,  &J.lists.p,   &J.cap,
-                    &J.touched.p, &J.state.p, &J.bar.p,  &max_steps, &J.d_status};
+    uint32_t* log = J.round_log.p;
+    uint32_t log_cap = (uint32_t)J.round_log.n;
+    void* args[] = {&J.gs,     &tris,   &J.snap.p,  &J.work.p,    &J.lists.p, &J.cap, &J.touched.p,
+                    &J.state.p, &J.bar.p, &max_steps, &J.d_status, &log,       &log_cap};
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(J.coop_blocks);
     cfg.blockDim = dim3(256);
@@ -1157,6 +1176,7 @@ int GridJob::read_state(cudaStream_t s, GridRunInfo* info) {
   info->far_phases = h->far_phases;
   info->skips = h->skips;
   info->max_list = h->max_list;
+  info->log_n = h->log_n;
   info->launches = J.launches;
   return M2S_OK;
 }
@@ -1175,6 +1195,7 @@ int run_grid_job(GridJob& job, cudaStream_t s, uint64_t stats[kGridStats], float
   GridRunInfo info;
   uint32_t restarts = 0;
   int st;
+  if (phase_ms && (st = job.enable_round_log(1u << 16, s))) return st;
   for (;; ++restarts) {
     if ((st = job.alloc_lists(s))) return st;
     if ((st = job.enqueue(s, phase_ms ? ev : nullptr))) return st;
@@ -1198,8 +1219,12 @@ int run_grid_job(GridJob& job, cudaStream_t s, uint64_t stats[kGridStats], float
     stats[8] = info.skips;
     stats[9] = info.max_list;
   }
-  if (phase_ms)
+  if (phase_ms) {
     for (int i = 0; i < 4; ++i) M2S_CUDA(cudaEventElapsedTime(&phase_ms[i], ev[i], ev[i + 1]));
+    std::vector<uint32_t> log;
+    if ((st = job.read_round_log(&log, (uint32_t)info.log_n, s))) return st;
+    record_round_log(log);
+  }
   return M2S_OK;
 }
 

@@ -167,7 +167,7 @@ struct GridTuning {
 struct GridRunInfo {
   bool overflow = false;
   uint64_t seeds = 0, rounds = 0, entries = 0, evals = 0, ray_hits = 0, far_phases = 0, launches = 0, skips = 0,
-           max_list = 0;
+           max_list = 0, log_n = 0;
 };
 
 // A set of (mesh, grid) pairs computed together: one cell index space (grid k
@@ -199,6 +199,10 @@ class GridJob {
   void set_cooperative_blocks(unsigned blocks);  // clamped to [1, max_cooperative_blocks()]
   int sign() const;
   uint32_t grids() const;
+  // Profiling: record the size of every relaxed list (and, top bit set, of
+  // every redistributed far list) in a device log of `cap` entries.
+  int enable_round_log(uint32_t cap, cudaStream_t s);
+  int read_round_log(std::vector<uint32_t>* out, uint32_t n, cudaStream_t s);
 
  private:
   struct Impl;
@@ -241,6 +245,7 @@ int require_device();
 // Records the counters / phase times of the last grid call of this thread.
 void record_grid_stats(const uint64_t stats[kGridStats]);
 float* grid_phase_slot();  // NULL unless profiling is on
+void record_round_log(const std::vector<uint32_t>& log);
 int status_from_bits(uint32_t bits);
 
 }  // namespace m2s
