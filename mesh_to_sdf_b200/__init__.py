@@ -481,10 +481,12 @@ class GridPlan:
             pass
 
 
-def set_grid_tuning(blocks_per_sm: int = 0, cells_per_block: int = 2048, wave_cells: int = 4 << 20):
+def set_grid_tuning(blocks_per_sm: int = 0, cells_per_block: int = 2048, wave_cells: int = 4 << 20,
+                    solo_max: int = 64):
     """Process-wide grid propagation knobs (speed only): cooperative blocks per
-    SM, cells per cooperative block, and the most cells a batch job holds."""
-    _lib.lib().m2s_set_grid_tuning(int(blocks_per_sm), int(cells_per_block), int(wave_cells))
+    SM, cells per cooperative block, the most cells a batch job holds, and the
+    largest relax round run on one block (0: none)."""
+    _lib.lib().m2s_set_grid_tuning(int(blocks_per_sm), int(cells_per_block), int(wave_cells), int(solo_max))
 
 
 def clear_grid_autotune():

@@ -150,7 +150,17 @@ __device__ __forceinline__ void cell_coords(const GridK& g, uint32_t cell, int* 
   *x = (int)xx;
 }
 
+// The bucket schedule every block keeps in shared memory.
+struct Sched {
+  uint32_t b, B;
+  uint32_t slot[kRing];
+  uint32_t cur, fp, round, n;
+  uint32_t steps;  // rounds + redistributions so far
+  int action;
+};
+
 struct PropState {
+  Sched handoff;         // the schedule block 0 leaves after relaxing rounds alone
   uint32_t b;            // current bucket
   uint32_t B;            // window: buckets B .. B + kRing - 1
   uint32_t slot[kRing];  // list holding bucket b + k
@@ -467,12 +477,6 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* bar, unsigned int nblo
 constexpr int kTouchStage = 6144;
 constexpr int kUnroll = 2;  // proposals per thread in flight
 
-struct Sched {
-  uint32_t b, B;
-  uint32_t slot[kRing];
-  uint32_t cur, fp, round, n;
-  int action;
-};
 enum { kRelax = 0, kRedistribute = 1, kDone = 2, kLimit = 3 };
 
 // Next step of the schedule, computed by thread 0 of every block from the
@@ -520,42 +524,166 @@ __device__ __forceinline__ int next_step(Sched& sh, PropState* st, bool leader) 
   return kRedistribute;
 }
 
+// Rounds of at most solo_max states are relaxed by block 0 alone, with block
+// barriers only, while the other blocks wait at one grid barrier: a grid-wide
+// round costs two grid barriers and the slowest block, far more than relaxing
+// a few states.  Far-field tails and lateral spreading along a surface make
+// long chains of such rounds.  A solo run lasts at most kSoloRounds rounds so
+// the waiting blocks' bounded wait always ends.  The work of a round does not
+// depend on which threads do it: results are the same either way.
+constexpr uint32_t kSoloRounds = 4096;  // the threshold (default 64 states) is GridTuning::solo_max
+
+// Propose phase of a relax round over list[0..n), proposals t0, t0 + T, ...
+template <int SIGN, bool MULTI>
+__device__ __forceinline__ void relax_propose(const GridSet& gs, const TriRec* __restrict__ tris,
+                                              const unsigned long long* snap_keys, unsigned long long* work_keys,
+                                              const uint2* list, uint32_t n, uint32_t T, uint32_t t0,
+                                              uint32_t* s_touch, uint32_t* s_ntouch, PropState* st, uint32_t parity,
+                                              uint32_t* spill, uint32_t cap, bool& nan, unsigned long long& evals,
+                                              unsigned long long& skips) {
+  // One thread per (state, neighbour) proposal; consecutive threads share a
+  // state, so its entry and triangle loads are warp broadcasts.  kUnroll
+  // independent proposals per iteration keep that many load chains in
+  // flight.  Proposals advance as (state e, neighbour k) pairs without
+  // division: T = 27 * dE + dK.
+  const uint32_t dE = T / 27u, dK = T % 27u;
+  uint32_t e = t0 / 27u, k = t0 % 27u;
+  while (e < n) {
+    bool first[kUnroll];
+    uint32_t jj[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      first[u] = false;
+      jj[u] = 0;
+      const uint32_t eu = e, ku = k;
+      k += dK;
+      e += dE;
+      if (k >= 27u) {
+        k -= 27u;
+        ++e;
+      }
+      if (eu >= n) continue;
+      const uint2 ent = __ldcg(&list[eu]);  // written by other blocks in earlier rounds
+      const uint32_t tri = ent.y;
+      const GridK& g = grid_of_tri<MULTI>(gs, tri);
+      int x, y, z;
+      cell_coords(g, ent.x - g.cell_off, &x, &y, &z);
+      // iproduct!(-1..=1, -1..=1, -1..=1) order (grid.rs:512): x outermost.
+      const int X = x + (int)(ku / 9u) - 1, Y = y + (int)((ku / 3u) % 3u) - 1, Z = z + (int)(ku % 3u) - 1;
+      if (X < 0 || Y < 0 || Z < 0 || X >= g.n[0] || Y >= g.n[1] || Z >= g.n[2]) continue;
+      const uint32_t j = g.cell_off + local_index(g, X, Y, Z);
+      const unsigned long long snap = __ldcg(&snap_keys[j]);
+      // Counted only: such a proposal recomputes the distance the cell holds
+      // and cannot win, but skipping it leaves its lanes idle in the warp.
+      if (key_tri(snap) == tri) ++skips;
+      const TriRec r = tris[tri];
+      const float d = cell_distance<SIGN>(center(g, X, Y, Z), p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
+      ++evals;
+      if (isnan(d)) nan = true;
+      const unsigned long long cand = pack(d, tri);
+      if (beats<SIGN>(cand, snap, &nan)) {
+        first[u] = improve_first<SIGN>(&work_keys[j], cand, snap, &nan);
+        jj[u] = j;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      if (first[u]) {
+        const uint32_t q = atomicAdd(s_ntouch, 1u);
+        if (q < kTouchStage) {
+          s_touch[q] = jj[u];
+        } else {
+          const uint32_t pos = atomicAdd(&st->touched2[parity], 1u);
+          if (pos < cap) spill[pos] = jj[u];
+          else atomicOr(&st->overflow2[parity], 1u);
+        }
+      }
+    }
+  }
+}
+
+// Commit phase: publish each touched cell's round winner to the snapshot and
+// queue (cell, winner) under the winner's bucket.  A block commits the cells
+// it staged; the spill list is shared out as spill_t0 + k * spill_T.
+template <bool MULTI>
+__device__ __forceinline__ void relax_commit(const GridSet& gs, unsigned long long* snap_keys,
+                                             const unsigned long long* work_keys, const uint32_t* s_touch,
+                                             uint32_t nloc, const uint32_t* spill, uint32_t nspill, uint32_t spill_t0,
+                                             uint32_t spill_T, PropState* st, const Sched& sh, uint2* lists,
+                                             uint32_t cap) {
+  for (uint32_t base = 0; base < nloc; base += blockDim.x) {
+    const uint32_t i = base + threadIdx.x;
+    const bool act = i < nloc;
+    uint32_t j = 0, nb = 0;
+    unsigned long long w = KEY_EMPTY;
+    if (act) {
+      j = s_touch[i];
+      w = __ldcg(&work_keys[j]);
+      snap_keys[j] = w;
+      nb = bucket_of(grid_of_tri<MULTI>(gs, key_tri(w)).inv_delta, key_dist(w));
+    }
+    push_entry_warp(st, sh.b, sh.B, sh.slot, sh.fp, lists, cap, act, j, key_tri(w), nb);
+  }
+  for (uint32_t base = spill_t0 - threadIdx.x; base < nspill; base += spill_T) {
+    const uint32_t i = base + threadIdx.x;
+    const bool act = i < nspill;
+    uint32_t j = 0, nb = 0;
+    unsigned long long w = KEY_EMPTY;
+    if (act) {
+      j = __ldcg(&spill[i]);
+      w = __ldcg(&work_keys[j]);
+      snap_keys[j] = w;
+      nb = bucket_of(grid_of_tri<MULTI>(gs, key_tri(w)).inv_delta, key_dist(w));
+    }
+    push_entry_warp(st, sh.b, sh.B, sh.slot, sh.fp, lists, cap, act, j, key_tri(w), nb);
+  }
+}
+
 template <int SIGN, bool MULTI>
 __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ GridSet gs, const TriRec* __restrict__ tris,
                                                    unsigned long long* snap_keys, unsigned long long* work_keys,
                                                    uint2* lists, uint32_t cap, uint32_t* spill_lists,
                                                    PropState* st, GridBarrier* bar, uint32_t max_steps,
-                                                   uint32_t* status, uint32_t* round_log, uint32_t log_cap) {
+                                                   uint32_t* status, uint32_t* round_log, uint32_t log_cap,
+                                                   uint32_t solo_max) {
   __shared__ Sched sh;
   __shared__ uint32_t s_touch[kTouchStage];
-  __shared__ uint32_t s_ntouch, s_gen;
+  __shared__ uint32_t s_ntouch, s_gen, s_pending, s_more, s_runs;
   const unsigned int nblocks = gridDim.x;
   const int lane = threadIdx.x & 31;
   const bool lead_block = blockIdx.x == 0;
   if (threadIdx.x == 0) {
     s_ntouch = 0;
     s_gen = 0;
+    s_pending = 0;
+    s_runs = 0;
     sh.b = st->b;
     sh.B = st->B;
     for (int k = 0; k < kRing; ++k) sh.slot[k] = st->slot[k];
     sh.cur = st->cur;
     sh.fp = st->fp;
     sh.round = 0;
+    sh.steps = 0;
   }
   bool nan = false;
   unsigned long long evals = 0, skips = 0;
   uint32_t far_phases = 0, logged = 0;
   bool aborted = false;
-  for (uint32_t it = 0;; ++it) {
+  // Thread 0: the next step (unless a solo run already chose it), logged by
+  // block 0 when profiling: the relaxed list's size, or (top bit) the far list's.
+  auto step = [&]() {
+    s_ntouch = 0;  // every thread read it in the last commit, before the last barrier
+    sh.action = sh.steps >= max_steps ? kLimit : next_step(sh, st, lead_block);
+    ++sh.steps;
+    if (lead_block && round_log && logged < log_cap) {
+      if (sh.action == kRelax) round_log[logged++] = sh.n;
+      else if (sh.action == kRedistribute) round_log[logged++] = 0x80000000u | *(volatile uint32_t*)&st->count[kFar0 + sh.fp];
+    }
+  };
+  for (;;) {
     if (threadIdx.x == 0) {
-      s_ntouch = 0;  // every thread read it in the last commit, before the last barrier
-      sh.action = it >= max_steps ? kLimit : next_step(sh, st, lead_block);
-      // Profiling: block 0 records each step, the size of the relaxed list or
-      // (top bit set) the size of the redistributed far list.
-      if (lead_block && round_log && logged < log_cap) {
-        if (sh.action == kRelax) round_log[logged++] = sh.n;
-        else if (sh.action == kRedistribute) round_log[logged++] = 0x80000000u | *(volatile uint32_t*)&st->count[kFar0 + sh.fp];
-      }
+      if (s_pending) s_pending = 0;
+      else step();
     }
     __syncthreads();
     const int action = sh.action;
@@ -608,113 +736,64 @@ __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ GridS
       }
       continue;
     }
+    // ---- a relax round: by every block, or by block 0 alone when it is small
+    const bool solo = sh.n <= solo_max;
+    if (solo && !lead_block) {  // wait for block 0's solo run, then take its schedule
+      if (!grid_barrier(bar, nblocks, &s_gen)) {
+        aborted = true;
+        break;
+      }
+      if (threadIdx.x == 0) {
+        const volatile uint32_t* src = (const volatile uint32_t*)&st->handoff;
+        uint32_t* dst = (uint32_t*)&sh;
+        for (uint32_t w = 0; w < sizeof(Sched) / 4; ++w) dst[w] = src[w];
+        s_pending = 1;
+      }
+      continue;
+    }
     const uint32_t parity = sh.round & 1u;
     uint32_t* spill = spill_lists + (unsigned long long)parity * cap;
-    // ---- propose: every state of the bucket evaluates its triangle at the 27
-    // cells of its 3x3x3 block; a proposal that beats the cell's value at the
-    // start of the round enters the working value (atomic minimum) and the
-    // first such proposal stages the cell as touched by this block.
     const uint32_t n = min(sh.n, cap);
-    const uint2* list = lists + (unsigned long long)sh.cur * cap;
-    // One thread per (state, neighbour) proposal; consecutive threads share a
-    // state, so its entry and triangle loads are warp broadcasts.  kUnroll
-    // independent proposals per iteration keep that many load chains in
-    // flight.  Thread t takes proposals t, t + T, t + 2T, ... as (state e,
-    // neighbour k) pairs advanced without division: T = 27 * dE + dK.
-    const uint32_t T = gridDim.x * blockDim.x;
-    const uint32_t dE = T / 27u, dK = T % 27u;
-    const uint32_t t0 = blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t e = t0 / 27u, k = t0 % 27u;
-    while (e < n) {
-      bool first[kUnroll];
-      uint32_t jj[kUnroll];
-#pragma unroll
-      for (int u = 0; u < kUnroll; ++u) {
-        first[u] = false;
-        jj[u] = 0;
-        const uint32_t eu = e, ku = k;
-        k += dK;
-        e += dE;
-        if (k >= 27u) {
-          k -= 27u;
-          ++e;
-        }
-        if (eu >= n) continue;
-        const uint2 ent = __ldcg(&list[eu]);  // written by other blocks in earlier rounds
-        const uint32_t tri = ent.y;
-        const GridK& g = grid_of_tri<MULTI>(gs, tri);
-        int x, y, z;
-        cell_coords(g, ent.x - g.cell_off, &x, &y, &z);
-        // iproduct!(-1..=1, -1..=1, -1..=1) order (grid.rs:512): x outermost.
-        const int X = x + (int)(ku / 9u) - 1, Y = y + (int)((ku / 3u) % 3u) - 1, Z = z + (int)(ku % 3u) - 1;
-        if (X < 0 || Y < 0 || Z < 0 || X >= g.n[0] || Y >= g.n[1] || Z >= g.n[2]) continue;
-        const uint32_t j = g.cell_off + local_index(g, X, Y, Z);
-        const unsigned long long snap = __ldcg(&snap_keys[j]);
-        // Counted only: such a proposal recomputes the distance the cell holds
-        // and cannot win, but skipping it leaves its lanes idle in the warp.
-        if (key_tri(snap) == tri) ++skips;
-        const TriRec r = tris[tri];
-        const float d = cell_distance<SIGN>(center(g, X, Y, Z), p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
-        ++evals;
-        if (isnan(d)) nan = true;
-        const unsigned long long cand = pack(d, tri);
-        if (beats<SIGN>(cand, snap, &nan)) {
-          first[u] = improve_first<SIGN>(&work_keys[j], cand, snap, &nan);
-          jj[u] = j;
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < kUnroll; ++u) {
-        if (first[u]) {
-          const uint32_t q = atomicAdd(&s_ntouch, 1u);
-          if (q < kTouchStage) {
-            s_touch[q] = jj[u];
-          } else {
-            const uint32_t pos = atomicAdd(&st->touched2[parity], 1u);
-            if (pos < cap) spill[pos] = jj[u];
-            else atomicOr(&st->overflow2[parity], 1u);
-          }
-        }
-      }
-    }
+    const uint32_t T = solo ? blockDim.x : gridDim.x * blockDim.x;
+    const uint32_t t0 = solo ? threadIdx.x : blockIdx.x * blockDim.x + threadIdx.x;
+    relax_propose<SIGN, MULTI>(gs, tris, snap_keys, work_keys, lists + (unsigned long long)sh.cur * cap, n, T, t0,
+                               s_touch, &s_ntouch, st, parity, spill, cap, nan, evals, skips);
     if (lead_block && threadIdx.x == 0) atomicAdd(&st->entries, (unsigned long long)n);
-    if (!grid_barrier(bar, nblocks, &s_gen)) {
+    if (solo) {
+      __syncthreads();
+    } else if (!grid_barrier(bar, nblocks, &s_gen)) {
       aborted = true;
       break;
     }
-    // ---- commit: each touched cell publishes its round winner to the snapshot
-    // and queues (cell, winning triangle) under the winner's distance bucket.
-    // A block commits the cells it staged; all blocks share the spill list.
     if (lead_block && threadIdx.x == 0) st->touched2[parity ^ 1u] = 0;
     const uint32_t nspill = min(*(volatile uint32_t*)&st->touched2[parity], cap);
-    const uint32_t nloc = min(s_ntouch, (uint32_t)kTouchStage);
-    for (uint32_t base = 0; base < nloc; base += blockDim.x) {
-      const uint32_t i = base + threadIdx.x;
-      const bool act = i < nloc;
-      uint32_t j = 0, nb = 0;
-      unsigned long long w = KEY_EMPTY;
-      if (act) {
-        j = s_touch[i];
-        w = __ldcg(&work_keys[j]);
-        snap_keys[j] = w;
-        nb = bucket_of(grid_of_tri<MULTI>(gs, key_tri(w)).inv_delta, key_dist(w));
+    relax_commit<MULTI>(gs, snap_keys, work_keys, s_touch, min(s_ntouch, (uint32_t)kTouchStage), spill, nspill, t0,
+                        T, st, sh, lists, cap);
+    if (!solo) {
+      if (!grid_barrier(bar, nblocks, &s_gen)) {
+        aborted = true;
+        break;
       }
-      push_entry_warp(st, sh.b, sh.B, sh.slot, sh.fp, lists, cap, act, j, key_tri(w), nb);
+      continue;
     }
-    for (uint32_t base = blockIdx.x * blockDim.x; base < nspill; base += gridDim.x * blockDim.x) {
-      const uint32_t i = base + threadIdx.x;
-      const bool act = i < nspill;
-      uint32_t j = 0, nb = 0;
-      unsigned long long w = KEY_EMPTY;
-      if (act) {
-        j = __ldcg(&spill[i]);
-        w = __ldcg(&work_keys[j]);
-        snap_keys[j] = w;
-        nb = bucket_of(grid_of_tri<MULTI>(gs, key_tri(w)).inv_delta, key_dist(w));
+    // Solo: block 0 chooses the next step at once; it goes on alone while the
+    // rounds stay small, else hands the schedule (next action included) to the
+    // other blocks at the barrier they wait at.
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      step();
+      ++s_runs;
+      s_more = sh.action == kRelax && sh.n <= solo_max && s_runs < kSoloRounds;
+      if (!s_more) {
+        volatile uint32_t* dst = (volatile uint32_t*)&st->handoff;
+        const uint32_t* src = (const uint32_t*)&sh;
+        for (uint32_t w = 0; w < sizeof(Sched) / 4; ++w) dst[w] = src[w];
+        s_runs = 0;
       }
-      push_entry_warp(st, sh.b, sh.B, sh.slot, sh.fp, lists, cap, act, j, key_tri(w), nb);
+      s_pending = 1;
     }
-    if (!grid_barrier(bar, nblocks, &s_gen)) {
+    __syncthreads();
+    if (!s_more && !grid_barrier(bar, nblocks, &s_gen)) {
       aborted = true;
       break;
     }
@@ -886,6 +965,7 @@ struct GridJob::Impl {
   uint32_t cap = 0;
   unsigned coop_blocks = 0;
   unsigned coop_max = 0;
+  uint32_t solo_max = 64;
   unsigned long long ray_words = 0;
   uint64_t launches = 0;
   DevBuf<TriRec> comb_tris;
@@ -1041,6 +1121,7 @@ int GridJob::prepare(const MeshView* meshes, uint32_t n, const GridDesc* gds, in
     return st;
   if (sign == M2S_SIGN_RAYCAST && (st = J.bits.alloc(woff, s))) return st;
   J.cap = tune.list_capacity ? tune.list_capacity : default_list_capacity(N);
+  J.solo_max = tune.solo_max;
   // Cooperative grid: co-resident blocks, fewer for small jobs (a barrier
   // over fewer blocks is faster and a small bucket does not fill many).
   const void* kern = sign == M2S_SIGN_RAYCAST ? propagate_kernel<M2S_SIGN_RAYCAST>(J.multi)
@@ -1110,8 +1191,8 @@ int GridJob::enqueue(cudaStream_t s, cudaEvent_t* ev) {
     const TriRec* tris = J.tris;
     uint32_t* log = J.round_log.p;
     uint32_t log_cap = (uint32_t)J.round_log.n;
-    void* args[] = {&J.gs,     &tris,   &J.snap.p,  &J.work.p,    &J.lists.p, &J.cap, &J.touched.p,
-                    &J.state.p, &J.bar.p, &max_steps, &J.d_status, &log,       &log_cap};
+    void* args[] = {&J.gs,     &tris,   &J.snap.p,  &J.work.p,    &J.lists.p, &J.cap,     &J.touched.p,
+                    &J.state.p, &J.bar.p, &max_steps, &J.d_status, &log,       &log_cap, &J.solo_max};
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(J.coop_blocks);
     cfg.blockDim = dim3(256);

@@ -129,12 +129,13 @@ def test_launch_shape_never_changes_results():
     meshes, grids = _workload(sign, seed=7)
     ref, _, _ = _batch(meshes, grids, sign)
     try:
-        # blocks per SM, cells per block, and wave size (1 cell: every grid in
-        # a job of its own; 1 << 30: the whole batch in one job)
-        for bps, cpb, wave in [(1, 2048, 4 << 20), (0, 64, 1), (2, 1 << 20, 1 << 30), (0, 2048, 20000)]:
-            m2s.set_grid_tuning(bps, cpb, wave)
+        # wave size 1 cell: every grid in a job of its own; 1 << 30: the whole batch in one job;
+        # blocks per SM, cells per block, wave size, solo rounds (0: every round on every block)
+        for bps, cpb, wave, solo in [(1, 2048, 4 << 20, 64), (0, 64, 1, 0), (2, 1 << 20, 1 << 30, 1000),
+                                     (0, 2048, 20000, 0), (0, 2048, 1 << 30, 0), (0, 2048, 1 << 30, 10)]:
+            m2s.set_grid_tuning(bps, cpb, wave, solo)
             got, _, _ = _batch(meshes, grids, sign)
-            assert np.array_equal(bits(got), bits(ref)), (bps, cpb, wave)
+            assert np.array_equal(bits(got), bits(ref)), (bps, cpb, wave, solo)
     finally:
         m2s.set_grid_tuning()
 

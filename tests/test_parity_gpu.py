@@ -346,3 +346,21 @@ def test_grid_coarse_mesh_far_states(orc):
     gpu, ref1, ref8, nn = grid_report(orc, v, idx, grid, S.Raycast)
     assert m2s.last_grid_stats()["far_phases"] > 0
     check_grid(gpu, ref1, ref8, nn, float(np.linalg.norm(grid.cell_size)), S.Raycast, "coarse")
+
+
+def test_grid_solo_rounds_do_not_change_results():
+    # small rounds relaxed by one block give the same bits as every block
+    # relaxing every round (terrain: thousands of tiny rounds; a coarse sphere)
+    cases = [(synth.terrain(64, seed=4), True, S.Normal), (synth.icosphere(1), False, S.Raycast)]
+    try:
+        for (v, idx), strip, sign in cases:
+            lo, hi = synth.padded_bbox(v)
+            grid = m2s.Grid.from_bounding_box(lo, hi, [40, 44, 36])
+            topo = T.TriangleStrip(idx) if strip else T.TriangleList(idx)
+            outs = []
+            for solo in (0, 64, 4096):
+                m2s.set_grid_tuning(solo_max=solo)
+                outs.append(m2s.generate_grid_sdf(v, topo, grid, sign))
+            assert np.array_equal(bits(outs[0]), bits(outs[1])) and np.array_equal(bits(outs[0]), bits(outs[2]))
+    finally:
+        m2s.set_grid_tuning()
