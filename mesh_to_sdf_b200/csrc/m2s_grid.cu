@@ -434,9 +434,18 @@ __device__ __forceinline__ void st_release(unsigned int* p, unsigned int v) {
 // passes the same sequence of barriers, so each keeps the generation count in
 // shared memory and waits for the global one to reach its next value: an
 // arrival costs the group atomic, the top atomic for the last of a group, and
-// the wait.  The wait is bounded: after kBarrierPolls polls it raises `abort`,
-// which makes every block leave the kernel at its next barrier.
-constexpr uint32_t kBarrierPolls = 1u << 22;  // about a second of polling
+// the wait.  A wait spins briefly, then backs off with __nanosleep so waiting
+// blocks leave the memory system to the ones working (block 0 alone during a
+// solo run).  It is bounded in time: after kBarrierTimeoutNs it raises
+// `abort`, which makes every block leave the kernel at its next barrier.
+constexpr uint64_t kBarrierTimeoutNs = 2000000000ull;  // two seconds
+constexpr uint32_t kBarrierSpins = 64;
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 __device__ __forceinline__ bool grid_barrier(GridBarrier* bar, unsigned int nblocks, unsigned int* gen) {
   __shared__ int ok;
@@ -456,9 +465,13 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* bar, unsigned int nblo
       st_release(&bar->gen, target);
     } else {
       uint32_t polls = 0;
+      uint64_t t0 = 0;
       while (ld_acquire(&bar->gen) != target) {
         if (ld_acquire(&bar->abort)) break;
-        if (++polls > kBarrierPolls) {
+        if (++polls < kBarrierSpins) continue;
+        if (polls == kBarrierSpins) t0 = global_ns();
+        __nanosleep(256);
+        if (global_ns() - t0 > kBarrierTimeoutNs) {
           atomicExch(&bar->abort, 1u);
           break;
         }
@@ -531,7 +544,7 @@ __device__ __forceinline__ int next_step(Sched& sh, PropState* st, bool leader) 
 // long chains of such rounds.  A solo run lasts at most kSoloRounds rounds so
 // the waiting blocks' bounded wait always ends.  The work of a round does not
 // depend on which threads do it: results are the same either way.
-constexpr uint32_t kSoloRounds = 4096;  // the threshold (default 64 states) is GridTuning::solo_max
+constexpr uint32_t kSoloRounds = 1024;  // the threshold (default 64 states) is GridTuning::solo_max
 
 // Propose phase of a relax round over list[0..n), proposals t0, t0 + T, ...
 template <int SIGN, bool MULTI>
