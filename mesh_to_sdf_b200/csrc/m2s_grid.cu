@@ -661,7 +661,7 @@ __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ GridS
                                                    uint32_t solo_max) {
   __shared__ Sched sh;
   __shared__ uint32_t s_touch[kTouchStage];
-  __shared__ uint32_t s_ntouch, s_gen, s_pending, s_more, s_runs;
+  __shared__ uint32_t s_ntouch, s_gen, s_pending, s_more, s_runs, s_solo_run;
   const unsigned int nblocks = gridDim.x;
   const int lane = threadIdx.x & 31;
   const bool lead_block = blockIdx.x == 0;
@@ -670,6 +670,7 @@ __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ GridS
     s_gen = 0;
     s_pending = 0;
     s_runs = 0;
+    s_solo_run = 0;
     sh.b = st->b;
     sh.B = st->B;
     for (int k = 0; k < kRing; ++k) sh.slot[k] = st->slot[k];
@@ -751,18 +752,28 @@ __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ GridS
     }
     // ---- a relax round: by every block, or by block 0 alone when it is small
     const bool solo = sh.n <= solo_max;
-    if (solo && !lead_block) {  // wait for block 0's solo run, then take its schedule
+    if (solo && !s_solo_run) {
+      // A solo run starts.  Block 0 will change list counts at once (pushes,
+      // and emptying the list it relaxes at its next step), so every block
+      // first finishes reading this step's counts.
       if (!grid_barrier(bar, nblocks, &s_gen)) {
         aborted = true;
         break;
       }
-      if (threadIdx.x == 0) {
-        const volatile uint32_t* src = (const volatile uint32_t*)&st->handoff;
-        uint32_t* dst = (uint32_t*)&sh;
-        for (uint32_t w = 0; w < sizeof(Sched) / 4; ++w) dst[w] = src[w];
-        s_pending = 1;
+      if (!lead_block) {  // wait for the run to end, then take block 0's schedule
+        if (!grid_barrier(bar, nblocks, &s_gen)) {
+          aborted = true;
+          break;
+        }
+        if (threadIdx.x == 0) {
+          const volatile uint32_t* src = (const volatile uint32_t*)&st->handoff;
+          uint32_t* dst = (uint32_t*)&sh;
+          for (uint32_t w = 0; w < sizeof(Sched) / 4; ++w) dst[w] = src[w];
+          s_pending = 1;
+        }
+        continue;
       }
-      continue;
+      if (threadIdx.x == 0) s_solo_run = 1;  // read again only after later block barriers
     }
     const uint32_t parity = sh.round & 1u;
     uint32_t* spill = spill_lists + (unsigned long long)parity * cap;
@@ -802,6 +813,7 @@ __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ GridS
         const uint32_t* src = (const uint32_t*)&sh;
         for (uint32_t w = 0; w < sizeof(Sched) / 4; ++w) dst[w] = src[w];
         s_runs = 0;
+        s_solo_run = 0;
       }
       s_pending = 1;
     }
