@@ -166,3 +166,24 @@ def test_batch_rejects_bad_grids():
     with pytest.raises(m2s.M2SError) as e:
         m2s.grid_sdf_batch_device([mesh, mesh], [m2s.Grid.new([0, 0, 0], [0.1] * 3, [4, 4, 4]), bad], S.Raycast, out)
     assert e.value.status == 1
+
+
+def test_many_small_rounds_at_full_occupancy_are_deterministic():
+    # coarse spheres in fine grids chain many small rounds (solo runs of block
+    # 0 while every other block waits); with as many blocks as fit, results
+    # must not depend on the launch shape or on solo runs
+    items = synth.batch_meshes(40, seed=21, subdivs=(1, 2, 3), edges=(24, 48, 64, 80))
+    sign = S.Raycast
+    meshes = [m2s.build_sdf_acceleration(v, T.TriangleList(i), A.none(sign)) for v, i, *_ in items]
+    grids = [m2s.Grid.from_bounding_box(lo, hi, [e, e, e]) for _, _, lo, hi, e in items]
+    ref = None
+    try:
+        for bps, cpb, wave, solo in [(0, 2048, 4 << 20, 0), (0, 1, 4 << 20, 64), (0, 1, 1 << 30, 64),
+                                     (3, 1, 1 << 20, 227), (0, 64, 4 << 20, 8), (1, 1, 4 << 20, 64)]:
+            m2s.set_grid_tuning(bps, cpb, wave, solo)
+            got, _, stats = _batch(meshes, grids, sign)
+            if ref is None:
+                ref = got
+            assert np.array_equal(bits(got), bits(ref)), (bps, cpb, wave, solo)
+    finally:
+        m2s.set_grid_tuning()
