@@ -580,6 +580,19 @@ def serving_workload(args):
     ids = [mid for mid, _ in ids]
     rng = np.random.default_rng(SEED + 7)
     unit = torch.from_numpy(rng.random((1_000_000, 3), dtype=np.float32)).pin_memory()
+    # Warm-up, untimed: every kernel loaded once and the memory pool grown to
+    # its working size (a pool growth may synchronise the device), as a
+    # server does before it takes traffic.
+    warm = []
+    wq = unit.numpy()
+    wo = torch.empty(256 ** 3, dtype=torch.float32).pin_memory().numpy()
+    for j, e in enumerate((64, 96, 128, 192, 256, 256)):
+        lo, hi = boxes[j]
+        warm.append(srv.submit_grid(ids[j], m2s.Grid.from_bounding_box(lo, hi, [e, e, e]), S.Raycast, wo[:e ** 3]))
+        warm.append(srv.submit_points(ids[j], wq, wo[:len(wq)]))
+        for t in warm:
+            assert srv.wait(t)[0] == 0
+        warm = []
     rates = [float(r) for r in args.rates.split(",") if r]
     n_req = args.requests
     lines = []
