@@ -585,11 +585,12 @@ def serving_workload(args):
     # server does before it takes traffic.
     warm = []
     wq = unit.numpy()
-    wo = torch.empty(256 ** 3, dtype=torch.float32).pin_memory().numpy()
+    wg = torch.empty(256 ** 3, dtype=torch.float32).pin_memory().numpy()
+    wp = torch.empty(len(wq), dtype=torch.float32).pin_memory().numpy()
     for j, e in enumerate((64, 96, 128, 192, 256, 256)):
         lo, hi = boxes[j]
-        warm.append(srv.submit_grid(ids[j], m2s.Grid.from_bounding_box(lo, hi, [e, e, e]), S.Raycast, wo[:e ** 3]))
-        warm.append(srv.submit_points(ids[j], wq, wo[:len(wq)]))
+        warm.append(srv.submit_grid(ids[j], m2s.Grid.from_bounding_box(lo, hi, [e, e, e]), S.Raycast, wg[:e ** 3]))
+        warm.append(srv.submit_points(ids[j], wq, wp))
         for t in warm:
             assert srv.wait(t)[0] == 0
         warm = []
