@@ -354,7 +354,16 @@ __global__ void k_state_init(PropState* st) {
 // (buckets at or below the current one to the list relaxed next), beyond it to
 // the far list fp.  Lanes of a warp that target the same list share one
 // atomicAdd.  Must be called by all 32 lanes; `act` says whether this lane pushes.
-__device__ __forceinline__ void push_entry_warp(PropState* st, uint32_t b, uint32_t B, const uint32_t* slots,
+// Where the list counts, far-list minima and the push-overflow flag live: in
+// PropState (global), or in block 0's shared memory during a solo run.
+struct Counters {
+  uint32_t* count;     // kLists
+  uint32_t* far_min;   // 2
+  uint32_t* overflow;  // push overflow
+};
+__device__ __forceinline__ Counters global_counters(PropState* st) { return {st->count, st->far_min, &st->overflow}; }
+
+__device__ __forceinline__ void push_entry_warp(const Counters& ct, uint32_t b, uint32_t B, const uint32_t* slots,
                                                 uint32_t fp, uint2* lists, uint32_t cap, bool act, uint32_t cell,
                                                 uint32_t tri, uint32_t nb) {
   const int lane = threadIdx.x & 31;
@@ -364,19 +373,19 @@ __device__ __forceinline__ void push_entry_warp(PropState* st, uint32_t b, uint3
   const uint32_t farmask = __ballot_sync(0xFFFFFFFFu, far);
   if (farmask) {
     const uint32_t m = __reduce_min_sync(0xFFFFFFFFu, far ? nb : kNoBucket);
-    if (lane == __ffs(farmask) - 1) atomicMin(&st->far_min[fp], m);
+    if (lane == __ffs(farmask) - 1) atomicMin(&ct.far_min[fp], m);
   }
   const uint32_t group = __match_any_sync(0xFFFFFFFFu, slot);
   if (!act) return;
   const int leader = __ffs(group) - 1;
   uint32_t base = 0;
-  if (lane == leader) base = atomicAdd(&st->count[slot], (uint32_t)__popc(group));
+  if (lane == leader) base = atomicAdd(&ct.count[slot], (uint32_t)__popc(group));
   base = __shfl_sync(group, base, leader);
   const uint32_t pos = base + __popc(group & ((1u << lane) - 1u));
   if (pos < cap)
     lists[(unsigned long long)slot * cap + pos] = make_uint2(cell, tri);
   else
-    atomicOr(&st->overflow, 1u);  // the job is rerun with larger lists
+    atomicOr(ct.overflow, 1u);  // the job is rerun with larger lists
 }
 
 // Initial states: every seeded cell with its seed triangle (window 0..15).
@@ -394,7 +403,7 @@ __global__ void k_collect(const __grid_constant__ GridSet gs, const unsigned lon
       const float inv = MULTI ? gs.table[sc.at(gs.cell_off, gs.ngrids, (uint32_t)i)].inv_delta : gs.g0.inv_delta;
       nb = bucket_of(inv, key_dist(k));
     }
-    push_entry_warp(st, 0, 0, st->slot, 0, lists, cap, act, (uint32_t)i, key_tri(k), nb);
+    push_entry_warp(global_counters(st), 0, 0, st->slot, 0, lists, cap, act, (uint32_t)i, key_tri(k), nb);
   }
 }
 
@@ -497,17 +506,18 @@ enum { kRelax = 0, kRedistribute = 1, kDone = 2, kLimit = 3 };
 // push before it).  All counts it may need are loaded together, one round trip.
 // Block 0 also empties the list relaxed last round, which no block reads here
 // and which receives pushes only after the next barrier.
-__device__ __forceinline__ int next_step(Sched& sh, PropState* st, bool leader) {
+__device__ __forceinline__ int next_step(Sched& sh, const Counters& ct, uint32_t spill_overflow, PropState* st,
+                                         bool leader) {
   uint32_t c[kRing];
 #pragma unroll
-  for (int k = 0; k < kRing; ++k) c[k] = *(volatile uint32_t*)&st->count[sh.slot[k]];
+  for (int k = 0; k < kRing; ++k) c[k] = *(volatile uint32_t*)&ct.count[sh.slot[k]];
   // Only values no block can change before every block has passed this step:
   // list counts (pushes come after the next barrier), the push overflow flag
   // and the spill overflow flag of the round just finished (the next propose
   // phase writes the other parity).
-  const uint32_t overflow = *(volatile uint32_t*)&st->overflow | *(volatile uint32_t*)&st->overflow2[sh.round & 1u];
-  const uint32_t far_n = *(volatile uint32_t*)&st->count[kFar0 + sh.fp];
-  const uint32_t far_b = *(volatile uint32_t*)&st->far_min[sh.fp];
+  const uint32_t overflow = *(volatile uint32_t*)ct.overflow | spill_overflow;
+  const uint32_t far_n = *(volatile uint32_t*)&ct.count[kFar0 + sh.fp];
+  const uint32_t far_b = *(volatile uint32_t*)&ct.far_min[sh.fp];
   if (overflow) return kDone;
   // slot[q] holds bucket b + q; the window ends at bucket B + kRing - 1.
   int q = 0;
@@ -525,7 +535,7 @@ __device__ __forceinline__ int next_step(Sched& sh, PropState* st, bool leader) 
     sh.n = c[q];
     sh.round += 1;
     if (leader) {
-      st->count[consumed] = 0;
+      ct.count[consumed] = 0;
       st->max_list = max(st->max_list, c[q]);
     }
     return kRelax;
@@ -622,7 +632,7 @@ template <bool MULTI>
 __device__ __forceinline__ void relax_commit(const GridSet& gs, unsigned long long* snap_keys,
                                              const unsigned long long* work_keys, const uint32_t* s_touch,
                                              uint32_t nloc, const uint32_t* spill, uint32_t nspill, uint32_t spill_t0,
-                                             uint32_t spill_T, PropState* st, const Sched& sh, uint2* lists,
+                                             uint32_t spill_T, const Counters& ct, const Sched& sh, uint2* lists,
                                              uint32_t cap) {
   for (uint32_t base = 0; base < nloc; base += blockDim.x) {
     const uint32_t i = base + threadIdx.x;
@@ -635,7 +645,7 @@ __device__ __forceinline__ void relax_commit(const GridSet& gs, unsigned long lo
       snap_keys[j] = w;
       nb = bucket_of(grid_of_tri<MULTI>(gs, key_tri(w)).inv_delta, key_dist(w));
     }
-    push_entry_warp(st, sh.b, sh.B, sh.slot, sh.fp, lists, cap, act, j, key_tri(w), nb);
+    push_entry_warp(ct, sh.b, sh.B, sh.slot, sh.fp, lists, cap, act, j, key_tri(w), nb);
   }
   for (uint32_t base = spill_t0 - threadIdx.x; base < nspill; base += spill_T) {
     const uint32_t i = base + threadIdx.x;
@@ -648,12 +658,12 @@ __device__ __forceinline__ void relax_commit(const GridSet& gs, unsigned long lo
       snap_keys[j] = w;
       nb = bucket_of(grid_of_tri<MULTI>(gs, key_tri(w)).inv_delta, key_dist(w));
     }
-    push_entry_warp(st, sh.b, sh.B, sh.slot, sh.fp, lists, cap, act, j, key_tri(w), nb);
+    push_entry_warp(ct, sh.b, sh.B, sh.slot, sh.fp, lists, cap, act, j, key_tri(w), nb);
   }
 }
 
 template <int SIGN, bool MULTI>
-__global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ GridSet gs, const TriRec* __restrict__ tris,
+__global__ void __launch_bounds__(256, 4) k_propagate(const __grid_constant__ GridSet gs, const TriRec* __restrict__ tris,
                                                    unsigned long long* snap_keys, unsigned long long* work_keys,
                                                    uint2* lists, uint32_t cap, uint32_t* spill_lists,
                                                    PropState* st, GridBarrier* bar, uint32_t max_steps,
@@ -662,6 +672,11 @@ __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ GridS
   __shared__ Sched sh;
   __shared__ uint32_t s_touch[kTouchStage];
   __shared__ uint32_t s_ntouch, s_gen, s_pending, s_more, s_runs, s_solo_run;
+  __shared__ uint32_t s_count[kLists], s_far_min[2], s_overflow;  // block 0's counters during a solo run
+  // (built where used, so no pointer stays live across the propose loop)
+  auto counters = [&](bool shared_ones) {
+    return shared_ones ? Counters{s_count, s_far_min, &s_overflow} : global_counters(st);
+  };
   const unsigned int nblocks = gridDim.x;
   const int lane = threadIdx.x & 31;
   const bool lead_block = blockIdx.x == 0;
@@ -687,11 +702,13 @@ __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ GridS
   // block 0 when profiling: the relaxed list's size, or (top bit) the far list's.
   auto step = [&]() {
     s_ntouch = 0;  // every thread read it in the last commit, before the last barrier
-    sh.action = sh.steps >= max_steps ? kLimit : next_step(sh, st, lead_block);
+    const bool in_run = lead_block && s_solo_run;
+    const uint32_t spill_ov = in_run ? 0u : *(volatile uint32_t*)&st->overflow2[sh.round & 1u];
+    sh.action = sh.steps >= max_steps ? kLimit : next_step(sh, counters(in_run), spill_ov, st, lead_block);
     ++sh.steps;
     if (lead_block && round_log && logged < log_cap) {
       if (sh.action == kRelax) round_log[logged++] = sh.n;
-      else if (sh.action == kRedistribute) round_log[logged++] = 0x80000000u | *(volatile uint32_t*)&st->count[kFar0 + sh.fp];
+      else if (sh.action == kRedistribute) round_log[logged++] = 0x80000000u | counters(in_run).count[kFar0 + sh.fp];
     }
   };
   for (;;) {
@@ -734,7 +751,7 @@ __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ GridS
           const float d = cell_distance<SIGN>(center(g, x, y, z), p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
           nb = bucket_of(g.inv_delta, d);
         }
-        push_entry_warp(st, sh.b, sh.B, sh.slot, sh.fp ^ 1u, lists, cap, act, ent.x, ent.y, nb);
+        push_entry_warp(global_counters(st), sh.b, sh.B, sh.slot, sh.fp ^ 1u, lists, cap, act, ent.x, ent.y, nb);
       }
       if (!grid_barrier(bar, nblocks, &s_gen)) {
         aborted = true;
@@ -773,7 +790,16 @@ __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ GridS
         }
         continue;
       }
-      if (threadIdx.x == 0) s_solo_run = 1;  // read again only after later block barriers
+      if (threadIdx.x == 0) {
+        // Block 0 alone pushes during the run: it keeps the counters in shared
+        // memory and writes them back when it hands the schedule over.
+        s_solo_run = 1;  // read again only after later block barriers
+        for (int k = 0; k < kLists; ++k) s_count[k] = *(volatile uint32_t*)&st->count[k];
+        s_far_min[0] = *(volatile uint32_t*)&st->far_min[0];
+        s_far_min[1] = *(volatile uint32_t*)&st->far_min[1];
+        s_overflow = *(volatile uint32_t*)&st->overflow | *(volatile uint32_t*)&st->overflow2[0] |
+                     *(volatile uint32_t*)&st->overflow2[1];
+      }
     }
     const uint32_t parity = sh.round & 1u;
     uint32_t* spill = spill_lists + (unsigned long long)parity * cap;
@@ -790,9 +816,10 @@ __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ GridS
       break;
     }
     if (lead_block && threadIdx.x == 0) st->touched2[parity ^ 1u] = 0;
-    const uint32_t nspill = min(*(volatile uint32_t*)&st->touched2[parity], cap);
+    // A solo round (at most solo_max <= kTouchStage / 27 states) never spills.
+    const uint32_t nspill = solo ? 0u : min(*(volatile uint32_t*)&st->touched2[parity], cap);
     relax_commit<MULTI>(gs, snap_keys, work_keys, s_touch, min(s_ntouch, (uint32_t)kTouchStage), spill, nspill, t0,
-                        T, st, sh, lists, cap);
+                        T, counters(solo), sh, lists, cap);
     if (!solo) {
       if (!grid_barrier(bar, nblocks, &s_gen)) {
         aborted = true;
@@ -809,6 +836,10 @@ __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ GridS
       ++s_runs;
       s_more = sh.action == kRelax && sh.n <= solo_max && s_runs < kSoloRounds;
       if (!s_more) {
+        for (int k = 0; k < kLists; ++k) st->count[k] = s_count[k];
+        st->far_min[0] = s_far_min[0];
+        st->far_min[1] = s_far_min[1];
+        if (s_overflow) st->overflow = 1u;
         volatile uint32_t* dst = (volatile uint32_t*)&st->handoff;
         const uint32_t* src = (const uint32_t*)&sh;
         for (uint32_t w = 0; w < sizeof(Sched) / 4; ++w) dst[w] = src[w];
@@ -1146,7 +1177,7 @@ int GridJob::prepare(const MeshView* meshes, uint32_t n, const GridDesc* gds, in
     return st;
   if (sign == M2S_SIGN_RAYCAST && (st = J.bits.alloc(woff, s))) return st;
   J.cap = tune.list_capacity ? tune.list_capacity : default_list_capacity(N);
-  J.solo_max = tune.solo_max;
+  J.solo_max = std::min<uint32_t>(tune.solo_max, kTouchStage / 27);  // a solo round never spills
   // Cooperative grid: co-resident blocks, fewer for small jobs (a barrier
   // over fewer blocks is faster and a small bucket does not fill many).
   const void* kern = sign == M2S_SIGN_RAYCAST ? propagate_kernel<M2S_SIGN_RAYCAST>(J.multi)
