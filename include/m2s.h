@@ -297,10 +297,12 @@ int m2s_last_grid_stats(uint64_t out[10]);
 void m2s_set_profiling(int enable);
 int m2s_last_grid_phase_ms(float out[4]);
 /* With profiling on, the last grid call on this thread also records its
- * propagation steps in order: the number of states of each relaxed bucket
- * list, or (top bit set) the number of far states of each redistribution.
- * Returns the number of steps recorded (at most 65,536), copying up to
- * `capacity` of them to `out` (may be NULL). */
+ * propagation steps in order, two words each: the step — the number of states
+ * of a relaxed bucket list (bit 30 set when one block relaxed it alone), or
+ * (bit 31 set) the number of far states of a redistribution, or 0xC0000000
+ * for the end — and the nanoseconds from the kernel's start to the moment the
+ * step was chosen.  Returns the number of steps recorded (at most 65,536),
+ * copying up to `capacity` steps (2 * capacity words) to `out` (may be NULL). */
 uint32_t m2s_last_grid_round_log(uint32_t* out, uint32_t capacity);
 
 /* Point queries run one thread per query; a query that visits more than

@@ -290,14 +290,17 @@ def last_grid_stats():
 
 def last_grid_round_log():
     """With profiling on: the last grid call's propagation steps in order, as
-    (kind, size) rows — kind 0 a relax round of `size` states, kind 1 a far-list
-    redistribution of `size` states."""
+    (kind, size, t_ns) rows — kind 0 a relax round on every block, 2 a relax
+    round on one block, 1 a far-list redistribution, 3 the end; size in states;
+    t_ns the time from the kernel's start at which the step was chosen."""
     L = _lib.lib()
     n = int(L.m2s_last_grid_round_log(None, 0))
-    a = np.zeros(n, np.uint32)
+    a = np.zeros(2 * n, np.uint32)
     if n:
         L.m2s_last_grid_round_log(_vp(a), n)
-    return np.stack([(a >> 31).astype(np.int64), (a & 0x7FFFFFFF).astype(np.int64)], 1)
+    v, t = a[0::2], a[1::2]
+    kind = np.where(v >> 31, np.where((v >> 30) & 1, 3, 1), np.where((v >> 30) & 1, 2, 0))
+    return np.stack([kind.astype(np.int64), (v & 0x3FFFFFFF).astype(np.int64), t.astype(np.int64)], 1)
 
 
 def set_profiling(enable: bool):

@@ -237,9 +237,12 @@ int m2s_last_grid_stats(uint64_t out[10]) {
 void m2s_set_profiling(int enable) { t_profile = enable != 0; }
 
 uint32_t m2s_last_grid_round_log(uint32_t* out, uint32_t capacity) {
-  const uint32_t n = (uint32_t)t_round_log.size();
+  const uint32_t n = (uint32_t)(t_round_log.size() / 2);
   if (out)
-    for (uint32_t i = 0; i < n && i < capacity; ++i) out[i] = t_round_log[i];
+    for (uint32_t i = 0; i < n && i < capacity; ++i) {
+      out[2 * i] = t_round_log[2 * i];
+      out[2 * i + 1] = t_round_log[2 * i + 1];
+    }
   return n;
 }
 

@@ -534,10 +534,7 @@ __device__ __forceinline__ int next_step(Sched& sh, const Counters& ct, uint32_t
     sh.b += q;
     sh.n = c[q];
     sh.round += 1;
-    if (leader) {
-      ct.count[consumed] = 0;
-      st->max_list = max(st->max_list, c[q]);
-    }
+    if (leader) ct.count[consumed] = 0;
     return kRelax;
   }
   // Every window list is empty.  Far states all lie at or beyond B + kRing, so
@@ -696,7 +693,8 @@ __global__ void __launch_bounds__(256, 4) k_propagate(const __grid_constant__ Gr
   }
   bool nan = false;
   unsigned long long evals = 0, skips = 0;
-  uint32_t far_phases = 0, logged = 0;
+  uint32_t far_phases = 0, logged = 0, max_list = 0;
+  const uint64_t t_start = (lead_block && threadIdx.x == 0 && round_log) ? global_ns() : 0;
   bool aborted = false;
   // Thread 0: the next step (unless a solo run already chose it), logged by
   // block 0 when profiling: the relaxed list's size, or (top bit) the far list's.
@@ -706,9 +704,17 @@ __global__ void __launch_bounds__(256, 4) k_propagate(const __grid_constant__ Gr
     const uint32_t spill_ov = in_run ? 0u : *(volatile uint32_t*)&st->overflow2[sh.round & 1u];
     sh.action = sh.steps >= max_steps ? kLimit : next_step(sh, counters(in_run), spill_ov, st, lead_block);
     ++sh.steps;
+    if (sh.action == kRelax) max_list = max(max_list, sh.n);
+    // Profiling: block 0 records each step — the relaxed list's size (bit 30:
+    // a solo round) or the far list's size (bit 31) — and when it was chosen.
     if (lead_block && round_log && logged < log_cap) {
-      if (sh.action == kRelax) round_log[logged++] = sh.n;
-      else if (sh.action == kRedistribute) round_log[logged++] = 0x80000000u | counters(in_run).count[kFar0 + sh.fp];
+      uint32_t v = 0;
+      if (sh.action == kRelax) v = sh.n | (sh.n <= solo_max ? 0x40000000u : 0u);
+      else if (sh.action == kRedistribute) v = 0x80000000u | counters(in_run).count[kFar0 + sh.fp];
+      else v = 0xC0000000u;  // the end
+      round_log[2 * logged] = v;
+      round_log[2 * logged + 1] = (uint32_t)(global_ns() - t_start);
+      ++logged;
     }
   };
   for (;;) {
@@ -864,6 +870,7 @@ __global__ void __launch_bounds__(256, 4) k_propagate(const __grid_constant__ Gr
     st->round = sh.round;
     st->far_phases = far_phases;
     st->log_n = logged;
+    st->max_list = max_list;
     st->done = 1;
   }
 }
@@ -1041,11 +1048,11 @@ struct GridJob::Impl {
 GridJob::GridJob() : p(new Impl) {}
 GridJob::~GridJob() { delete p; }
 uint32_t GridJob::capacity() const { return p->cap; }
-int GridJob::enable_round_log(uint32_t cap, cudaStream_t s) { return p->round_log.alloc(cap, s); }
+int GridJob::enable_round_log(uint32_t cap, cudaStream_t s) { return p->round_log.alloc(2ull * cap, s); }
 int GridJob::read_round_log(std::vector<uint32_t>* out, uint32_t n, cudaStream_t s) {
-  n = std::min<uint32_t>(n, (uint32_t)p->round_log.n);
-  out->resize(n);
-  if (n) M2S_CUDA(cudaMemcpyAsync(out->data(), p->round_log.p, 4ull * n, cudaMemcpyDeviceToHost, s));
+  n = std::min<uint32_t>(n, (uint32_t)(p->round_log.n / 2));
+  out->resize(2ull * n);
+  if (n) M2S_CUDA(cudaMemcpyAsync(out->data(), p->round_log.p, 8ull * n, cudaMemcpyDeviceToHost, s));
   M2S_CUDA(cudaStreamSynchronize(s));
   return M2S_OK;
 }
@@ -1246,7 +1253,7 @@ int GridJob::enqueue(cudaStream_t s, cudaEvent_t* ev) {
     uint32_t max_steps = kMaxSteps;
     const TriRec* tris = J.tris;
     uint32_t* log = J.round_log.p;
-    uint32_t log_cap = (uint32_t)J.round_log.n;
+    uint32_t log_cap = (uint32_t)(J.round_log.n / 2);
     void* args[] = {&J.gs,     &tris,   &J.snap.p,  &J.work.p,    &J.lists.p, &J.cap,     &J.touched.p,
                     &J.state.p, &J.bar.p, &max_steps, &J.d_status, &log,       &log_cap, &J.solo_max};
     cudaLaunchConfig_t cfg{};

@@ -202,8 +202,8 @@ class GridJob {
   void set_cooperative_blocks(unsigned blocks);  // clamped to [1, max_cooperative_blocks()]
   int sign() const;
   uint32_t grids() const;
-  // Profiling: record the size of every relaxed list (and, top bit set, of
-  // every redistributed far list) in a device log of `cap` entries.
+  // Profiling: record every propagation step (kind and size, and the time it
+  // was chosen) in a device log of `cap` steps.
   int enable_round_log(uint32_t cap, cudaStream_t s);
   int read_round_log(std::vector<uint32_t>* out, uint32_t n, cudaStream_t s);
 
