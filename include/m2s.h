@@ -285,9 +285,8 @@ int m2s_radix_sort_pairs_device(uint32_t* d_keys, uint32_t* d_values, uint64_t n
 
 /* Diagnostics of the last grid call on this thread: [seed updates, relax
  * rounds, states relaxed, neighbour evaluations, ray hits, propagation
- * restarts, kernel launches, far-list redistributions, proposals to a cell
- * that already held the proposing triangle, largest bucket list
- * relaxed in one round]. */
+ * restarts, kernel launches, far-list redistributions, rounds relaxed by one
+ * block alone, largest bucket list relaxed in one round]. */
 int m2s_last_grid_stats(uint64_t out[10]);
 
 /* When enabled (per thread), grid calls time their phases with CUDA events on

@@ -278,7 +278,7 @@ def generate_grid_sdf(vertices, indices: Topology, grid: Grid, sign_method: Sign
 
 
 GRID_STATS = ("seed_updates", "rounds", "states_relaxed", "neighbour_evals", "ray_hits", "restarts",
-              "kernel_launches", "far_phases", "same_triangle_proposals", "max_list")
+              "kernel_launches", "far_phases", "solo_rounds", "max_list")
 
 
 def last_grid_stats():

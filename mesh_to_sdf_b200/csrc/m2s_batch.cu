@@ -142,7 +142,7 @@ struct m2s_grid_plan {
         sum[4] += info.ray_hits;
         sum[6] += info.launches;
         sum[7] += info.far_phases;
-        sum[8] += info.skips;
+        sum[8] += info.solo_rounds;
         sum[9] = std::max<uint64_t>(sum[9], info.max_list);
         if (!info.overflow) continue;
         if (attempt >= 6 || j->capacity() >= 0x40000000u) {

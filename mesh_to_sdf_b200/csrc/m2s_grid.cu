@@ -176,7 +176,8 @@ struct PropState {
   uint32_t far_phases;
   uint32_t max_list;      // largest bucket list relaxed in one round
   uint32_t log_n;         // steps recorded in the round log
-  unsigned long long entries, evals, seeds, ray_hits, skips;
+  uint32_t solo_rounds;   // rounds relaxed by block 0 alone
+  unsigned long long entries, evals, seeds, ray_hits;
 };
 
 __device__ __forceinline__ P3 center(const GridK& g, int x, int y, int z) {
@@ -559,8 +560,7 @@ __device__ __forceinline__ void relax_propose(const GridSet& gs, const TriRec* _
                                               const unsigned long long* snap_keys, unsigned long long* work_keys,
                                               const uint2* list, uint32_t n, uint32_t T, uint32_t t0,
                                               uint32_t* s_touch, uint32_t* s_ntouch, PropState* st, uint32_t parity,
-                                              uint32_t* spill, uint32_t cap, bool& nan, unsigned long long& evals,
-                                              unsigned long long& skips) {
+                                              uint32_t* spill, uint32_t cap, bool& nan, unsigned long long& evals) {
   // One thread per (state, neighbour) proposal; consecutive threads share a
   // state, so its entry and triangle loads are warp broadcasts.  kUnroll
   // independent proposals per iteration keep that many load chains in
@@ -590,12 +590,9 @@ __device__ __forceinline__ void relax_propose(const GridSet& gs, const TriRec* _
       cell_coords(g, ent.x - g.cell_off, &x, &y, &z);
       // iproduct!(-1..=1, -1..=1, -1..=1) order (grid.rs:512): x outermost.
       const int X = x + (int)(ku / 9u) - 1, Y = y + (int)((ku / 3u) % 3u) - 1, Z = z + (int)(ku % 3u) - 1;
-      if (X < 0 || Y < 0 || Z < 0 || X >= g.n[0] || Y >= g.n[1] || Z >= g.n[2]) continue;
+      if ((unsigned)X >= (unsigned)g.n[0] || (unsigned)Y >= (unsigned)g.n[1] || (unsigned)Z >= (unsigned)g.n[2]) continue;
       const uint32_t j = g.cell_off + local_index(g, X, Y, Z);
       const unsigned long long snap = __ldcg(&snap_keys[j]);
-      // Counted only: such a proposal recomputes the distance the cell holds
-      // and cannot win, but skipping it leaves its lanes idle in the warp.
-      if (key_tri(snap) == tri) ++skips;
       const TriRec r = tris[tri];
       const float d = cell_distance<SIGN>(center(g, X, Y, Z), p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
       ++evals;
@@ -692,8 +689,8 @@ __global__ void __launch_bounds__(256, 4) k_propagate(const __grid_constant__ Gr
     sh.steps = 0;
   }
   bool nan = false;
-  unsigned long long evals = 0, skips = 0;
-  uint32_t far_phases = 0, logged = 0, max_list = 0;
+  unsigned long long evals = 0;
+  uint32_t far_phases = 0, logged = 0, max_list = 0, solo_rounds = 0;
   const uint64_t t_start = (lead_block && threadIdx.x == 0 && round_log) ? global_ns() : 0;
   bool aborted = false;
   // Thread 0: the next step (unless a solo run already chose it), logged by
@@ -813,7 +810,7 @@ __global__ void __launch_bounds__(256, 4) k_propagate(const __grid_constant__ Gr
     const uint32_t T = solo ? blockDim.x : gridDim.x * blockDim.x;
     const uint32_t t0 = solo ? threadIdx.x : blockIdx.x * blockDim.x + threadIdx.x;
     relax_propose<SIGN, MULTI>(gs, tris, snap_keys, work_keys, lists + (unsigned long long)sh.cur * cap, n, T, t0,
-                               s_touch, &s_ntouch, st, parity, spill, cap, nan, evals, skips);
+                               s_touch, &s_ntouch, st, parity, spill, cap, nan, evals);
     if (lead_block && threadIdx.x == 0) atomicAdd(&st->entries, (unsigned long long)n);
     if (solo) {
       __syncthreads();
@@ -840,6 +837,7 @@ __global__ void __launch_bounds__(256, 4) k_propagate(const __grid_constant__ Gr
     if (threadIdx.x == 0) {
       step();
       ++s_runs;
+      ++solo_rounds;
       s_more = sh.action == kRelax && sh.n <= solo_max && s_runs < kSoloRounds;
       if (!s_more) {
         for (int k = 0; k < kLists; ++k) st->count[k] = s_count[k];
@@ -863,14 +861,13 @@ __global__ void __launch_bounds__(256, 4) k_propagate(const __grid_constant__ Gr
   if (nan) atomicOr(status, bit(M2S_ERR_NAN_DISTANCE));
   for (int o = 16; o; o >>= 1) evals += __shfl_xor_sync(0xFFFFFFFFu, evals, o);
   if (lane == 0 && evals) atomicAdd(&st->evals, evals);
-  for (int o = 16; o; o >>= 1) skips += __shfl_xor_sync(0xFFFFFFFFu, skips, o);
-  if (lane == 0 && skips) atomicAdd(&st->skips, skips);
   if (aborted && lead_block && threadIdx.x == 0) atomicOr(status, bit(M2S_ERR_LIMIT));
   if (lead_block && threadIdx.x == 0) {
     st->round = sh.round;
     st->far_phases = far_phases;
     st->log_n = logged;
     st->max_list = max_list;
+    st->solo_rounds = solo_rounds;
     st->done = 1;
   }
 }
@@ -1318,7 +1315,7 @@ int GridJob::read_state(cudaStream_t s, GridRunInfo* info) {
   info->evals = h->evals;
   info->ray_hits = h->ray_hits;
   info->far_phases = h->far_phases;
-  info->skips = h->skips;
+  info->solo_rounds = h->solo_rounds;
   info->max_list = h->max_list;
   info->log_n = h->log_n;
   info->launches = J.launches;
@@ -1360,7 +1357,7 @@ int run_grid_job(GridJob& job, cudaStream_t s, uint64_t stats[kGridStats], float
     stats[5] = restarts;
     stats[6] = info.launches;
     stats[7] = info.far_phases;
-    stats[8] = info.skips;
+    stats[8] = info.solo_rounds;
     stats[9] = info.max_list;
   }
   if (phase_ms) {

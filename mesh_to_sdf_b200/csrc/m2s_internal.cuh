@@ -147,8 +147,7 @@ struct GridDesc {
 
 // stats: [seed updates, relax rounds, states relaxed, neighbour evaluations,
 // ray hits, overflow restarts, kernel launches, far-list redistributions,
-// proposals to a cell that already held the proposing triangle, largest list
-// relaxed in one round].  phase_ms (may be NULL) receives device time of
+// rounds relaxed by one block alone, largest list relaxed in one round].  phase_ms (may be NULL) receives device time of
 // [seeding, propagation, rays, finalize].
 constexpr int kGridStats = 10;
 int grid_sdf(const MeshView& m, const GridDesc& g, int sign, float* d_out, uint32_t* d_status, cudaStream_t s,
@@ -169,7 +168,7 @@ struct GridTuning {
 
 struct GridRunInfo {
   bool overflow = false;
-  uint64_t seeds = 0, rounds = 0, entries = 0, evals = 0, ray_hits = 0, far_phases = 0, launches = 0, skips = 0,
+  uint64_t seeds = 0, rounds = 0, entries = 0, evals = 0, ray_hits = 0, far_phases = 0, launches = 0, solo_rounds = 0,
            max_list = 0, log_n = 0;
 };
 
