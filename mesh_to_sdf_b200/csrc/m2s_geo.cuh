@@ -108,6 +108,50 @@ __device__ __forceinline__ float point_triangle_distance2(P3 p, P3 a, P3 b, P3 c
   return vdot(d, d);
 }
 
+// closest_point_proper without branches: every dot product is formed, the
+// first region whose test holds (in the reference's order) is chosen by
+// selects, and the one division that region needs is done once.  Each
+// region's value comes from the same operations as above, so the result is
+// bit-identical; lanes of a warp in different regions no longer run every
+// region's path and division one after another.
+__device__ __forceinline__ P3 closest_point_proper_sel(P3 p, P3 a, P3 b, P3 c) {
+  const P3 ab = vsub(b, a), ac = vsub(c, a);
+  const P3 ap = vsub(p, a), bp = vsub(p, b), cp = vsub(p, c);
+  const float d1 = vdot(ab, ap), d2 = vdot(ac, ap);
+  const float d3 = vdot(ab, bp), d4 = vdot(ac, bp);
+  const float d5 = vdot(ab, cp), d6 = vdot(ac, cp);
+  const float vc = fs(fm(d1, d4), fm(d3, d2));
+  const float vb = fs(fm(d5, d2), fm(d1, d6));
+  const float va = fs(fm(d3, d6), fm(d5, d4));
+  const float d43 = fs(d4, d3), d56 = fs(d5, d6);
+  const bool rA = d1 <= 0.0f && d2 <= 0.0f;
+  const bool rB = d3 >= 0.0f && d4 <= d3;
+  const bool rC = d6 >= 0.0f && d5 <= d6;
+  const bool eAB = vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f;
+  const bool eAC = !eAB && vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f;
+  const bool eBC = !eAB && !eAC && va <= 0.0f && d43 >= 0.0f && d56 >= 0.0f;
+  const bool face = !eAB && !eAC && !eBC;
+  const float num = eAB ? d1 : (eAC ? d2 : (eBC ? d43 : 1.0f));
+  const float den = eAB ? fs(d1, d3) : (eAC ? fs(d2, d6) : (eBC ? fa(d43, d56) : fa(fa(va, vb), vc)));
+  const float q = fd(num, den);
+  const P3 cb = vsub(c, b);
+  const P3 base = eBC ? b : a;
+  const P3 e1 = eAC ? ac : (eBC ? cb : ab);
+  const float s1 = face ? fm(vb, q) : q;
+  P3 x = vadd(base, vmul(e1, s1));
+  const P3 x2 = vadd(x, vmul(ac, fm(vc, q)));
+  if (face) x = x2;
+  if (rA || rB || rC) x = rA ? a : (rB ? b : c);
+  return x;
+}
+
+// point_triangle_distance2 with the branch-free proper case.
+__device__ __forceinline__ float point_triangle_distance2_sel(P3 p, P3 a, P3 b, P3 c, int kind) {
+  const P3 cp = kind == TRI_PROPER ? closest_point_proper_sel(p, a, b, c) : closest_point_triangle(p, a, b, c, kind);
+  const P3 d = vsub(p, cp);
+  return vdot(d, d);
+}
+
 // geo.rs:43-56: positive when (p - closest) . (ab x ac) > 0, else -distance.
 __device__ __forceinline__ float point_triangle_signed_distance(P3 p, P3 a, P3 b, P3 c, int kind) {
   P3 cp = closest_point_triangle(p, a, b, c, kind);

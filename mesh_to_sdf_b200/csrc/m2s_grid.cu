@@ -215,7 +215,7 @@ __device__ __forceinline__ void snap(const GridK& g, P3 p, int cell[3]) {
 
 template <int SIGN>
 __device__ __forceinline__ float cell_distance(P3 pos, P3 a, P3 b, P3 c, int kind) {
-  if (SIGN == M2S_SIGN_RAYCAST) return fsqrt(point_triangle_distance2(pos, a, b, c, kind));
+  if (SIGN == M2S_SIGN_RAYCAST) return fsqrt(point_triangle_distance2_sel(pos, a, b, c, kind));
   return point_triangle_signed_distance(pos, a, b, c, kind);
 }
 
@@ -554,68 +554,146 @@ __device__ __forceinline__ int next_step(Sched& sh, const Counters& ct, uint32_t
 // depend on which threads do it: results are the same either way.
 constexpr uint32_t kSoloRounds = 1024;  // the threshold (default 64 states) is GridTuning::solo_max
 
-// Propose phase of a relax round over list[0..n), proposals t0, t0 + T, ...
+// Queue of one warp's proposals that need a distance evaluation (Normal sign).
+constexpr uint32_t kQueue = 64;
+struct WarpQueue {
+  uint32_t tri[kQueue], j[kQueue], x[kQueue], y[kQueue], z[kQueue];
+  unsigned long long snap[kQueue];
+};
+constexpr int kWarps = 8;  // k_propagate runs 256 threads per block
+
+// Stages cell j, which this proposal moved off its snapshot value, for the
+// block's commit (spilling to the round's global list when the stage is full).
+__device__ __forceinline__ void stage_touch(uint32_t j, uint32_t* s_touch, uint32_t* s_ntouch, PropState* st,
+                                            uint32_t parity, uint32_t* spill, uint32_t cap) {
+  const uint32_t q = atomicAdd(s_ntouch, 1u);
+  if (q < kTouchStage) {
+    s_touch[q] = j;
+  } else {
+    const uint32_t pos = atomicAdd(&st->touched2[parity], 1u);
+    if (pos < cap) spill[pos] = j;
+    else atomicOr(&st->overflow2[parity], 1u);
+  }
+}
+
+// Propose phase of a relax round over list[0..n): every state offers its
+// triangle to the 26 cells around it (its own cell holds that triangle's
+// distance or a better one, so it never gains).  Proposals t0, t0 + T, ...
+// advance as (state e, neighbour k) pairs without division: T = 26 * dE + dK;
+// consecutive threads share a state, so its entry and triangle loads are warp
+// broadcasts.
+//
+// Raycast: each thread evaluates its proposals, kUnroll at a time.  Normal:
+// a proposal whose neighbour already holds the same triangle cannot gain (the
+// distance of a (cell, triangle) pair is one deterministic value), and the
+// signed distance costs more, so the warp first filters its proposals and
+// queues the rest in shared memory, then evaluates them 32 at a time with
+// every lane busy.  Results do not depend on the order of proposals.
 template <int SIGN, bool MULTI>
 __device__ __forceinline__ void relax_propose(const GridSet& gs, const TriRec* __restrict__ tris,
                                               const unsigned long long* snap_keys, unsigned long long* work_keys,
                                               const uint2* list, uint32_t n, uint32_t T, uint32_t t0,
                                               uint32_t* s_touch, uint32_t* s_ntouch, PropState* st, uint32_t parity,
-                                              uint32_t* spill, uint32_t cap, bool& nan, unsigned long long& evals) {
-  // One thread per (state, neighbour) proposal; consecutive threads share a
-  // state, so its entry and triangle loads are warp broadcasts.  kUnroll
-  // independent proposals per iteration keep that many load chains in
-  // flight.  Proposals advance as (state e, neighbour k) pairs without
-  // division: T = 27 * dE + dK.
-  const uint32_t dE = T / 27u, dK = T % 27u;
-  uint32_t e = t0 / 27u, k = t0 % 27u;
-  while (e < n) {
-    bool first[kUnroll];
-    uint32_t jj[kUnroll];
+                                              uint32_t* spill, uint32_t cap, bool& nan, unsigned long long& evals,
+                                              WarpQueue* q) {
+  const uint32_t dE = T / 26u, dK = T % 26u;
+  uint32_t e = t0 / 26u, k = t0 % 26u;
+  // The neighbour of state e for proposal k: false when it lies off the grid.
+  auto neighbour = [&](uint32_t eu, uint32_t kk, uint32_t& tri, uint32_t& j, int& X, int& Y, int& Z) {
+    const uint2 ent = __ldcg(&list[eu]);  // written by other blocks in earlier rounds
+    tri = ent.y;
+    const GridK& g = grid_of_tri<MULTI>(gs, tri);
+    int x, y, z;
+    cell_coords(g, ent.x - g.cell_off, &x, &y, &z);
+    // iproduct!(-1..=1, -1..=1, -1..=1) order (grid.rs:512): x outermost; 13 is the cell itself.
+    const uint32_t ku = kk + (kk >= 13u);
+    X = x + (int)(ku / 9u) - 1;
+    Y = y + (int)((ku / 3u) % 3u) - 1;
+    Z = z + (int)(ku % 3u) - 1;
+    if ((unsigned)X >= (unsigned)g.n[0] || (unsigned)Y >= (unsigned)g.n[1] || (unsigned)Z >= (unsigned)g.n[2])
+      return false;
+    j = g.cell_off + local_index(g, X, Y, Z);
+    return true;
+  };
+  // Distance of triangle tri at cell (X, Y, Z) = j against its snapshot key;
+  // true when this proposal moved the cell off the snapshot.
+  auto evaluate = [&](uint32_t tri, uint32_t j, int X, int Y, int Z, unsigned long long snap) {
+    const GridK& g = grid_of_tri<MULTI>(gs, tri);
+    const TriRec r = tris[tri];
+    const float d = cell_distance<SIGN>(center(g, X, Y, Z), p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
+    if (isnan(d)) nan = true;
+    const unsigned long long cand = pack(d, tri);
+    return beats<SIGN>(cand, snap, &nan) && improve_first<SIGN>(&work_keys[j], cand, snap, &nan);
+  };
+  auto step = [&]() {
+    k += dK;
+    e += dE;
+    if (k >= 26u) {
+      k -= 26u;
+      ++e;
+    }
+  };
+  if constexpr (SIGN == M2S_SIGN_RAYCAST) {
+    while (e < n) {
+      bool first[kUnroll];
+      uint32_t jj[kUnroll];
 #pragma unroll
-    for (int u = 0; u < kUnroll; ++u) {
-      first[u] = false;
-      jj[u] = 0;
-      const uint32_t eu = e, ku = k;
-      k += dK;
-      e += dE;
-      if (k >= 27u) {
-        k -= 27u;
-        ++e;
-      }
-      if (eu >= n) continue;
-      const uint2 ent = __ldcg(&list[eu]);  // written by other blocks in earlier rounds
-      const uint32_t tri = ent.y;
-      const GridK& g = grid_of_tri<MULTI>(gs, tri);
-      int x, y, z;
-      cell_coords(g, ent.x - g.cell_off, &x, &y, &z);
-      // iproduct!(-1..=1, -1..=1, -1..=1) order (grid.rs:512): x outermost.
-      const int X = x + (int)(ku / 9u) - 1, Y = y + (int)((ku / 3u) % 3u) - 1, Z = z + (int)(ku % 3u) - 1;
-      if ((unsigned)X >= (unsigned)g.n[0] || (unsigned)Y >= (unsigned)g.n[1] || (unsigned)Z >= (unsigned)g.n[2]) continue;
-      const uint32_t j = g.cell_off + local_index(g, X, Y, Z);
-      const unsigned long long snap = __ldcg(&snap_keys[j]);
-      const TriRec r = tris[tri];
-      const float d = cell_distance<SIGN>(center(g, X, Y, Z), p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
-      ++evals;
-      if (isnan(d)) nan = true;
-      const unsigned long long cand = pack(d, tri);
-      if (beats<SIGN>(cand, snap, &nan)) {
-        first[u] = improve_first<SIGN>(&work_keys[j], cand, snap, &nan);
+      for (int u = 0; u < kUnroll; ++u) {
+        first[u] = false;
+        jj[u] = 0;
+        const uint32_t eu = e, ku = k;
+        step();
+        uint32_t tri, j;
+        int X, Y, Z;
+        if (eu >= n || !neighbour(eu, ku, tri, j, X, Y, Z)) continue;
+        ++evals;
+        first[u] = evaluate(tri, j, X, Y, Z, __ldcg(&snap_keys[j]));
         jj[u] = j;
       }
-    }
 #pragma unroll
-    for (int u = 0; u < kUnroll; ++u) {
-      if (first[u]) {
-        const uint32_t q = atomicAdd(s_ntouch, 1u);
-        if (q < kTouchStage) {
-          s_touch[q] = jj[u];
-        } else {
-          const uint32_t pos = atomicAdd(&st->touched2[parity], 1u);
-          if (pos < cap) spill[pos] = jj[u];
-          else atomicOr(&st->overflow2[parity], 1u);
-        }
+      for (int u = 0; u < kUnroll; ++u)
+        if (first[u]) stage_touch(jj[u], s_touch, s_ntouch, st, parity, spill, cap);
+    }
+  } else {
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t qn = 0;  // warp-uniform queue length, < 32 between iterations
+    auto run = [&](uint32_t i) {
+      if (evaluate(q->tri[i], q->j[i], (int)q->x[i], (int)q->y[i], (int)q->z[i], q->snap[i]))
+        stage_touch(q->j[i], s_touch, s_ntouch, st, parity, spill, cap);
+    };
+    while (__any_sync(0xFFFFFFFFu, e < n)) {
+      const uint32_t eu = e, ku = k;
+      step();
+      uint32_t tri = 0, j = 0;
+      int X = 0, Y = 0, Z = 0;
+      unsigned long long snap = 0;
+      bool keep = false;
+      if (eu < n && neighbour(eu, ku, tri, j, X, Y, Z)) {
+        ++evals;
+        snap = __ldcg(&snap_keys[j]);
+        keep = key_tri(snap) != tri;
+      }
+      const unsigned m = __ballot_sync(0xFFFFFFFFu, keep);
+      if (keep) {
+        const uint32_t w = qn + __popc(m & ((1u << lane) - 1u));  // qn + 31 at most
+        q->tri[w] = tri;
+        q->j[w] = j;
+        q->x[w] = (uint32_t)X;
+        q->y[w] = (uint32_t)Y;
+        q->z[w] = (uint32_t)Z;
+        q->snap[w] = snap;
+      }
+      qn += __popc(m);
+      if (qn >= 32u) {
+        __syncwarp();
+        run(qn - 32u + lane);
+        __syncwarp();  // the slots are written again next iteration
+        qn -= 32u;
       }
     }
+    __syncwarp();
+    if (lane < qn) run(lane);
+    __syncwarp();
   }
 }
 
@@ -665,6 +743,7 @@ __global__ void __launch_bounds__(256, 4) k_propagate(const __grid_constant__ Gr
                                                    uint32_t solo_max) {
   __shared__ Sched sh;
   __shared__ uint32_t s_touch[kTouchStage];
+  __shared__ WarpQueue s_queue[SIGN == M2S_SIGN_NORMAL ? kWarps : 1];
   __shared__ uint32_t s_ntouch, s_gen, s_pending, s_more, s_runs, s_solo_run;
   __shared__ uint32_t s_count[kLists], s_far_min[2], s_overflow;  // block 0's counters during a solo run
   // (built where used, so no pointer stays live across the propose loop)
@@ -810,7 +889,8 @@ __global__ void __launch_bounds__(256, 4) k_propagate(const __grid_constant__ Gr
     const uint32_t T = solo ? blockDim.x : gridDim.x * blockDim.x;
     const uint32_t t0 = solo ? threadIdx.x : blockIdx.x * blockDim.x + threadIdx.x;
     relax_propose<SIGN, MULTI>(gs, tris, snap_keys, work_keys, lists + (unsigned long long)sh.cur * cap, n, T, t0,
-                               s_touch, &s_ntouch, st, parity, spill, cap, nan, evals);
+                               s_touch, &s_ntouch, st, parity, spill, cap, nan, evals,
+                               &s_queue[SIGN == M2S_SIGN_NORMAL ? threadIdx.x >> 5 : 0]);
     if (lead_block && threadIdx.x == 0) atomicAdd(&st->entries, (unsigned long long)n);
     if (solo) {
       __syncthreads();
