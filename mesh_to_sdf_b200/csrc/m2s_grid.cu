@@ -243,7 +243,9 @@ template <int SIGN>
 __device__ __forceinline__ bool improve_first(unsigned long long* slot, unsigned long long cand, unsigned long long snap,
                                               bool* nan) {
   if (SIGN == M2S_SIGN_RAYCAST) return atomicMin(slot, cand) == snap;
-  unsigned long long old = *(volatile unsigned long long*)slot;
+  // The slot still holds the snapshot unless another proposal of this round
+  // won it already, so the snapshot is the first guess of the exchange.
+  unsigned long long old = snap;
   while (beats<SIGN>(cand, old, nan)) {
     unsigned long long prev = atomicCAS(slot, old, cand);
     if (prev == old) return old == snap;
@@ -509,9 +511,12 @@ enum { kRelax = 0, kRedistribute = 1, kDone = 2, kLimit = 3 };
 // and which receives pushes only after the next barrier.
 __device__ __forceinline__ int next_step(Sched& sh, const Counters& ct, uint32_t spill_overflow, PropState* st,
                                          bool leader) {
-  uint32_t c[kRing];
+  // Bit k: the list of bucket b + k holds states (bits past the window's end cleared).
+  uint32_t nonempty = 0;
 #pragma unroll
-  for (int k = 0; k < kRing; ++k) c[k] = *(volatile uint32_t*)&ct.count[sh.slot[k]];
+  for (int k = 0; k < kRing; ++k) nonempty |= (*(volatile uint32_t*)&ct.count[sh.slot[k]] != 0u ? 1u : 0u) << k;
+  const uint32_t left = sh.B + kRing - sh.b;  // buckets b .. B + kRing - 1 lie in the window
+  if (left < kRing) nonempty &= (1u << left) - 1u;
   // Only values no block can change before every block has passed this step:
   // list counts (pushes come after the next barrier), the push overflow flag
   // and the spill overflow flag of the round just finished (the next propose
@@ -521,9 +526,9 @@ __device__ __forceinline__ int next_step(Sched& sh, const Counters& ct, uint32_t
   const uint32_t far_b = *(volatile uint32_t*)&ct.far_min[sh.fp];
   if (overflow) return kDone;
   // slot[q] holds bucket b + q; the window ends at bucket B + kRing - 1.
-  int q = 0;
-  while (q < kRing && sh.b + q < sh.B + kRing && c[q] == 0) ++q;
-  if (q < kRing && sh.b + q < sh.B + kRing) {
+  if (nonempty) {
+    const int q = __ffs(nonempty) - 1;
+    const uint32_t nq = *(volatile uint32_t*)&ct.count[sh.slot[q]];
     uint32_t rot[kRing];
 #pragma unroll
     for (int k = 0; k < kRing; ++k) rot[k] = sh.slot[(k + q) % kRing];  // advance b by q
@@ -533,7 +538,7 @@ __device__ __forceinline__ int next_step(Sched& sh, const Counters& ct, uint32_t
 #pragma unroll
     for (int k = 0; k < kRing; ++k) sh.slot[k] = rot[k];
     sh.b += q;
-    sh.n = c[q];
+    sh.n = nq;
     sh.round += 1;
     if (leader) ct.count[consumed] = 0;
     return kRelax;
@@ -553,6 +558,7 @@ __device__ __forceinline__ int next_step(Sched& sh, const Counters& ct, uint32_t
 // the waiting blocks' bounded wait always ends.  The work of a round does not
 // depend on which threads do it: results are the same either way.
 constexpr uint32_t kSoloRounds = 1024;  // the threshold (default 64 states) is GridTuning::solo_max
+constexpr uint32_t kSoloCap = 64;  // largest solo_max
 
 // Queue of one warp's proposals that need a distance evaluation (Normal sign).
 constexpr uint32_t kQueue = 64;
@@ -573,6 +579,132 @@ __device__ __forceinline__ void stage_touch(uint32_t j, uint32_t* s_touch, uint3
     const uint32_t pos = atomicAdd(&st->touched2[parity], 1u);
     if (pos < cap) spill[pos] = j;
     else atomicOr(&st->overflow2[parity], 1u);
+  }
+}
+
+// Neighbour kk (0..25, the cell itself skipped) of the state with entry ent:
+// its coordinates and index j; false when it lies off the grid.
+template <bool MULTI>
+__device__ __forceinline__ bool neighbour_cell(const GridSet& gs, uint2 ent, uint32_t kk, uint32_t& j, int& X, int& Y,
+                                               int& Z) {
+  const GridK& g = grid_of_tri<MULTI>(gs, ent.y);
+  int x, y, z;
+  cell_coords(g, ent.x - g.cell_off, &x, &y, &z);
+  // iproduct!(-1..=1, -1..=1, -1..=1) order (grid.rs:512): x outermost; 13 is the cell itself.
+  const uint32_t ku = kk + (kk >= 13u);
+  X = x + (int)(ku / 9u) - 1;
+  Y = y + (int)((ku / 3u) % 3u) - 1;
+  Z = z + (int)(ku % 3u) - 1;
+  if ((unsigned)X >= (unsigned)g.n[0] || (unsigned)Y >= (unsigned)g.n[1] || (unsigned)Z >= (unsigned)g.n[2])
+    return false;
+  j = g.cell_off + local_index(g, X, Y, Z);
+  return true;
+}
+
+// Distance of triangle tri (record r) at cell (X, Y, Z) = j against the
+// cell's snapshot key; true when this proposal moved the cell off the
+// snapshot (it is then the cell's one staging proposal of the round).
+template <int SIGN, bool MULTI>
+__device__ __forceinline__ bool propose_at(const GridSet& gs, const TriRec& r, uint32_t tri, uint32_t j, int X, int Y,
+                                           int Z, unsigned long long snap, unsigned long long* work_keys, bool& nan) {
+  const GridK& g = grid_of_tri<MULTI>(gs, tri);
+  const float d = cell_distance<SIGN>(center(g, X, Y, Z), p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
+  if (isnan(d)) nan = true;
+  const unsigned long long cand = pack(d, tri);
+  return beats<SIGN>(cand, snap, &nan) && improve_first<SIGN>(&work_keys[j], cand, snap, &nan);
+}
+
+// A solo round (block 0 alone, n <= kSoloCap states) forms the round's minima
+// in a table in shared memory instead of in the working keys: a proposal
+// that beats its cell's snapshot meets the cell's other proposals in the
+// cell's slot (open addressing, linear probing; at most 26 * kSoloCap cells
+// ever take a slot, fewer than kHash), and the commit writes each slot's
+// winner to both key arrays.  The round saves the working-key atomic and the
+// commit's read of it: two dependent trips to L2 of the few a solo round
+// waits for.  The table occupies the block's touch stage, free in a solo run.
+constexpr uint32_t kHash = 2048;
+constexpr uint32_t kNoCell = 0xFFFFFFFFu;
+static_assert(26 * kSoloCap < kHash, "a solo round could fill the table");
+static_assert(kHash * 3 <= (uint32_t)kTouchStage, "the table exceeds the touch stage");
+
+__device__ __forceinline__ uint32_t hash_slot(uint32_t j) { return (j * 2654435761u) >> 21; }  // 11 bits
+
+// Lowers cell j's slot to cand (which beats the cell's snapshot) if it beats
+// the slot's value; a slot taken here is listed for the commit.  Slots start
+// as (kNoCell, KEY_EMPTY); every candidate that beats a snapshot beats
+// KEY_EMPTY too, the order being a total one.
+template <int SIGN>
+__device__ __forceinline__ void table_improve(uint32_t* HJ, unsigned long long* HK, uint16_t* taken,
+                                              uint32_t* ntaken, uint32_t j, unsigned long long cand, bool& nan) {
+  uint32_t h = hash_slot(j);
+  for (uint32_t probe = 0; probe < kHash; ++probe) {  // ends at a free slot: fewer cells than slots
+    const uint32_t cur = atomicCAS(&HJ[h], kNoCell, j);
+    if (cur == kNoCell) taken[atomicAdd(ntaken, 1u)] = (uint16_t)h;
+    if (cur == kNoCell || cur == j) {
+      if (SIGN == M2S_SIGN_RAYCAST) {
+        atomicMin(&HK[h], cand);
+      } else {
+        unsigned long long old = *(volatile unsigned long long*)&HK[h];
+        while (beats<SIGN>(cand, old, &nan)) {
+          const unsigned long long prev = atomicCAS(&HK[h], old, cand);
+          if (prev == old) break;
+          old = prev;
+        }
+      }
+      return;
+    }
+    h = (h + 1) & (kHash - 1);
+  }
+}
+
+// Propose phase of a solo round: one thread per (state, neighbour) proposal.
+// A neighbour that holds the state's triangle already cannot gain.
+template <int SIGN, bool MULTI>
+__device__ __forceinline__ void relax_propose_solo(const GridSet& gs, const TriRec* __restrict__ tris,
+                                                   const unsigned long long* snap_keys, const uint2* list, uint32_t n,
+                                                   uint32_t* HJ, unsigned long long* HK, uint16_t* taken,
+                                                   uint32_t* ntaken, bool& nan, unsigned long long& evals) {
+  const uint32_t P = 26u * n;
+  for (uint32_t p = threadIdx.x; p < P; p += blockDim.x) {
+    const uint2 ent = __ldcg(&list[p / 26u]);  // written by other blocks in earlier rounds
+    uint32_t j;
+    int X, Y, Z;
+    if (!neighbour_cell<MULTI>(gs, ent, p % 26u, j, X, Y, Z)) continue;
+    ++evals;
+    const unsigned long long snap = __ldcg(&snap_keys[j]);
+    const TriRec r = tris[ent.y];
+    if (key_tri(snap) == ent.y) continue;
+    const GridK& g = grid_of_tri<MULTI>(gs, ent.y);
+    const float d = cell_distance<SIGN>(center(g, X, Y, Z), p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
+    if (isnan(d)) nan = true;
+    const unsigned long long cand = pack(d, ent.y);
+    if (beats<SIGN>(cand, snap, &nan)) table_improve<SIGN>(HJ, HK, taken, ntaken, j, cand, nan);
+  }
+}
+
+// Commit phase of a solo round: every taken slot's winner becomes the cell's
+// snapshot and working key and is queued under its bucket; the slot is freed.
+template <bool MULTI>
+__device__ __forceinline__ void relax_commit_solo(const GridSet& gs, unsigned long long* snap_keys,
+                                                  unsigned long long* work_keys, uint32_t* HJ,
+                                                  unsigned long long* HK, const uint16_t* taken, uint32_t ntaken,
+                                                  const Counters& ct, const Sched& sh, uint2* lists, uint32_t cap) {
+  for (uint32_t base = 0; base < ntaken; base += blockDim.x) {  // warp-uniform trip count
+    const uint32_t i = base + threadIdx.x;
+    const bool act = i < ntaken;
+    uint32_t j = 0, nb = 0;
+    unsigned long long w = KEY_EMPTY;
+    if (act) {
+      const uint32_t h = taken[i];
+      j = HJ[h];
+      w = HK[h];
+      snap_keys[j] = w;
+      work_keys[j] = w;
+      nb = bucket_of(grid_of_tri<MULTI>(gs, key_tri(w)).inv_delta, key_dist(w));
+      HJ[h] = kNoCell;
+      HK[h] = KEY_EMPTY;
+    }
+    push_entry_warp(ct, sh.b, sh.B, sh.slot, sh.fp, lists, cap, act, j, key_tri(w), nb);
   }
 }
 
@@ -602,28 +734,12 @@ __device__ __forceinline__ void relax_propose(const GridSet& gs, const TriRec* _
   auto neighbour = [&](uint32_t eu, uint32_t kk, uint32_t& tri, uint32_t& j, int& X, int& Y, int& Z) {
     const uint2 ent = __ldcg(&list[eu]);  // written by other blocks in earlier rounds
     tri = ent.y;
-    const GridK& g = grid_of_tri<MULTI>(gs, tri);
-    int x, y, z;
-    cell_coords(g, ent.x - g.cell_off, &x, &y, &z);
-    // iproduct!(-1..=1, -1..=1, -1..=1) order (grid.rs:512): x outermost; 13 is the cell itself.
-    const uint32_t ku = kk + (kk >= 13u);
-    X = x + (int)(ku / 9u) - 1;
-    Y = y + (int)((ku / 3u) % 3u) - 1;
-    Z = z + (int)(ku % 3u) - 1;
-    if ((unsigned)X >= (unsigned)g.n[0] || (unsigned)Y >= (unsigned)g.n[1] || (unsigned)Z >= (unsigned)g.n[2])
-      return false;
-    j = g.cell_off + local_index(g, X, Y, Z);
-    return true;
+    return neighbour_cell<MULTI>(gs, ent, kk, j, X, Y, Z);
   };
   // Distance of triangle tri at cell (X, Y, Z) = j against its snapshot key;
   // true when this proposal moved the cell off the snapshot.
   auto evaluate = [&](uint32_t tri, uint32_t j, int X, int Y, int Z, unsigned long long snap) {
-    const GridK& g = grid_of_tri<MULTI>(gs, tri);
-    const TriRec r = tris[tri];
-    const float d = cell_distance<SIGN>(center(g, X, Y, Z), p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
-    if (isnan(d)) nan = true;
-    const unsigned long long cand = pack(d, tri);
-    return beats<SIGN>(cand, snap, &nan) && improve_first<SIGN>(&work_keys[j], cand, snap, &nan);
+    return propose_at<SIGN, MULTI>(gs, tris[tri], tri, j, X, Y, Z, snap, work_keys, nan);
   };
   auto step = [&]() {
     k += dK;
@@ -742,7 +858,8 @@ __global__ void __launch_bounds__(256, 4) k_propagate(const __grid_constant__ Gr
                                                    uint32_t* status, uint32_t* round_log, uint32_t log_cap,
                                                    uint32_t solo_max) {
   __shared__ Sched sh;
-  __shared__ uint32_t s_touch[kTouchStage];
+  __shared__ __align__(16) uint32_t s_touch[kTouchStage];  // also a solo run's min table
+  __shared__ uint16_t s_taken[26 * kSoloCap];              // a solo round's taken table slots
   __shared__ WarpQueue s_queue[SIGN == M2S_SIGN_NORMAL ? kWarps : 1];
   __shared__ uint32_t s_ntouch, s_gen, s_pending, s_more, s_runs, s_solo_run;
   __shared__ uint32_t s_count[kLists], s_far_min[2], s_overflow;  // block 0's counters during a solo run
@@ -793,12 +910,16 @@ __global__ void __launch_bounds__(256, 4) k_propagate(const __grid_constant__ Gr
       ++logged;
     }
   };
+  bool chosen = false;  // a solo round's tail chose this step already (block-uniform)
   for (;;) {
-    if (threadIdx.x == 0) {
-      if (s_pending) s_pending = 0;
-      else step();
+    if (!chosen) {
+      if (threadIdx.x == 0) {
+        if (s_pending) s_pending = 0;
+        else step();
+      }
+      __syncthreads();
     }
-    __syncthreads();
+    chosen = false;
     const int action = sh.action;
     if (action == kDone) break;
     if (action == kLimit) {
@@ -882,15 +1003,26 @@ __global__ void __launch_bounds__(256, 4) k_propagate(const __grid_constant__ Gr
         s_overflow = *(volatile uint32_t*)&st->overflow | *(volatile uint32_t*)&st->overflow2[0] |
                      *(volatile uint32_t*)&st->overflow2[1];
       }
+      for (uint32_t h = threadIdx.x; h < kHash; h += blockDim.x) {  // the run's min table, kept empty between rounds
+        s_touch[h] = kNoCell;
+        reinterpret_cast<unsigned long long*>(s_touch + kHash)[h] = KEY_EMPTY;
+      }
+      __syncthreads();
     }
     const uint32_t parity = sh.round & 1u;
     uint32_t* spill = spill_lists + (unsigned long long)parity * cap;
     const uint32_t n = min(sh.n, cap);
     const uint32_t T = solo ? blockDim.x : gridDim.x * blockDim.x;
     const uint32_t t0 = solo ? threadIdx.x : blockIdx.x * blockDim.x + threadIdx.x;
-    relax_propose<SIGN, MULTI>(gs, tris, snap_keys, work_keys, lists + (unsigned long long)sh.cur * cap, n, T, t0,
-                               s_touch, &s_ntouch, st, parity, spill, cap, nan, evals,
-                               &s_queue[SIGN == M2S_SIGN_NORMAL ? threadIdx.x >> 5 : 0]);
+    uint32_t* HJ = s_touch;
+    unsigned long long* HK = reinterpret_cast<unsigned long long*>(s_touch + kHash);
+    if (solo)
+      relax_propose_solo<SIGN, MULTI>(gs, tris, snap_keys, lists + (unsigned long long)sh.cur * cap, n, HJ, HK,
+                                      s_taken, &s_ntouch, nan, evals);
+    else
+      relax_propose<SIGN, MULTI>(gs, tris, snap_keys, work_keys, lists + (unsigned long long)sh.cur * cap, n, T, t0,
+                                 s_touch, &s_ntouch, st, parity, spill, cap, nan, evals,
+                                 &s_queue[SIGN == M2S_SIGN_NORMAL ? threadIdx.x >> 5 : 0]);
     if (lead_block && threadIdx.x == 0) atomicAdd(&st->entries, (unsigned long long)n);
     if (solo) {
       __syncthreads();
@@ -898,11 +1030,15 @@ __global__ void __launch_bounds__(256, 4) k_propagate(const __grid_constant__ Gr
       aborted = true;
       break;
     }
-    if (lead_block && threadIdx.x == 0) st->touched2[parity ^ 1u] = 0;
-    // A solo round (at most solo_max <= kTouchStage / 27 states) never spills.
-    const uint32_t nspill = solo ? 0u : min(*(volatile uint32_t*)&st->touched2[parity], cap);
-    relax_commit<MULTI>(gs, snap_keys, work_keys, s_touch, min(s_ntouch, (uint32_t)kTouchStage), spill, nspill, t0,
-                        T, counters(solo), sh, lists, cap);
+    if (solo) {
+      relax_commit_solo<MULTI>(gs, snap_keys, work_keys, HJ, HK, s_taken, min(s_ntouch, 26u * kSoloCap),
+                               counters(true), sh, lists, cap);
+    } else {
+      if (lead_block && threadIdx.x == 0) st->touched2[parity ^ 1u] = 0;
+      const uint32_t nspill = min(*(volatile uint32_t*)&st->touched2[parity], cap);
+      relax_commit<MULTI>(gs, snap_keys, work_keys, s_touch, min(s_ntouch, (uint32_t)kTouchStage), spill, nspill, t0,
+                          T, global_counters(st), sh, lists, cap);
+    }
     if (!solo) {
       if (!grid_barrier(bar, nblocks, &s_gen)) {
         aborted = true;
@@ -929,11 +1065,15 @@ __global__ void __launch_bounds__(256, 4) k_propagate(const __grid_constant__ Gr
         for (uint32_t w = 0; w < sizeof(Sched) / 4; ++w) dst[w] = src[w];
         s_runs = 0;
         s_solo_run = 0;
+        s_pending = 1;
       }
-      s_pending = 1;
     }
     __syncthreads();
-    if (!s_more && !grid_barrier(bar, nblocks, &s_gen)) {
+    if (s_more) {
+      chosen = true;
+      continue;
+    }
+    if (!grid_barrier(bar, nblocks, &s_gen)) {
       aborted = true;
       break;
     }
@@ -1261,7 +1401,7 @@ int GridJob::prepare(const MeshView* meshes, uint32_t n, const GridDesc* gds, in
     return st;
   if (sign == M2S_SIGN_RAYCAST && (st = J.bits.alloc(woff, s))) return st;
   J.cap = tune.list_capacity ? tune.list_capacity : default_list_capacity(N);
-  J.solo_max = std::min<uint32_t>(tune.solo_max, kTouchStage / 27);  // a solo round never spills
+  J.solo_max = std::min<uint32_t>(tune.solo_max, kSoloCap);  // a solo round never spills
   // Cooperative grid: co-resident blocks, fewer for small jobs (a barrier
   // over fewer blocks is faster and a small bucket does not fill many).
   const void* kern = sign == M2S_SIGN_RAYCAST ? propagate_kernel<M2S_SIGN_RAYCAST>(J.multi)
