@@ -168,11 +168,11 @@ void m2s_clear_grid_autotune(void);
 /* Process-wide grid knobs; they change speed, never results.  blocks_per_sm:
  * cooperative propagation blocks per SM (0 = occupancy limit);
  * cells_per_block: the propagation launch uses ceil(cells / this) blocks, at
- * least 8 (0 = 2048); wave_cells: a batch runs as jobs of at most this many
+ * least one per SM (0 = 1024); wave_cells: a batch runs as jobs of at most this many
  * cells, largest grids first (a larger grid alone), so each job's working set
  * stays near L2 size (0 = 4M); solo_max: propagation rounds of at most this
  * many states run on one block with block barriers only (0 = never, negative
- * = the default 64). */
+ * = the default 64, at most 64). */
 void m2s_set_grid_tuning(int blocks_per_sm, uint32_t cells_per_block, uint64_t wave_cells, int solo_max);
 
 /* generate_sdf with AccelerationMethod::None for callers that cannot allocate

@@ -94,14 +94,25 @@ int upload_mesh(const float* vertices, uint64_t nv, const void* indices, uint64_
   return M2S_OK;
 }
 
+// A pinned status word per host thread, allocated once: freeing pinned memory
+// waits for the whole device, which would stall a caller's other streams.
+struct PinnedWord {
+  uint32_t* p = nullptr;
+  ~PinnedWord() {
+    if (p) cudaFreeHost(p);
+  }
+};
+
 struct StatusWord {
   DevBuf<uint32_t> d;
   uint32_t* h = nullptr;
   int init(cudaStream_t s) {
+    thread_local PinnedWord pw;
+    if (!pw.p) M2S_CUDA(cudaMallocHost(&pw.p, 4));
+    h = pw.p;
     int st = d.alloc(1, s);
     if (st) return st;
     M2S_CUDA(cudaMemsetAsync(d.p, 0, 4, s));
-    M2S_CUDA(cudaMallocHost(&h, 4));
     *h = 0;
     return M2S_OK;
   }
@@ -110,9 +121,6 @@ struct StatusWord {
     M2S_CUDA(cudaMemcpyAsync(h, d.p, 4, cudaMemcpyDeviceToHost, s));
     M2S_CUDA(cudaStreamSynchronize(s));
     return status_from_bits(*h);
-  }
-  ~StatusWord() {
-    if (h) cudaFreeHost(h);
   }
 };
 

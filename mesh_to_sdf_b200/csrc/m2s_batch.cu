@@ -342,7 +342,7 @@ void m2s_grid_plan_free(m2s_grid_plan* plan) {
 
 void m2s_set_grid_tuning(int blocks_per_sm, uint32_t cells_per_block, uint64_t wave_cells, int solo_max) {
   g_grid_tuning.blocks_per_sm = blocks_per_sm > 0 ? blocks_per_sm : 0;
-  g_grid_tuning.cells_per_block = cells_per_block ? cells_per_block : 2048;
+  g_grid_tuning.cells_per_block = cells_per_block ? cells_per_block : 1024;
   g_grid_tuning.wave_cells = wave_cells ? wave_cells : (4ull << 20);
   g_grid_tuning.solo_max = solo_max < 0 ? 64u : (uint32_t)solo_max;
 }

@@ -156,7 +156,7 @@ int grid_sdf(const MeshView& m, const GridDesc& g, int sign, float* d_out, uint3
 // Knobs that change speed, never results.
 struct GridTuning {
   int blocks_per_sm = 0;             // cooperative blocks per SM (0: occupancy limit)
-  uint32_t cells_per_block = 2048;   // cooperative grid = ceil(cells / this) blocks, at least 8
+  uint32_t cells_per_block = 1024;   // cooperative grid = ceil(cells / this) blocks, at least one per SM
   uint32_t list_capacity = 0;        // entries per bucket list (0: derived from the cell count)
   // A batch runs as jobs ("waves") of at most this many cells each (a larger
   // grid alone), so a job's 16 bytes of keys per cell stay near L2 size.

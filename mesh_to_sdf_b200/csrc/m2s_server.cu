@@ -11,11 +11,12 @@
 //  * points: each request is copied in, queried and copied out on one of a
 //    pool of streams, so requests on different meshes overlap on the device;
 //    completions are picked up from CUDA events;
-//  * grids: every grid request waiting when the previous batch finishes joins
-//    the next batch, computed as waves of the batched grid job.  A grid's
-//    values in a batch are bit-identical to computing it alone, and a point
-//    request runs exactly the kernels of m2s_query_sdf, so every result is the
-//    same alone and in the mix.
+//  * grids: the grid requests waiting when the previous batch finishes join
+//    the next batch (up to four waves' worth of cells), computed as the
+//    batched grid job's waves, smallest wave first; a wave's requests complete
+//    when it is done.  A grid's values in a batch are bit-identical to
+//    computing it alone, and a point request runs exactly the kernels of
+//    m2s_query_sdf, so every result is the same alone and in the mix.
 //
 // Admission: every request reserves an estimate of the device memory it will
 // hold (workspace and outputs; a mesh's resident structure for an upload)
@@ -91,6 +92,9 @@ uint64_t upload_bytes(uint64_t tris, uint64_t nv, uint64_t ni, int bits, int acc
 // A point request: queries in and results out (16 B), Morton keys and order
 // with their sort buffers, and the continuation list of the two-pass query.
 uint64_t point_bytes(uint64_t nq) { return 64 * nq + (1u << 20); }
+
+// Largest grid batch, in waves of the batched job.
+constexpr uint64_t kBatchWaves = 4;
 
 }  // namespace
 
@@ -330,11 +334,17 @@ void m2s_server::grid_loop() {
   for (;;) {
     std::vector<RequestP> batch;
     std::vector<MeshView> views;
+    const GridTuning tune = g_grid_tuning;
+    const uint64_t wave_cells = tune.wave_cells ? tune.wave_cells : (4ull << 20);
     {
       std::unique_lock<std::mutex> lk(mu);
       cv_work.wait(lk, [&] { return stop || head_ready(kGrid); });
       if (stop) break;
-      // Everything waiting that fits joins the batch, in arrival order.
+      // What waits joins the batch, in arrival order, up to kBatchWaves
+      // waves' worth of cells (a larger grid alone): a batch's requests
+      // complete wave by wave, and a bounded batch keeps the wait of a
+      // request that arrives during one bounded too.
+      uint64_t cells = 0;
       while (!q[kGrid].empty()) {
         RequestP r = q[kGrid].front();
         auto it = meshes.find(r->mesh_id);
@@ -345,45 +355,65 @@ void m2s_server::grid_loop() {
         }
         if (!it->second.mesh || !fits(r->need)) break;
         if (!batch.empty() && r->grid_sign != batch.front()->grid_sign) break;  // one sign per batch
+        if (!batch.empty() && cells + r->cells > kBatchWaves * wave_cells) break;
         q[kGrid].pop_front();
         reserve(r->need);
         it->second.last_use = ++clock;
         batch.push_back(r);
         views.push_back(it->second.mesh->mesh.view());
+        cells += r->cells;
       }
     }
     if (batch.empty()) continue;
     std::vector<GridDesc> grids;
-    uint64_t cells = 0;
-    for (auto& r : batch) {
-      grids.push_back(r->grid);
-      cells += r->cells;
-    }
-    int st = M2S_OK;
-    {
-      DevBuf<float> dout;
-      DevBuf<uint32_t> dst;
-      if (!(st = dout.alloc(cells, s_grid)) && !(st = dst.alloc(1, s_grid))) {
-        if (cudaMemsetAsync(dst.p, 0, 4, s_grid) != cudaSuccess) st = M2S_ERR_CUDA;
-        if (!st)
-          st = grid_sdf_batch(views.data(), (uint32_t)batch.size(), grids.data(), batch.front()->grid_sign, dout.p,
-                              dst.p, s_grid, nullptr, nullptr, g_grid_tuning);
-        uint64_t off = 0;
-        for (auto& r : batch) {
-          if (!st && cudaMemcpyAsync(r->out, dout.p + off, 4 * r->cells, cudaMemcpyDeviceToHost, s_grid) != cudaSuccess)
-            st = M2S_ERR_CUDA;
-          off += r->cells;
-        }
-        if (!st && cudaMemcpyAsync(h_status, dst.p, 4, cudaMemcpyDeviceToHost, s_grid) != cudaSuccess) st = M2S_ERR_CUDA;
-        if (cudaStreamSynchronize(s_grid) != cudaSuccess && !st) st = M2S_ERR_CUDA;
-        if (!st) st = status_from_bits(*h_status);
+    for (auto& r : batch) grids.push_back(r->grid);
+    // Waves as the batched job forms them, run smallest first: the requests
+    // of a wave complete as soon as it is done.
+    auto waves = plan_waves(grids.data(), (uint32_t)batch.size(), wave_cells);
+    auto wave_size = [&](const std::vector<uint32_t>& w) {
+      uint64_t c = 0;
+      for (uint32_t k : w) c += batch[k]->cells;
+      return c;
+    };
+    std::stable_sort(waves.begin(), waves.end(),
+                     [&](const auto& a, const auto& b) { return wave_size(a) < wave_size(b); });
+    for (const auto& w : waves) {
+      std::vector<MeshView> wv;
+      std::vector<GridDesc> wg;
+      for (uint32_t k : w) {
+        wv.push_back(views[k]);
+        wg.push_back(grids[k]);
       }
+      int st = M2S_OK;
+      {
+        DevBuf<float> dout;
+        DevBuf<uint32_t> dst;
+        if (!(st = dout.alloc(wave_size(w), s_grid)) && !(st = dst.alloc(1, s_grid))) {
+          if (cudaMemsetAsync(dst.p, 0, 4, s_grid) != cudaSuccess) st = M2S_ERR_CUDA;
+          if (!st)
+            st = grid_sdf_batch(wv.data(), (uint32_t)w.size(), wg.data(), batch.front()->grid_sign, dout.p, dst.p,
+                                s_grid, nullptr, nullptr, tune);
+          uint64_t off = 0;
+          for (uint32_t k : w) {
+            const RequestP& r = batch[k];
+            if (!st && cudaMemcpyAsync(r->out, dout.p + off, 4 * r->cells, cudaMemcpyDeviceToHost, s_grid) !=
+                           cudaSuccess)
+              st = M2S_ERR_CUDA;
+            off += r->cells;
+          }
+          if (!st && cudaMemcpyAsync(h_status, dst.p, 4, cudaMemcpyDeviceToHost, s_grid) != cudaSuccess)
+            st = M2S_ERR_CUDA;
+          if (cudaStreamSynchronize(s_grid) != cudaSuccess && !st) st = M2S_ERR_CUDA;
+          if (!st) st = status_from_bits(*h_status);
+        }
+      }
+      std::lock_guard<std::mutex> lk(mu);
+      for (uint32_t k : w) finish(batch[k], st);
     }
     std::lock_guard<std::mutex> lk(mu);
     ++grid_batches;
     grid_batched += batch.size();
     max_batch = std::max<uint64_t>(max_batch, batch.size());
-    for (auto& r : batch) finish(r, st);
   }
   cudaStreamSynchronize(s_grid);
   cudaFreeHost(h_status);
