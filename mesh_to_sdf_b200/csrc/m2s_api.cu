@@ -44,6 +44,12 @@ int current_pool(cudaMemPool_t* out) {
     // Keep freed blocks cached in the pool between calls.
     uint64_t keep = UINT64_MAX;
     cudaMemPoolSetAttribute(g_pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+    // A block freed on one stream is not handed to another stream before the
+    // free has run: otherwise the pool makes the new stream wait for the old
+    // one's queued work, and independent callers (a point query and a grid
+    // job on their own streams) wait for each other.
+    int no = 0;
+    cudaMemPoolSetAttribute(g_pools[dev], cudaMemPoolReuseAllowInternalDependencies, &no);
     g_pool_ready[dev] = true;
   }
   *out = g_pools[dev];
