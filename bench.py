@@ -275,8 +275,9 @@ def main():
         pass
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     # Algorithmic bytes of a relax round: per relaxed state its entry (8 B) and
-    # triangle record (48 B); per neighbour evaluation the neighbour's snapshot
-    # key read (8 B) and its working key (8 B).
+    # triangle record (48 B); per neighbour proposal (the on-grid cells of the
+    # 26 around the state) the neighbour's snapshot key read (8 B) and its
+    # working key (8 B).
     relax_bytes = stats["states_relaxed"] * 56 + stats["neighbour_evals"] * 16
     prop_s = phases["propagation"] / 1e3
     achieved = relax_bytes / prop_s / 1e9 if prop_s > 0 else 0.0

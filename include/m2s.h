@@ -284,7 +284,9 @@ int m2s_radix_sort_pairs_device(uint32_t* d_keys, uint32_t* d_values, uint64_t n
                                 void* stream);
 
 /* Diagnostics of the last grid call on this thread: [seed updates, relax
- * rounds, states relaxed, neighbour evaluations, ray hits, propagation
+ * rounds, states relaxed, neighbour proposals (the on-grid cells of the 26
+ * around each relaxed state; a Normal proposal to a cell that already holds
+ * its triangle is counted but not evaluated), ray hits, propagation
  * restarts, kernel launches, far-list redistributions, rounds relaxed by one
  * block alone, largest bucket list relaxed in one round]. */
 int m2s_last_grid_stats(uint64_t out[10]);

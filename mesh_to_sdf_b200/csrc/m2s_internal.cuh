@@ -145,7 +145,7 @@ struct GridDesc {
   }
 };
 
-// stats: [seed updates, relax rounds, states relaxed, neighbour evaluations,
+// stats: [seed updates, relax rounds, states relaxed, neighbour proposals,
 // ray hits, overflow restarts, kernel launches, far-list redistributions,
 // rounds relaxed by one block alone, largest list relaxed in one round].  phase_ms (may be NULL) receives device time of
 // [seeding, propagation, rays, finalize].
