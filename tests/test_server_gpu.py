@@ -8,7 +8,10 @@ Bars:
   * admission: a request larger than the whole budget is refused at
     submission; requests that fit one at a time but not together all complete,
     and the reserved bytes never exceed the budget;
-  * an upload that does not fit evicts an idle mesh, least recently used first.
+  * an upload that does not fit evicts an idle mesh, least recently used first;
+  * grid requests that queue up beyond one batch (more than four waves' worth
+    of cells) are split over several batches, and every grid still equals its
+    single-grid call bit for bit.
 """
 import numpy as np
 import pytest
@@ -137,5 +140,36 @@ def test_eviction_and_errors():
         assert e.value.status == 2
         with pytest.raises(m2s.M2SError):
             srv.submit_points(12345, np.zeros((4, 3), np.float32), np.empty(4, np.float32))
+    finally:
+        srv.close()
+
+
+def test_grid_backlog_spans_batches():
+    v, idx = synth.star(4, seed=21)
+    lo, hi = synth.padded_bbox(v)
+    srv = m2s.Server(64 << 30, point_streams=2)
+    import torch
+
+    try:
+        mid, t = srv.submit_upload(v, T.TriangleList(idx), A.rtree_bvh())
+        assert srv.wait(t)[0] == 0
+        # 12 grids of 96^3..176^3 (about 32M cells): more than one batch of four
+        # 4M-cell waves, submitted without waiting
+        edges = [96, 176, 128, 160, 112, 144, 176, 96, 128, 160, 144, 112]
+        jobs = []
+        for k, e in enumerate(edges):
+            grid = m2s.Grid.from_bounding_box(lo, hi, [e, e - 8, e + 8])
+            sign = S.Normal if k % 4 == 3 else S.Raycast
+            out = np.full(grid.get_total_cell_count(), np.nan, np.float32)
+            jobs.append((grid, sign, out, srv.submit_grid(mid, grid, sign, out)))
+        single = m2s.build_sdf_acceleration(v, T.TriangleList(idx), A.none())
+        for grid, sign, out, t in jobs:
+            assert srv.wait(t)[0] == 0
+            d = torch.empty(grid.get_total_cell_count(), dtype=torch.float32, device="cuda")
+            single.grid_device(grid, sign, d)
+            assert np.array_equal(bits(out), bits(d.cpu().numpy()))
+        st = srv.stats()
+        assert st["grid_requests"] == len(edges) and st["failed"] == 0
+        assert st["grid_batches"] >= 3  # at most four waves of cells per batch
     finally:
         srv.close()
