@@ -152,6 +152,46 @@ def run_cpu_grid(v, idx, g, threads):
     return time.perf_counter() - t
 
 
+def grid_accuracy(v, idx, grid, gpu, threads, n_sample=10_000):
+    """Accuracy of the GPU grid against the oracle (reported, not timed): the
+    restatement's own grid on all host threads (cells whose value or sign
+    differ; the reference's propagation is order-dependent, so values may
+    differ where triangles tie), and an FP64 brute force on seeded sample cells
+    (max / RMS distance error, sign mismatches, those at cells within 1e-5 of
+    the bbox diagonal of the surface counted apart as ambiguous)."""
+    import oracle
+
+    ref = oracle.generate_grid_sdf(v, idx, grid.first_cell, grid.cell_size, grid.cell_count, "raycast",
+                                   n_threads=threads)
+    ga, ra = np.abs(gpu), np.abs(ref)
+    differ = ga.view(np.uint32) != ra.view(np.uint32)
+    cell_diag = float(np.linalg.norm(grid.cell_size.astype(np.float64)))
+    nx, ny, nz = (int(c) for c in grid.cell_count)
+    rng = np.random.default_rng(SEED + 3)
+    cells = rng.choice(len(gpu), n_sample, replace=False)
+    ijk = np.stack([cells // (ny * nz), (cells // nz) % ny, cells % nz], axis=1)
+    centres = (grid.first_cell.astype(np.float32) + ijk.astype(np.float32) * grid.cell_size.astype(np.float32))
+    d64, inside64 = oracle.generate_sdf_f64(v, idx, centres.astype(np.float32), n_threads=threads)
+    lo, hi = synth_bbox(v)
+    diag = float(np.linalg.norm(hi - lo))
+    err = np.abs(np.abs(gpu[cells].astype(np.float64)) - d64)
+    flip = np.signbit(gpu[cells]) != inside64.astype(bool)
+    near = d64 <= 1e-5 * diag
+    return {"restatement": {"cells": int(len(gpu)), "value_differs": int(differ.sum()),
+                            "value_differs_frac": float(differ.mean()),
+                            "sign_differs": int((np.signbit(gpu) != np.signbit(ref)).sum()),
+                            "max_value_diff_cell_diagonals": float((np.abs(ga.astype(np.float64) - ra)).max() / cell_diag),
+                            "threads": threads},
+            "fp64": {"sample_cells": n_sample, "max_err": float(err.max()), "rms_err": float(np.sqrt(np.mean(err ** 2))),
+                     "max_err_rel_bbox_diag": float(err.max() / diag),
+                     "sign_mismatch": int((flip & ~near).sum()), "sign_mismatch_ambiguous": int((flip & near).sum())}}
+
+
+def synth_bbox(v):
+    v = np.asarray(v, np.float64)
+    return v.min(axis=0), v.max(axis=0)
+
+
 def reference_arm(args, world, rank):
     """The reference's CPU path (its C++ restatement; cargo is not on this image), all host cores."""
     if rank != 0:
@@ -390,13 +430,14 @@ def main():
                                  "watertight": verdict is None}
 
     # ---- CPU baseline (rank 0, N = 1 only): the oracle port on a bounded sample
-    cpu = None
+    cpu = accuracy = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         slab = cpu_slab(grid)
         cores = os.cpu_count() or 1
         sec = run_cpu_grid(v, idx, slab, cores)
         cpu = {"value": slab.get_total_cell_count() / sec, "unit": "cells/s", "cores": cores, "kind": "port",
                "sample": "256x256x32 middle z-slab (2.1M cells) of the 256^3 grid, C++ restatement, all host threads"}
+        accuracy = grid_accuracy(v, idx, grid, out.cpu().numpy(), cores)
 
     if rank == 0:
         line = {"metric": "SDF cells/s (generate_grid_sdf, Raycast)", "value": value, "unit": "cells/s",
@@ -407,7 +448,8 @@ def main():
                            "sign": "Raycast", "parallelism": f"replicas x{world}",
                            "l2": "flushed between steps (256 MiB write, untimed)"},
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": int(launches),
-                "clocks": clk.summary(), "points": points, "results": results, "wall_s_timed": t_wall}
+                "clocks": clk.summary(), "points": points, "results": results, "accuracy": accuracy,
+                "wall_s_timed": t_wall}
         print(json.dumps(line), flush=True)
     mesh.close()
     if world > 1:
