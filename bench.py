@@ -403,6 +403,14 @@ def main():
             points[name] = {"points": n, "ms": ms, "pts_per_s": n / (ms / 1e3)}
             if name.startswith("none"):
                 points[name]["pairs_per_s"] = n * T / (ms / 1e3)
+            else:  # traversal counts per query, from one profiled (untimed) run
+                m2s.set_profiling(True)
+                acc.query_device(qq, qo, status, stream)
+                torch.cuda.synchronize()
+                qs = m2s.last_query_stats()
+                m2s.set_profiling(False)
+                points[name]["per_query"] = {k[:-len("_per_query")]: round(v_, 2) for k, v_ in qs.items()
+                                             if k.endswith("_per_query")}
             acc.close()
         assert int(status.item()) == 0
 

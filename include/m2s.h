@@ -296,6 +296,15 @@ int m2s_last_grid_stats(uint64_t out[10]);
  * 342-346 and 369-373 — readable with m2s_last_grid_phase_ms as
  * [seeding, propagation, rays, finalize] in milliseconds. */
 void m2s_set_profiling(int enable);
+
+/* Traversal counts of the last point query made on this thread with
+ * profiling on (LBVH methods; no counterpart in the reference):
+ * [queries, nearest-triangle search node fetches, search triangle tests,
+ * sign-step node fetches, sign-step triangle tests].  The sign step is the
+ * three axis rays (Bvh Raycast, RtreeBvh) or the Normal tie band (Bvh
+ * Normal); Rtree has none.  Counting runs separate kernel instantiations and
+ * reads the totals back, so a profiled query synchronises its stream. */
+int m2s_last_query_stats(uint64_t out[5]);
 int m2s_last_grid_phase_ms(float out[4]);
 /* With profiling on, the last grid call on this thread also records its
  * propagation steps in order, two words each: the step — the number of states

@@ -288,6 +288,21 @@ def last_grid_stats():
     return dict(zip(GRID_STATS, (int(x) for x in a)))
 
 
+QUERY_STATS = ("queries", "search_node_fetches", "search_triangle_tests", "sign_node_fetches", "sign_triangle_tests")
+
+
+def last_query_stats():
+    """With profiling on (set_profiling): traversal counts of the last point
+    query on this thread (names in QUERY_STATS), plus per-query averages."""
+    a = np.zeros(len(QUERY_STATS), np.uint64)
+    _lib.lib().m2s_last_query_stats(_vp(a))
+    d = dict(zip(QUERY_STATS, (int(x) for x in a)))
+    n = max(d["queries"], 1)
+    for k in QUERY_STATS[1:]:
+        d[k + "_per_query"] = d[k] / n
+    return d
+
+
 def last_grid_round_log():
     """With profiling on: the last grid call's propagation steps in order, as
     (kind, size, t_ns) rows — kind 0 a relax round on every block, 2 a relax

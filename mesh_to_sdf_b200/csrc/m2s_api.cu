@@ -22,6 +22,7 @@ thread_local std::string t_last_error;
 thread_local uint64_t t_grid_stats[kGridStats];
 thread_local float t_grid_phase_ms[4];
 thread_local bool t_profile = false;
+thread_local uint64_t t_query_stats[5];
 thread_local std::vector<uint32_t> t_round_log;
 
 std::mutex g_pool_mu;
@@ -177,6 +178,12 @@ void record_grid_stats(const uint64_t stats[kGridStats]) {
 
 float* grid_phase_slot() { return t_profile ? t_grid_phase_ms : nullptr; }
 
+bool profiling_enabled() { return t_profile; }
+
+void record_query_stats(const uint64_t stats[5]) {
+  for (int i = 0; i < 5; ++i) t_query_stats[i] = stats[i];
+}
+
 void record_round_log(const std::vector<uint32_t>& log) { t_round_log = log; }
 
 int dev_alloc(void** p, size_t bytes, cudaStream_t s) {
@@ -249,6 +256,12 @@ int m2s_last_grid_stats(uint64_t out[10]) {
 }
 
 void m2s_set_profiling(int enable) { t_profile = enable != 0; }
+
+int m2s_last_query_stats(uint64_t out[5]) {
+  if (!out) return M2S_ERR_INVALID_ARGUMENT;
+  for (int i = 0; i < 5; ++i) out[i] = t_query_stats[i];
+  return M2S_OK;
+}
 
 uint32_t m2s_last_grid_round_log(uint32_t* out, uint32_t capacity) {
   const uint32_t n = (uint32_t)(t_round_log.size() / 2);

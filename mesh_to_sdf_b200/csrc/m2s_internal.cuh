@@ -126,6 +126,13 @@ int query_points(const MeshView& m, int accel, int sign, const float* d_q, uint6
 // continued one warp per query (0 disables the second pass).
 extern uint32_t g_query_budget;
 
+// Profiling (m2s_set_profiling, per host thread): whether it is on, and the
+// traversal counts of the last point query made with it on:
+// [queries, search node fetches, search triangle tests, sign node fetches,
+// sign triangle tests].
+bool profiling_enabled();
+void record_query_stats(const uint64_t stats[5]);
+
 // allow_alloc = false keeps the brute force in one pass with no scratch buffer.
 int brute_force_sdf(const MeshView& m, int sign, const float* d_q, uint64_t nq, float* d_out,
                     uint32_t* d_status, cudaStream_t s, bool allow_alloc = true);

@@ -168,15 +168,24 @@ struct Nearest {
   uint32_t leaf;  // LBVH leaf position
 };
 
+// Traversal counts of one query, kept only by the STATS instantiations
+// (profiling): nearest-triangle search node fetches and triangle tests, and
+// the same for the sign step (the three axis rays, or the Normal tie band).
+struct QCount {
+  uint32_t visits = 0, tests = 0, sign_visits = 0, sign_tests = 0;
+};
+
 // Exact nearest triangle under the f32 point_triangle_distance2 (geo.rs:33-37),
 // ties to the lowest triangle index.  Boxes are padded by 1e-4 (geo.rs:4-22),
 // which keeps the f32 box test conservative.  Starts from `best` (an upper
 // bound from an earlier, unfinished search, or +inf).  With a budget, the
 // search gives up after `budget` node visits and clears *finished; `best` is
 // then still a valid upper bound for a second pass.
+template <bool STATS = false>
 __device__ Nearest nearest_triangle(const MeshView& m, P3 p, bool* overflow, Nearest best = {INFINITY, 0xFFFFFFFFu, 0},
-                                    uint32_t budget = 0xFFFFFFFFu, bool* finished = nullptr) {
+                                    uint32_t budget = 0xFFFFFFFFu, bool* finished = nullptr, QCount* qc = nullptr) {
   auto eval = [&](uint32_t leaf) {
+    if constexpr (STATS) ++qc->tests;
     TriRec r = load_tri(m.stris, leaf);
     float d2 = point_triangle_distance2(p, p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
     uint32_t idx = __float_as_uint(r.b.w);
@@ -197,6 +206,7 @@ __device__ Nearest nearest_triangle(const MeshView& m, P3 p, bool* overflow, Nea
       *finished = false;
       break;
     }
+    if constexpr (STATS) ++qc->visits;
     BvhNode nd = load_node(m.nodes, node);
     float dl = box_dist2(p, nd.l_lo, nd.l_hi), dr = box_dist2(p, nd.r_lo, nd.r_hi);
     uint32_t L = __float_as_uint(nd.l_lo.w), R = __float_as_uint(nd.l_hi.w);
@@ -266,7 +276,9 @@ __device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v)
 // search on one lane).
 constexpr int kWarpStack = 2048;
 
-__device__ bool nearest_triangle_warp(const MeshView& m, P3 p, Nearest* io, uint32_t* s_node, float* s_dist) {
+template <bool STATS = false>
+__device__ bool nearest_triangle_warp(const MeshView& m, P3 p, Nearest* io, uint32_t* s_node, float* s_dist,
+                                      QCount* qc = nullptr) {
   const int lane = threadIdx.x & 31;
   // Non-negative d2 (or +inf / NaN-free boxes) order like their bits.
   unsigned long long best = nn_key(io->d2, io->tri);
@@ -296,6 +308,7 @@ __device__ bool nearest_triangle_warp(const MeshView& m, P3 p, Nearest* io, uint
     unsigned long long cand = ~0ull;
     uint32_t cand_leaf = 0;
     if (node != 0xFFFFFFFFu && nd2 <= bound) {
+      if constexpr (STATS) ++qc->visits;
       BvhNode nd = load_node(m.nodes, node);
       const uint32_t ch[2] = {__float_as_uint(nd.l_lo.w), __float_as_uint(nd.l_hi.w)};
       const float cd[2] = {box_dist2(p, nd.l_lo, nd.l_hi), box_dist2(p, nd.r_lo, nd.r_hi)};
@@ -304,6 +317,7 @@ __device__ bool nearest_triangle_warp(const MeshView& m, P3 p, Nearest* io, uint
         if (!(cd[c] <= bound)) continue;
         if (ch[c] & LEAF_BIT) {
           const uint32_t leaf = ch[c] & ~LEAF_BIT;
+          if constexpr (STATS) ++qc->tests;
           TriRec r = load_tri(m.stris, leaf);
           float d2 = point_triangle_distance2(p, p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
           if (!(d2 <= d2)) continue;  // NaN distances never win
@@ -355,12 +369,13 @@ __device__ bool nearest_triangle_warp(const MeshView& m, P3 p, Nearest* io, uint
 
 // Number of triangles the +AXIS ray from o crosses (geo.rs:165-216).  A box is
 // entered when the ray's (y, z) lies inside it and its far side is ahead of o.
-template <int AXIS>
-__device__ uint32_t ray_crossings(const MeshView& m, P3 o, bool* overflow) {
+template <int AXIS, bool STATS = false>
+__device__ uint32_t ray_crossings(const MeshView& m, P3 o, bool* overflow, QCount* qc = nullptr) {
   constexpr int IY = (AXIS + 1) % 3, IZ = (AXIS + 2) % 3;
   const float oy = vget(o, IY), oz = vget(o, IZ), ox = vget(o, AXIS);
   uint32_t count = 0;
   auto test = [&](uint32_t leaf) {
+    if constexpr (STATS) ++qc->sign_tests;
     TriRec r = load_tri(m.stris, leaf);
     float t;
     count += ray_hit_aligned<AXIS>(o, p3(r.a), p3(r.b), p3(r.c), &t) ? 1u : 0u;
@@ -379,6 +394,7 @@ __device__ uint32_t ray_crossings(const MeshView& m, P3 o, bool* overflow) {
   int sp = 0;
   uint32_t node = 0;
   while (true) {
+    if constexpr (STATS) ++qc->sign_visits;
     BvhNode nd = load_node(m.nodes, node);
     uint32_t L = __float_as_uint(nd.l_lo.w), R = __float_as_uint(nd.l_hi.w);
     bool goL = inside(nd.l_lo, nd.l_hi), goR = inside(nd.r_lo, nd.r_hi);
@@ -411,9 +427,10 @@ __device__ uint32_t ray_crossings(const MeshView& m, P3 o, bool* overflow) {
 }
 
 // bvh.rs:293-328 / rtree_bvh.rs:163-199: inside when >= 2 of 3 axis rays are odd.
-__device__ __forceinline__ bool vote_inside(const MeshView& m, P3 p, bool* overflow) {
-  int insides = (ray_crossings<0>(m, p, overflow) & 1u) + (ray_crossings<1>(m, p, overflow) & 1u) +
-                (ray_crossings<2>(m, p, overflow) & 1u);
+template <bool STATS = false>
+__device__ __forceinline__ bool vote_inside(const MeshView& m, P3 p, bool* overflow, QCount* qc = nullptr) {
+  int insides = (ray_crossings<0, STATS>(m, p, overflow, qc) & 1u) + (ray_crossings<1, STATS>(m, p, overflow, qc) & 1u) +
+                (ray_crossings<2, STATS>(m, p, overflow, qc) & 1u);
   return insides > 1;
 }
 
@@ -422,7 +439,8 @@ __device__ __forceinline__ bool vote_inside(const MeshView& m, P3 p, bool* overf
 // from f32::MAX with the rule of bvh.rs:277-279.
 constexpr int kBand = 32;
 
-__device__ float normal_band_fold(const MeshView& m, P3 p, float d2min, bool* nan, bool* overflow) {
+template <bool STATS = false>
+__device__ float normal_band_fold(const MeshView& m, P3 p, float d2min, bool* nan, bool* overflow, QCount* qc = nullptr) {
   const double band = sqrt((double)d2min) * (1.0 + 1e-5) + 4e-6;
   const float reach = (float)((band + 2e-4) * (1.0 + 1e-6));
   const float reach2 = reach * reach;
@@ -431,6 +449,7 @@ __device__ float normal_band_fold(const MeshView& m, P3 p, float d2min, bool* na
   int n = 0;
   bool full = false;
   auto consider = [&](const TriRec& r) {
+    if constexpr (STATS) ++qc->sign_tests;
     float d = point_triangle_signed_distance(p, p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
     if (!(fabs((double)d) <= band)) return;
     if (n < kBand) {
@@ -448,6 +467,7 @@ __device__ float normal_band_fold(const MeshView& m, P3 p, float d2min, bool* na
     int sp = 0;
     uint32_t node = 0;
     while (true) {
+      if constexpr (STATS) ++qc->sign_visits;
       BvhNode nd = load_node(m.nodes, node);
       uint32_t L = __float_as_uint(nd.l_lo.w), R = __float_as_uint(nd.l_hi.w);
       bool goL = box_dist2(p, nd.l_lo, nd.l_hi) <= reach2, goR = box_dist2(p, nd.r_lo, nd.r_hi) <= reach2;
@@ -517,9 +537,10 @@ struct HardQuery {
 };
 
 // Result of a query from its nearest triangle (and ray vote), per method.
-template <int MODE>
+template <int MODE, bool STATS = false>
 __device__ __forceinline__ void finish_query(const MeshView& m, uint64_t i, P3 p, Nearest nn, bool inside,
-                                             float* out, float* vec, uint8_t* inside_out, bool* nan, bool* overflow) {
+                                             float* out, float* vec, uint8_t* inside_out, bool* nan, bool* overflow,
+                                             QCount* qc = nullptr) {
   if (nn.tri == 0xFFFFFFFFu) nn = {INFINITY, 0u, 0u};  // every distance NaN
   if (MODE == Q_BVH_RAYCAST) {
     // bvh.rs:283-328 / rtree_bvh.rs:156-199: unsigned distance, 3-ray vote.
@@ -530,7 +551,7 @@ __device__ __forceinline__ void finish_query(const MeshView& m, uint64_t i, P3 p
     TriRec r = load_tri(m.tris, nn.tri);
     out[i] = point_triangle_signed_distance(p, p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
   } else if (MODE == Q_BVH_NORMAL) {
-    out[i] = normal_band_fold(m, p, nn.d2, nan, overflow);
+    out[i] = normal_band_fold<STATS>(m, p, nn.d2, nan, overflow, qc);
   } else {
     TriRec r = load_tri(m.tris, nn.tri);
     P3 cp = closest_point_triangle(p, p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
@@ -544,41 +565,54 @@ __device__ __forceinline__ void finish_query(const MeshView& m, uint64_t i, P3 p
 
 // Pass 1: one thread per query.  Searches that exceed `budget` node visits
 // are handed to pass 2 (k_query_hard) with their partial result.
-template <int MODE>
+// Adds a thread's traversal counts to qstats[0..3] (one atomic per warp).
+__device__ __forceinline__ void add_counts(const QCount& c, unsigned long long* qstats) {
+  const unsigned mask = __activemask();  // lanes past the last query have left
+  const unsigned v[4] = {__reduce_add_sync(mask, c.visits), __reduce_add_sync(mask, c.tests),
+                         __reduce_add_sync(mask, c.sign_visits), __reduce_add_sync(mask, c.sign_tests)};
+  if ((threadIdx.x & 31) == (unsigned)(__ffs(mask) - 1))
+    for (int f = 0; f < 4; ++f) atomicAdd(&qstats[f], (unsigned long long)v[f]);
+}
+
+template <int MODE, bool STATS = false>
 __global__ void __launch_bounds__(128) k_query(MeshView m, const float* __restrict__ q,
                                                const uint32_t* __restrict__ order, uint64_t nq,
                                                float* __restrict__ out, float* __restrict__ vec,
                                                uint8_t* __restrict__ inside_out, uint32_t* status, uint32_t budget,
-                                               HardQuery* hard, uint32_t* hard_count) {
+                                               HardQuery* hard, uint32_t* hard_count,
+                                               unsigned long long* qstats = nullptr) {
   uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nq) return;
   uint64_t i = order ? order[k] : k;
   P3 p = load_query(q, i);
   bool overflow = false, nan = false;
   bool inside = false;
-  if (MODE == Q_BVH_RAYCAST || MODE == Q_VECTOR) inside = vote_inside(m, p, &overflow);
+  QCount qc;
+  if (MODE == Q_BVH_RAYCAST || MODE == Q_VECTOR) inside = vote_inside<STATS>(m, p, &overflow, &qc);
   bool finished = true;
-  Nearest nn = nearest_triangle(m, p, &overflow, Nearest{INFINITY, 0xFFFFFFFFu, 0},
-                                (MODE == Q_BVH_NORMAL || !hard) ? 0xFFFFFFFFu : budget, &finished);
+  Nearest nn = nearest_triangle<STATS>(m, p, &overflow, Nearest{INFINITY, 0xFFFFFFFFu, 0},
+                                       (MODE == Q_BVH_NORMAL || !hard) ? 0xFFFFFFFFu : budget, &finished, &qc);
   if (finished) {
-    finish_query<MODE>(m, i, p, nn, inside, out, vec, inside_out, &nan, &overflow);
+    finish_query<MODE, STATS>(m, i, p, nn, inside, out, vec, inside_out, &nan, &overflow, &qc);
   } else {
     uint32_t pos = atomicAdd(hard_count, 1u);
     hard[pos] = HardQuery{(uint32_t)i, nn.d2, nn.tri, nn.leaf | (inside ? 0x80000000u : 0u)};
   }
   if (overflow) atomicOr(status, bit(M2S_ERR_LIMIT));
   if (nan) atomicOr(status, bit(M2S_ERR_NAN_DISTANCE));
+  if constexpr (STATS) add_counts(qc, qstats);
 }
 
 // Pass 2: one warp per hard query (see nearest_triangle_warp).
 constexpr int kHardWarps = 2;  // warps per block; each owns a kWarpStack-entry stack
 
-template <int MODE>
+template <int MODE, bool STATS = false>
 __global__ void __launch_bounds__(32 * kHardWarps) k_query_hard(MeshView m, const float* __restrict__ q,
                                                                const HardQuery* __restrict__ hard,
                                                                const uint32_t* hard_count, float* __restrict__ out,
                                                                float* __restrict__ vec, uint8_t* __restrict__ inside_out,
-                                                               uint32_t* status) {
+                                                               uint32_t* status, unsigned long long* qstats = nullptr) {
+  QCount qc;  // every lane's node fetches and tests of the warp searches
   __shared__ uint32_t s_node[kHardWarps][kWarpStack];
   __shared__ float s_dist[kHardWarps][kWarpStack];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -589,15 +623,16 @@ __global__ void __launch_bounds__(32 * kHardWarps) k_query_hard(MeshView m, cons
     const P3 p = load_query(q, hq.i);
     Nearest nn{hq.d2, hq.tri, hq.leaf_inside & 0x7FFFFFFFu};
     const bool inside = (hq.leaf_inside >> 31) != 0;
-    const bool ok = nearest_triangle_warp(m, p, &nn, s_node[w], s_dist[w]);
+    const bool ok = nearest_triangle_warp<STATS>(m, p, &nn, s_node[w], s_dist[w], &qc);
     if (lane == 0) {
-      if (!ok) nn = nearest_triangle(m, p, &overflow, nn);  // stack full: finish on one lane
-      finish_query<MODE>(m, hq.i, p, nn, inside, out, vec, inside_out, &nan, &overflow);
+      if (!ok) nn = nearest_triangle<STATS>(m, p, &overflow, nn, 0xFFFFFFFFu, nullptr, &qc);  // stack full: finish on one lane
+      finish_query<MODE, STATS>(m, hq.i, p, nn, inside, out, vec, inside_out, &nan, &overflow, &qc);
     }
     __syncwarp();
   }
   if (overflow) atomicOr(status, bit(M2S_ERR_LIMIT));
   if (nan) atomicOr(status, bit(M2S_ERR_NAN_DISTANCE));
+  if constexpr (STATS) add_counts(qc, qstats);
 }
 
 // Morton order of the queries (spatially coherent warps).
@@ -660,6 +695,40 @@ int brute_force_sdf(const MeshView& m, int sign, const float* d_q, uint64_t nq, 
   return M2S_OK;
 }
 
+namespace {
+template <bool ST>
+void launch_queries(int mode, const MeshView& m, const float* d_q, const uint32_t* ord, uint64_t nq, float* d_out,
+                    float* d_vec, uint8_t* d_inside, uint32_t* d_status, uint32_t budget, HardQuery* hp, uint32_t* hc,
+                    bool two_pass, unsigned blocks, unsigned long long* qs, cudaStream_t s) {
+  const unsigned hard_blocks = 148u * 32u;
+  switch (mode) {
+    case Q_BVH_RAYCAST:
+      k_query<Q_BVH_RAYCAST, ST><<<blocks, 128, 0, s>>>(m, d_q, ord, nq, d_out, nullptr, nullptr, d_status, budget, hp,
+                                                        hc, qs);
+      if (two_pass)
+        k_query_hard<Q_BVH_RAYCAST, ST><<<hard_blocks, 32 * kHardWarps, 0, s>>>(m, d_q, hp, hc, d_out, nullptr,
+                                                                                  nullptr, d_status, qs);
+      break;
+    case Q_BVH_NORMAL:
+      k_query<Q_BVH_NORMAL, ST><<<blocks, 128, 0, s>>>(m, d_q, ord, nq, d_out, nullptr, nullptr, d_status, budget,
+                                                       nullptr, nullptr, qs);
+      break;
+    case Q_RTREE:
+      k_query<Q_RTREE, ST><<<blocks, 128, 0, s>>>(m, d_q, ord, nq, d_out, nullptr, nullptr, d_status, budget, hp, hc, qs);
+      if (two_pass)
+        k_query_hard<Q_RTREE, ST><<<hard_blocks, 32 * kHardWarps, 0, s>>>(m, d_q, hp, hc, d_out, nullptr, nullptr,
+                                                                            d_status, qs);
+      break;
+    default:
+      k_query<Q_VECTOR, ST><<<blocks, 128, 0, s>>>(m, d_q, ord, nq, nullptr, d_vec, d_inside, d_status, budget, hp, hc,
+                                                   qs);
+      if (two_pass)
+        k_query_hard<Q_VECTOR, ST><<<hard_blocks, 32 * kHardWarps, 0, s>>>(m, d_q, hp, hc, nullptr, d_vec, d_inside,
+                                                                             d_status, qs);
+  }
+}
+}  // namespace
+
 int query_points(const MeshView& m, int accel, int sign, const float* d_q, uint64_t nq, float* d_out, float* d_vec,
                  uint8_t* d_inside, uint32_t* d_status, cudaStream_t s) {
   if (nq == 0) return M2S_OK;
@@ -693,30 +762,28 @@ int query_points(const MeshView& m, int accel, int sign, const float* d_q, uint6
   const uint32_t budget = g_query_budget;
   HardQuery* hp = two_pass ? hard.p : nullptr;
   uint32_t* hc = two_pass ? hard_count.p : nullptr;
-  const unsigned hard_blocks = 148u * 32u;
-  switch (mode) {
-    case Q_BVH_RAYCAST:
-      k_query<Q_BVH_RAYCAST><<<blocks, 128, 0, s>>>(m, d_q, ord, nq, d_out, nullptr, nullptr, d_status, budget, hp, hc);
-      if (two_pass)
-        k_query_hard<Q_BVH_RAYCAST><<<hard_blocks, 32 * kHardWarps, 0, s>>>(m, d_q, hp, hc, d_out, nullptr, nullptr,
-                                                                              d_status);
-      break;
-    case Q_BVH_NORMAL:
-      k_query<Q_BVH_NORMAL><<<blocks, 128, 0, s>>>(m, d_q, ord, nq, d_out, nullptr, nullptr, d_status, budget, nullptr,
-                                                   nullptr);
-      break;
-    case Q_RTREE:
-      k_query<Q_RTREE><<<blocks, 128, 0, s>>>(m, d_q, ord, nq, d_out, nullptr, nullptr, d_status, budget, hp, hc);
-      if (two_pass)
-        k_query_hard<Q_RTREE><<<hard_blocks, 32 * kHardWarps, 0, s>>>(m, d_q, hp, hc, d_out, nullptr, nullptr, d_status);
-      break;
-    default:
-      k_query<Q_VECTOR><<<blocks, 128, 0, s>>>(m, d_q, ord, nq, nullptr, d_vec, d_inside, d_status, budget, hp, hc);
-      if (two_pass)
-        k_query_hard<Q_VECTOR><<<hard_blocks, 32 * kHardWarps, 0, s>>>(m, d_q, hp, hc, nullptr, d_vec, d_inside,
-                                                                         d_status);
+  // With profiling on, the counting instantiations run and their totals are
+  // read back (a synchronisation, as profiling's phase timings are).
+  const bool counting = profiling_enabled();
+  DevBuf<unsigned long long> qs;
+  if (counting) {
+    if ((st = qs.alloc(4, s))) return st;
+    M2S_CUDA(cudaMemsetAsync(qs.p, 0, 32, s));
   }
+  if (counting)
+    launch_queries<true>(mode, m, d_q, ord, nq, d_out, d_vec, d_inside, d_status, budget, hp, hc, two_pass, blocks,
+                         qs.p, s);
+  else
+    launch_queries<false>(mode, m, d_q, ord, nq, d_out, d_vec, d_inside, d_status, budget, hp, hc, two_pass, blocks,
+                          nullptr, s);
   M2S_CUDA(cudaGetLastError());
+  if (counting) {
+    unsigned long long h[4];
+    M2S_CUDA(cudaMemcpyAsync(h, qs.p, 32, cudaMemcpyDeviceToHost, s));
+    M2S_CUDA(cudaStreamSynchronize(s));
+    const uint64_t rec[5] = {nq, h[0], h[1], h[2], h[3]};
+    record_query_stats(rec);
+  }
   return M2S_OK;
 }
 

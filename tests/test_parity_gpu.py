@@ -174,6 +174,28 @@ def test_large_batch_morton_order(orc):
         assert_bit_equal(m2s.generate_sdf(v, T.TriangleList(idx), q, am), orc_sdf(orc, v, idx, q, am), repr(am))
 
 
+def test_query_counting_changes_no_result():
+    # profiling runs the counting kernel instantiations: same bits, sane counts
+    v, idx = synth.star(4, seed=5)
+    q = synth.mixed_points(v, idx, 6000, seed=6)
+    for am in (A.bvh(S.Raycast), A.bvh(S.Normal), A.rtree(), A.rtree_bvh()):
+        acc = m2s.build_sdf_acceleration(v, T.TriangleList(idx), am)
+        plain = m2s.query_sdf(acc, q)
+        m2s.set_profiling(True)
+        try:
+            counted = m2s.query_sdf(acc, q)
+            st = m2s.last_query_stats()
+        finally:
+            m2s.set_profiling(False)
+        assert_bit_equal(counted, plain, repr(am))
+        assert st["queries"] == len(q), repr(am)
+        assert st["search_node_fetches"] >= len(q) and st["search_triangle_tests"] >= len(q), (repr(am), st)
+        if am.kind == A.RTREE:
+            assert st["sign_node_fetches"] == 0 and st["sign_triangle_tests"] == 0, st
+        else:
+            assert st["sign_node_fetches"] >= len(q), (repr(am), st)
+
+
 def test_fp64_error_report(orc):
     # north_star error report: distance error against an FP64 brute force
     v, idx = synth.star(4, seed=9)
