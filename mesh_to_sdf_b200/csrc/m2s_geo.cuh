@@ -161,6 +161,16 @@ __device__ __forceinline__ float point_triangle_signed_distance(P3 p, P3 a, P3 b
   return vdot(dir, n) > 0.0f ? d : -d;
 }
 
+// signed distance with the branch-free proper case.
+__device__ __forceinline__ float point_triangle_signed_distance_sel(P3 p, P3 a, P3 b, P3 c, int kind) {
+  P3 cp = kind == TRI_PROPER ? closest_point_proper_sel(p, a, b, c) : closest_point_triangle(p, a, b, c, kind);
+  P3 dir = vsub(p, cp);
+  P3 n = vcross(vsub(b, a), vsub(c, a));
+  float d = fsqrt(vdot(dir, dir));
+  return vdot(dir, n) > 0.0f ? d : -d;
+}
+
+
 // geo.rs:165-216 for a +axis ray; (y, z) of the projection rotate with the axis
 // as in the reference (X: y,z; Y: z,x; Z: x,y).  Returns true with *t on a hit.
 template <int AXIS>

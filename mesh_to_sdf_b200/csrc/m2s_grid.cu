@@ -216,7 +216,7 @@ __device__ __forceinline__ void snap(const GridK& g, P3 p, int cell[3]) {
 template <int SIGN>
 __device__ __forceinline__ float cell_distance(P3 pos, P3 a, P3 b, P3 c, int kind) {
   if (SIGN == M2S_SIGN_RAYCAST) return fsqrt(point_triangle_distance2_sel(pos, a, b, c, kind));
-  return point_triangle_signed_distance(pos, a, b, c, kind);
+  return point_triangle_signed_distance_sel(pos, a, b, c, kind);
 }
 
 __device__ __forceinline__ unsigned long long pack(float d, uint32_t tri) {
