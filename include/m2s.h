@@ -305,6 +305,14 @@ void m2s_set_profiling(int enable);
  * Normal); Rtree has none.  Counting runs separate kernel instantiations and
  * reads the totals back, so a profiled query synchronises its stream. */
 int m2s_last_query_stats(uint64_t out[5]);
+
+/* Diagnostics of the grid propagation's barrier bound (no counterpart in the
+ * reference): launches `blocks` blocks (1..64) that wait at one grid barrier
+ * expecting `expected` blocks (1..64).  With blocks == expected all pass; with
+ * fewer, every wait gives up after the barrier's two-second limit and raises
+ * the abort flag, and the kernel returns.  out[0] = blocks that passed,
+ * out[1] = blocks that gave up.  Synchronous. */
+int m2s_test_grid_barrier(uint32_t blocks, uint32_t expected, uint32_t out[2]);
 int m2s_last_grid_phase_ms(float out[4]);
 /* With profiling on, the last grid call on this thread also records its
  * propagation steps in order, two words each: the step — the number of states

@@ -496,6 +496,18 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* bar, unsigned int nblo
   return ok != 0;
 }
 
+// Diagnostics of the barrier's bound: the launched blocks wait at one grid
+// barrier that expects `expected` blocks.  With fewer launched, no block is
+// the last to arrive, every wait gives up after kBarrierTimeoutNs and the
+// abort flag is raised; result[0] counts blocks that passed, result[1] blocks
+// that gave up.
+__global__ void k_barrier_probe(GridBarrier* bar, unsigned int expected, unsigned int* result) {
+  __shared__ unsigned int gen;
+  if (threadIdx.x == 0) gen = 0;
+  const bool ok = grid_barrier(bar, expected, &gen);
+  if (threadIdx.x == 0) atomicAdd(&result[ok ? 0 : 1], 1u);
+}
+
 // Touched cells staged per block and round in shared memory; a block commits
 // the cells it touched itself, so only a block whose stage fills up writes to
 // the global spill list.
@@ -1689,3 +1701,22 @@ int grid_sdf(const MeshView& m, const GridDesc& gd, int sign, float* d_out, uint
 }
 
 }  // namespace m2s
+
+using namespace m2s;
+
+extern "C" int m2s_test_grid_barrier(uint32_t blocks, uint32_t expected, uint32_t out[2]) {
+  if (!out || blocks == 0 || blocks > 64 || expected == 0 || expected > 64) return M2S_ERR_INVALID_ARGUMENT;
+  int st;
+  if ((st = require_device())) return st;
+  cudaStream_t s = nullptr;
+  DevBuf<GridBarrier> bar;
+  DevBuf<unsigned int> res;
+  if ((st = bar.alloc(1, s)) || (st = res.alloc(2, s))) return st;
+  M2S_CUDA(cudaMemsetAsync(bar.p, 0, sizeof(GridBarrier), s));
+  M2S_CUDA(cudaMemsetAsync(res.p, 0, 8, s));
+  k_barrier_probe<<<blocks, 64, 0, s>>>(bar.p, expected, res.p);
+  M2S_CUDA(cudaGetLastError());
+  M2S_CUDA(cudaMemcpyAsync(out, res.p, 8, cudaMemcpyDeviceToHost, s));
+  M2S_CUDA(cudaStreamSynchronize(s));
+  return M2S_OK;
+}

@@ -187,3 +187,25 @@ def test_many_small_rounds_at_full_occupancy_are_deterministic():
             assert np.array_equal(bits(got), bits(ref)), (bps, cpb, wave, solo)
     finally:
         m2s.set_grid_tuning()
+
+
+def test_grid_barrier_wait_is_bounded():
+    # the propagation's grid barrier gives up after its time limit instead of
+    # waiting for blocks that never arrive (here: one block fewer than it
+    # expects), and the context stays usable
+    import time
+
+    L = m2s._lib.lib()
+    out = np.zeros(2, np.uint32)
+    assert L.m2s_test_grid_barrier(8, 8, out.ctypes.data) == 0
+    assert out.tolist() == [8, 0]
+    t0 = time.perf_counter()
+    assert L.m2s_test_grid_barrier(3, 4, out.ctypes.data) == 0
+    waited = time.perf_counter() - t0
+    assert out.tolist() == [0, 3]
+    assert 1.5 < waited < 30.0, waited
+    v, idx = synth.icosphere(2)
+    grid = m2s.Grid.from_bounding_box([-1.2] * 3, [1.2] * 3, [24, 24, 24])
+    a = m2s.generate_grid_sdf(v, T.TriangleList(idx), grid, S.Raycast)
+    b = m2s.generate_grid_sdf(v, T.TriangleList(idx), grid, S.Raycast)
+    assert np.array_equal(bits(a), bits(b))
