@@ -100,6 +100,8 @@ class ClockSampler:
 
 
 def dist_setup():
+    """One process per GPU (replicas): NCCL on GPUs; gloo where there is no
+    GPU, so the launch and the max-over-ranks plumbing run on CPU too."""
     import torch
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -108,9 +110,12 @@ def dist_setup():
     if world > 1:
         import datetime
 
-        torch.cuda.set_device(local)
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                             device_id=torch.device("cuda", local))
+        timeout = datetime.timedelta(seconds=120)
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            torch.distributed.init_process_group("nccl", timeout=timeout, device_id=torch.device("cuda", local))
+        else:
+            torch.distributed.init_process_group("gloo", timeout=timeout)
     return world, rank, local
 
 
@@ -119,7 +124,8 @@ def max_over_ranks(x: float, world: int) -> float:
         return x
     import torch
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if torch.distributed.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
     return float(t.item())
 
@@ -129,7 +135,8 @@ def barrier(world):
 
     if world > 1:
         torch.distributed.barrier()
-    torch.cuda.synchronize()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
 
 
 # --------------------------------------------------------------------------- CPU baseline
