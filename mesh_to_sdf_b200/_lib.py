@@ -6,7 +6,11 @@ import os
 import threading
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libm2s.so")
+# M2S_BUILD=fast selects the fast build (fused multiply-adds in the distance
+# arithmetic; distances within 4 ulp or 1e-6 of the bbox diagonal of the
+# strict build, same Raycast signs).  The default is the strict build.
+FAST = os.environ.get("M2S_BUILD", "strict") == "fast"
+LIB_PATH = os.path.join(_HERE, "libm2s_fast.so" if FAST else "libm2s.so")
 _lock = threading.Lock()
 _lib = None
 
@@ -79,9 +83,9 @@ def lib():
         if _lib is None:
             from . import build as _build
 
-            if not _build.up_to_date():
+            if not _build.up_to_date(FAST) and LIB_PATH == _build.lib_path(FAST):
                 try:
-                    _build.build()
+                    _build.build(fast=FAST)
                 except Exception as e:  # no nvcc: the prebuilt library must exist
                     if not os.path.exists(LIB_PATH):
                         raise LibraryMissing(f"libm2s.so is missing and cannot be built: {e}") from e

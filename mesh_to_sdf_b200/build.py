@@ -17,6 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libm2s.so")
+FAST_LIB = os.path.join(HERE, "libm2s_fast.so")
 ROOT = os.path.dirname(HERE)
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -41,22 +42,34 @@ def _deps():
     return hdrs
 
 
-def up_to_date() -> bool:
-    if not os.path.exists(LIB):
+def lib_path(fast: bool = False) -> str:
+    return FAST_LIB if fast else LIB
+
+
+def up_to_date(fast: bool = False) -> bool:
+    lib = lib_path(fast)
+    if not os.path.exists(lib):
         return False
-    t = os.path.getmtime(LIB)
+    t = os.path.getmtime(lib)
     return all(os.path.getmtime(f) <= t for f in sources() + _deps() + [__file__])
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and up_to_date():
-        return LIB
-    os.makedirs(BUILD, exist_ok=True)
+def build(force: bool = False, verbose: bool = False, fast: bool = False) -> str:
+    """The strict build (libm2s.so: every distance operation rounds like the
+    reference) or, with fast=True, the fast build (libm2s_fast.so: compiled
+    with M2S_FAST_MATH, multiply-adds fused in the closest-point and distance
+    arithmetic only)."""
+    lib = lib_path(fast)
+    if not force and up_to_date(fast):
+        return lib
+    bdir = os.path.join(BUILD, "fast") if fast else BUILD
+    os.makedirs(bdir, exist_ok=True)
     cc = nvcc()
+    defs = ["-DM2S_FAST_MATH"] if fast else []
 
     def compile_one(src):
-        obj = os.path.join(BUILD, os.path.basename(src) + ".o")
-        cmd = [cc, *ARCH, *FLAGS, "-c", src, "-o", obj]
+        obj = os.path.join(bdir, os.path.basename(src) + ".o")
+        cmd = [cc, *ARCH, *FLAGS, *defs, "-c", src, "-o", obj]
         if verbose:
             cmd += ["-Xptxas", "-v"]
         r = subprocess.run(cmd, capture_output=True, text=True)
@@ -70,14 +83,14 @@ def build(force: bool = False, verbose: bool = False) -> str:
         for _, err in results:
             sys.stderr.write(err)
     objs = [o for o, _ in results]
-    tmp = LIB + ".tmp"
+    tmp = lib + ".tmp"
     r = subprocess.run([cc, *ARCH, "-shared", "-o", tmp, *objs], capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, lib)
+    return lib
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose="--verbose" in sys.argv)
-    print(LIB)
+    fast = "--fast" in sys.argv
+    print(build(force="--force" in sys.argv, verbose="--verbose" in sys.argv, fast=fast))

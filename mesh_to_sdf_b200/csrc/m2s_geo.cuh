@@ -33,6 +33,26 @@ __device__ __forceinline__ P3 vcross(P3 a, P3 b) {
 }
 __device__ __forceinline__ float vget(P3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
 
+// Arithmetic of the closest-point and distance computations.  The default
+// (strict) build rounds every operation like the reference; the fast build
+// (M2S_FAST_MATH) lets the compiler fuse multiply-adds there, and only there:
+// ray-triangle tests, cell centres and the Normal sign's dot product stay
+// strict, so Raycast signs are the strict build's.  Division and square root
+// are IEEE in both.
+#ifdef M2S_FAST_MATH
+__device__ __forceinline__ float da(float a, float b) { return a + b; }
+__device__ __forceinline__ float ds(float a, float b) { return a - b; }
+__device__ __forceinline__ float dm(float a, float b) { return a * b; }
+#else
+__device__ __forceinline__ float da(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float ds(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float dm(float a, float b) { return __fmul_rn(a, b); }
+#endif
+__device__ __forceinline__ P3 dvsub(P3 a, P3 b) { return {ds(a.x, b.x), ds(a.y, b.y), ds(a.z, b.z)}; }
+__device__ __forceinline__ P3 dvadd(P3 a, P3 b) { return {da(a.x, b.x), da(a.y, b.y), da(a.z, b.z)}; }
+__device__ __forceinline__ P3 dvmul(P3 a, float s) { return {dm(a.x, s), dm(a.y, s), dm(a.z, s)}; }
+__device__ __forceinline__ float dvdot(P3 a, P3 b) { return da(da(dm(a.x, b.x), dm(a.y, b.y)), dm(a.z, b.z)); }
+
 // Rust f32::clamp: a NaN stays NaN.
 __device__ __forceinline__ float rs_clamp01(float v) {
   if (v < 0.0f) v = 0.0f;
@@ -58,40 +78,40 @@ __host__ __device__ __forceinline__ int degenerate_kind(float ax, float ay, floa
 
 // geo.rs:141-151
 __device__ __forceinline__ P3 closest_point_segment(P3 p, P3 a, P3 b) {
-  P3 ab = vsub(b, a);
-  float m = vdot(ab, ab);
-  P3 ap = vsub(p, a);
-  float s = rs_clamp01(fd(vdot(ab, ap), m));
-  return vadd(a, vmul(ab, s));
+  P3 ab = dvsub(b, a);
+  float m = dvdot(ab, ab);
+  P3 ap = dvsub(p, a);
+  float s = rs_clamp01(fd(dvdot(ab, ap), m));
+  return dvadd(a, dvmul(ab, s));
 }
 
 // geo.rs:70-138 (Embree Voronoi regions) for a proper triangle.
 __device__ __forceinline__ P3 closest_point_proper(P3 p, P3 a, P3 b, P3 c) {
-  P3 ab = vsub(b, a);
-  P3 ac = vsub(c, a);
-  P3 ap = vsub(p, a);
-  float d1 = vdot(ab, ap);
-  float d2 = vdot(ac, ap);
+  P3 ab = dvsub(b, a);
+  P3 ac = dvsub(c, a);
+  P3 ap = dvsub(p, a);
+  float d1 = dvdot(ab, ap);
+  float d2 = dvdot(ac, ap);
   if (d1 <= 0.0f && d2 <= 0.0f) return a;
-  P3 bp = vsub(p, b);
-  float d3 = vdot(ab, bp);
-  float d4 = vdot(ac, bp);
+  P3 bp = dvsub(p, b);
+  float d3 = dvdot(ab, bp);
+  float d4 = dvdot(ac, bp);
   if (d3 >= 0.0f && d4 <= d3) return b;
-  P3 cp = vsub(p, c);
-  float d5 = vdot(ab, cp);
-  float d6 = vdot(ac, cp);
+  P3 cp = dvsub(p, c);
+  float d5 = dvdot(ab, cp);
+  float d6 = dvdot(ac, cp);
   if (d6 >= 0.0f && d5 <= d6) return c;
-  float vc = fs(fm(d1, d4), fm(d3, d2));
-  if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) return vadd(a, vmul(ab, fd(d1, fs(d1, d3))));
-  float vb = fs(fm(d5, d2), fm(d1, d6));
-  if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) return vadd(a, vmul(ac, fd(d2, fs(d2, d6))));
-  float va = fs(fm(d3, d6), fm(d5, d4));
-  float d43 = fs(d4, d3), d56 = fs(d5, d6);
-  if (va <= 0.0f && d43 >= 0.0f && d56 >= 0.0f) return vadd(b, vmul(vsub(c, b), fd(d43, fa(d43, d56))));
-  float denom = fd(1.0f, fa(fa(va, vb), vc));
-  float v = fm(vb, denom);
-  float w = fm(vc, denom);
-  return vadd(vadd(a, vmul(ab, v)), vmul(ac, w));
+  float vc = ds(dm(d1, d4), dm(d3, d2));
+  if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) return dvadd(a, dvmul(ab, fd(d1, ds(d1, d3))));
+  float vb = ds(dm(d5, d2), dm(d1, d6));
+  if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) return dvadd(a, dvmul(ac, fd(d2, ds(d2, d6))));
+  float va = ds(dm(d3, d6), dm(d5, d4));
+  float d43 = ds(d4, d3), d56 = ds(d5, d6);
+  if (va <= 0.0f && d43 >= 0.0f && d56 >= 0.0f) return dvadd(b, dvmul(dvsub(c, b), fd(d43, da(d43, d56))));
+  float denom = fd(1.0f, da(da(va, vb), vc));
+  float v = dm(vb, denom);
+  float w = dm(vc, denom);
+  return dvadd(dvadd(a, dvmul(ab, v)), dvmul(ac, w));
 }
 
 // geo.rs:70-138 including the degenerate fallbacks (kind from degenerate_kind).
@@ -104,8 +124,8 @@ __device__ __forceinline__ P3 closest_point_triangle(P3 p, P3 a, P3 b, P3 c, int
 
 // geo.rs:33-37
 __device__ __forceinline__ float point_triangle_distance2(P3 p, P3 a, P3 b, P3 c, int kind) {
-  P3 d = vsub(p, closest_point_triangle(p, a, b, c, kind));
-  return vdot(d, d);
+  P3 d = dvsub(p, closest_point_triangle(p, a, b, c, kind));
+  return dvdot(d, d);
 }
 
 // closest_point_proper without branches: every dot product is formed, the
@@ -115,15 +135,15 @@ __device__ __forceinline__ float point_triangle_distance2(P3 p, P3 a, P3 b, P3 c
 // bit-identical; lanes of a warp in different regions no longer run every
 // region's path and division one after another.
 __device__ __forceinline__ P3 closest_point_proper_sel(P3 p, P3 a, P3 b, P3 c) {
-  const P3 ab = vsub(b, a), ac = vsub(c, a);
-  const P3 ap = vsub(p, a), bp = vsub(p, b), cp = vsub(p, c);
-  const float d1 = vdot(ab, ap), d2 = vdot(ac, ap);
-  const float d3 = vdot(ab, bp), d4 = vdot(ac, bp);
-  const float d5 = vdot(ab, cp), d6 = vdot(ac, cp);
-  const float vc = fs(fm(d1, d4), fm(d3, d2));
-  const float vb = fs(fm(d5, d2), fm(d1, d6));
-  const float va = fs(fm(d3, d6), fm(d5, d4));
-  const float d43 = fs(d4, d3), d56 = fs(d5, d6);
+  const P3 ab = dvsub(b, a), ac = dvsub(c, a);
+  const P3 ap = dvsub(p, a), bp = dvsub(p, b), cp = dvsub(p, c);
+  const float d1 = dvdot(ab, ap), d2 = dvdot(ac, ap);
+  const float d3 = dvdot(ab, bp), d4 = dvdot(ac, bp);
+  const float d5 = dvdot(ab, cp), d6 = dvdot(ac, cp);
+  const float vc = ds(dm(d1, d4), dm(d3, d2));
+  const float vb = ds(dm(d5, d2), dm(d1, d6));
+  const float va = ds(dm(d3, d6), dm(d5, d4));
+  const float d43 = ds(d4, d3), d56 = ds(d5, d6);
   const bool rA = d1 <= 0.0f && d2 <= 0.0f;
   const bool rB = d3 >= 0.0f && d4 <= d3;
   const bool rC = d6 >= 0.0f && d5 <= d6;
@@ -132,14 +152,14 @@ __device__ __forceinline__ P3 closest_point_proper_sel(P3 p, P3 a, P3 b, P3 c) {
   const bool eBC = !eAB && !eAC && va <= 0.0f && d43 >= 0.0f && d56 >= 0.0f;
   const bool face = !eAB && !eAC && !eBC;
   const float num = eAB ? d1 : (eAC ? d2 : (eBC ? d43 : 1.0f));
-  const float den = eAB ? fs(d1, d3) : (eAC ? fs(d2, d6) : (eBC ? fa(d43, d56) : fa(fa(va, vb), vc)));
+  const float den = eAB ? ds(d1, d3) : (eAC ? ds(d2, d6) : (eBC ? da(d43, d56) : da(da(va, vb), vc)));
   const float q = fd(num, den);
-  const P3 cb = vsub(c, b);
+  const P3 cb = dvsub(c, b);
   const P3 base = eBC ? b : a;
   const P3 e1 = eAC ? ac : (eBC ? cb : ab);
-  const float s1 = face ? fm(vb, q) : q;
-  P3 x = vadd(base, vmul(e1, s1));
-  const P3 x2 = vadd(x, vmul(ac, fm(vc, q)));
+  const float s1 = face ? dm(vb, q) : q;
+  P3 x = dvadd(base, dvmul(e1, s1));
+  const P3 x2 = dvadd(x, dvmul(ac, dm(vc, q)));
   if (face) x = x2;
   if (rA || rB || rC) x = rA ? a : (rB ? b : c);
   return x;
@@ -148,25 +168,25 @@ __device__ __forceinline__ P3 closest_point_proper_sel(P3 p, P3 a, P3 b, P3 c) {
 // point_triangle_distance2 with the branch-free proper case.
 __device__ __forceinline__ float point_triangle_distance2_sel(P3 p, P3 a, P3 b, P3 c, int kind) {
   const P3 cp = kind == TRI_PROPER ? closest_point_proper_sel(p, a, b, c) : closest_point_triangle(p, a, b, c, kind);
-  const P3 d = vsub(p, cp);
-  return vdot(d, d);
+  const P3 d = dvsub(p, cp);
+  return dvdot(d, d);
 }
 
 // geo.rs:43-56: positive when (p - closest) . (ab x ac) > 0, else -distance.
 __device__ __forceinline__ float point_triangle_signed_distance(P3 p, P3 a, P3 b, P3 c, int kind) {
   P3 cp = closest_point_triangle(p, a, b, c, kind);
-  P3 dir = vsub(p, cp);
+  P3 dir = dvsub(p, cp);
   P3 n = vcross(vsub(b, a), vsub(c, a));
-  float d = fsqrt(vdot(dir, dir));
+  float d = fsqrt(dvdot(dir, dir));
   return vdot(dir, n) > 0.0f ? d : -d;
 }
 
 // signed distance with the branch-free proper case.
 __device__ __forceinline__ float point_triangle_signed_distance_sel(P3 p, P3 a, P3 b, P3 c, int kind) {
   P3 cp = kind == TRI_PROPER ? closest_point_proper_sel(p, a, b, c) : closest_point_triangle(p, a, b, c, kind);
-  P3 dir = vsub(p, cp);
+  P3 dir = dvsub(p, cp);
   P3 n = vcross(vsub(b, a), vsub(c, a));
-  float d = fsqrt(vdot(dir, dir));
+  float d = fsqrt(dvdot(dir, dir));
   return vdot(dir, n) > 0.0f ? d : -d;
 }
 
