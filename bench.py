@@ -54,7 +54,9 @@ def grid_for(lo, hi, n=(GRID_N, GRID_N, GRID_N)):
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons while running."""
+    """Samples nvidia-smi clocks and throttle reasons every 20 ms.  Started
+    before the timed region (nvidia-smi needs a moment to print its first
+    row); summary() keeps the rows that arrived inside [t0, t1]."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -64,21 +66,31 @@ class ClockSampler:
         self.gpu = gpu_index
         self.rows = []
         self.proc = None
+        self.t0, self.t1 = 0.0, float("inf")
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            deadline = time.perf_counter() + 5.0
+            while not self.rows and time.perf_counter() < deadline:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
+            self.rows.append((time.perf_counter(), [x.strip() for x in line.split(",")]))
+
+    def mark_start(self):
+        self.t0 = time.perf_counter()
+
+    def mark_end(self):
+        self.t1 = time.perf_counter() + 0.025  # a row printed at the end arrives a moment later
 
     def __exit__(self, *a):
         if self.proc:
@@ -89,14 +101,15 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        if not self.rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        rows = [r for t, r in self.rows if self.t0 <= t <= self.t1]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+                "reasons": reasons, "samples": len(rows)}
 
 
 def dist_setup():
@@ -291,6 +304,7 @@ def main():
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     barrier(world)
     with ClockSampler(local) as clk:
+        clk.mark_start()
         t_wall = time.perf_counter()
         for i in range(args.steps):
             flush.fill_(i & 0xFF)
@@ -299,6 +313,7 @@ def main():
             ev[i][1].record()
         torch.cuda.synchronize()
         t_wall = time.perf_counter() - t_wall
+        clk.mark_end()
     barrier(world)
     step_ms = [a.elapsed_time(b) for a, b in ev]
     total_ms = max_over_ranks(float(np.sum(step_ms)), world)
