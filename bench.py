@@ -386,23 +386,11 @@ def main():
     if not args.no_points:
         q = torch.from_numpy(synth.mixed_points(v, idx, N_POINTS, seed=SEED)).to(dev)
         qo = torch.empty(N_POINTS, dtype=torch.float32, device=dev)
-        # autotune the single-thread node budget on the Bvh+Raycast batch
-        L = m2s._lib.lib()
+        # the library's query autotuner picks the node budget (one thread per
+        # query, then one warp) on the Bvh+Raycast batch
         acc = m2s.build_sdf_acceleration(v, m2s.Topology.TriangleList(idx), A.bvh(S.Raycast))
-        tune = {}
-        for budget in (0, 256, 512, 768, 1024, 1536, 2048, 4096):
-            L.m2s_set_query_budget(budget)
-            acc.query_device(q, qo, status, stream)
-            torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            acc.query_device(q, qo, status, stream)
-            e1.record()
-            torch.cuda.synchronize()
-            tune[budget] = e0.elapsed_time(e1)
+        best_budget, tune = acc.autotune_queries(q, stream)
         acc.close()
-        best_budget = min(tune, key=tune.get)
-        L.m2s_set_query_budget(best_budget)
         points["budget_sweep_ms"] = {str(k): round(v_, 3) for k, v_ in tune.items()}
         points["node_budget"] = best_budget
         for name, am, n in (("bvh_raycast", A.bvh(S.Raycast), N_POINTS), ("rtree", A.rtree(), N_POINTS),

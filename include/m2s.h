@@ -330,6 +330,17 @@ uint32_t m2s_last_grid_round_log(uint32_t* out, uint32_t capacity);
 void m2s_set_query_budget(uint32_t node_visits);
 uint32_t m2s_query_budget(void);
 
+/* The query autotuner (no counterpart in the reference): times the resident
+ * mesh's LBVH query on the caller's device queries d_q[0..nq) at each node
+ * budget of {0, 256, 512, 768, 1024, 1536, 2048, 4096} (the point where a
+ * query moves from one thread to one warp) and sets the process-wide budget
+ * to the fastest.  Results do not depend on the budget.  out_budget (may be
+ * NULL) receives the choice, out_ms (may be NULL, 8 entries) each
+ * candidate's time.  Synchronous; meshes built with AccelerationMethod::None
+ * have no traversal to tune (M2S_ERR_INVALID_ARGUMENT). */
+int m2s_query_autotune(const m2s_mesh* mesh, const float* d_q, uint64_t nq, void* stream, uint32_t* out_budget,
+                       float out_ms[8]);
+
 const char* m2s_status_string(int status);
 /* Detail of the last failure on the calling thread ("" if none). */
 const char* m2s_last_error(void);

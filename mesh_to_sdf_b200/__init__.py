@@ -365,6 +365,22 @@ class SdfAccelerationMesh:
                                              None if stream is None else ctypes.c_void_p(stream))
         _check(st, "query_sdf_device")
 
+    QUERY_BUDGETS = (0, 256, 512, 768, 1024, 1536, 2048, 4096)
+
+    def autotune_queries(self, q, stream=None):
+        """The query autotuner: times this mesh's query on the device tensor q
+        (n,3) float32 at each node budget of QUERY_BUDGETS (where a query moves
+        from one thread to one warp), sets the process-wide budget to the
+        fastest and returns (budget, {budget: ms}).  Results do not depend on
+        the budget."""
+        b = ctypes.c_uint32(0)
+        ms = np.zeros(len(self.QUERY_BUDGETS), np.float32)
+        st = _lib.lib().m2s_query_autotune(self._h, ctypes.c_void_p(q.data_ptr()), q.shape[0],
+                                           None if stream is None else ctypes.c_void_p(stream), ctypes.byref(b),
+                                           _vp(ms))
+        _check(st, "query_autotune")
+        return int(b.value), {k: float(v) for k, v in zip(self.QUERY_BUDGETS, ms)}
+
     def grid_device(self, grid: Grid, sign_method: SignMethod, out, status=None, stream=None):
         """generate_grid_sdf into a device tensor `out` of grid.get_total_cell_count() float32."""
         first = np.ascontiguousarray(grid.first_cell, F32)

@@ -59,6 +59,7 @@ SIGNATURES = {
     "m2s_generate_sdf_none_noalloc": (I, [P, U64, P, U64, I, I, P, U64, I, P, P]),
     "m2s_last_grid_stats": (I, [P]),
     "m2s_last_query_stats": (I, [P]),
+    "m2s_query_autotune": (I, [P, P, U64, P, P, P]),
     "m2s_test_grid_barrier": (I, [ctypes.c_uint32, ctypes.c_uint32, P]),
     "m2s_set_profiling": (None, [I]),
     "m2s_last_grid_phase_ms": (I, [P]),

@@ -449,6 +449,52 @@ int m2s_query_sdf_device(const m2s_mesh* mesh, const float* d_q, uint64_t nq, fl
   return query_points(mesh->mesh.view(), mesh->accel, mesh->sign, d_q, nq, d_out, nullptr, nullptr, d_status, s);
 }
 
+int m2s_query_autotune(const m2s_mesh* mesh, const float* d_q, uint64_t nq, void* stream, uint32_t* out_budget,
+                       float out_ms[kQueryBudgetCandidates]) {
+  if (!mesh || !d_q || nq == 0) return M2S_ERR_INVALID_ARGUMENT;
+  int st;
+  if ((st = require_device())) return st;
+  if (mesh->mesh.n_tris == 0 || mesh->accel == M2S_ACCEL_NONE) return M2S_ERR_INVALID_ARGUMENT;
+  cudaStream_t s = (cudaStream_t)stream;
+  DevBuf<float> out;
+  DevBuf<uint32_t> status;
+  if ((st = out.alloc(nq, s)) || (st = status.alloc(1, s))) return st;
+  M2S_CUDA(cudaMemsetAsync(status.p, 0, 4, s));
+  cudaEvent_t e0, e1;
+  M2S_CUDA(cudaEventCreate(&e0));
+  M2S_CUDA(cudaEventCreate(&e1));
+  const uint32_t saved = g_query_budget;
+  float best_ms = INFINITY;
+  uint32_t best = saved;
+  for (int c = 0; c < kQueryBudgetCandidates && !st; ++c) {
+    g_query_budget = kQueryBudgets[c];
+    float ms = INFINITY;
+    // one warm-up, then the faster of two timed runs
+    for (int rep = 0; rep < 3 && !st; ++rep) {
+      if (rep && cudaEventRecord(e0, s) != cudaSuccess) st = M2S_ERR_CUDA;
+      if (!st) st = query_points(mesh->mesh.view(), mesh->accel, mesh->sign, d_q, nq, out.p, nullptr, nullptr,
+                                 status.p, s);
+      if (!st && rep) {
+        float t = 0.0f;
+        if (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+            cudaEventElapsedTime(&t, e0, e1) != cudaSuccess)
+          st = M2S_ERR_CUDA;
+        ms = std::min(ms, t);
+      }
+    }
+    if (out_ms) out_ms[c] = ms;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = kQueryBudgets[c];
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  g_query_budget = st ? saved : best;
+  if (out_budget) *out_budget = g_query_budget;
+  return st;
+}
+
 int m2s_grid_sdf_device(const m2s_mesh* mesh, const float first_cell[3], const float cell_size[3],
                         const uint64_t cell_count[3], int sign, float* d_out, uint32_t* d_status, void* stream) {
   if (!mesh || !first_cell || !cell_size || !cell_count || sign < 0 || sign > 1) return M2S_ERR_INVALID_ARGUMENT;

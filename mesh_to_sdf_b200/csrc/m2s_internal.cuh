@@ -125,6 +125,9 @@ int query_points(const MeshView& m, int accel, int sign, const float* d_q, uint6
 // Node visits a query may spend in the one-thread-per-query pass before it is
 // continued one warp per query (0 disables the second pass).
 extern uint32_t g_query_budget;
+// Node budgets the query autotuner tries.
+constexpr int kQueryBudgetCandidates = 8;
+constexpr uint32_t kQueryBudgets[kQueryBudgetCandidates] = {0, 256, 512, 768, 1024, 1536, 2048, 4096};
 
 // Profiling (m2s_set_profiling, per host thread): whether it is on, and the
 // traversal counts of the last point query made with it on:

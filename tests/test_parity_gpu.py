@@ -196,6 +196,28 @@ def test_query_counting_changes_no_result():
             assert st["sign_node_fetches"] >= len(q), (repr(am), st)
 
 
+def test_query_autotune_keeps_results():
+    import torch
+
+    v, idx = synth.star(4, seed=12)
+    q = synth.mixed_points(v, idx, 20000, seed=13)
+    L = m2s._lib.lib()
+    saved = L.m2s_query_budget()
+    try:
+        for am in (A.bvh(S.Raycast), A.rtree(), A.rtree_bvh()):
+            acc = m2s.build_sdf_acceleration(v, T.TriangleList(idx), am)
+            ref = m2s.query_sdf(acc, q)
+            budget, ms = acc.autotune_queries(torch.from_numpy(q).cuda())
+            assert budget in acc.QUERY_BUDGETS and L.m2s_query_budget() == budget
+            assert all(t > 0 for t in ms.values()), ms
+            assert min(ms, key=ms.get) == budget
+            for b in (0, 256, 4096):  # the budget moves work between passes, never results
+                L.m2s_set_query_budget(b)
+                assert_bit_equal(m2s.query_sdf(acc, q), ref, f"{am!r} budget {b}")
+    finally:
+        L.m2s_set_query_budget(saved)
+
+
 def test_fp64_error_report(orc):
     # north_star error report: distance error against an FP64 brute force
     v, idx = synth.star(4, seed=9)
