@@ -323,18 +323,21 @@ int m2s_last_grid_phase_ms(float out[4]);
  * copying up to `capacity` steps (2 * capacity words) to `out` (may be NULL). */
 uint32_t m2s_last_grid_round_log(uint32_t* out, uint32_t capacity);
 
-/* Point queries run one thread per query; a query that visits more than
- * `node_visits` LBVH nodes is continued by a whole warp (points deep inside a
- * closed mesh see most triangles at nearly the same distance).  0 keeps every
- * query on one thread.  Process-wide tuning knob; the autotuner sets it. */
+/* Point queries run one thread per query; a query that visits more than its
+ * node budget is continued by a whole warp (points deep inside a closed mesh
+ * see most triangles at nearly the same distance).  `node_visits` is the
+ * budget of batches of 2^20 queries and more; a smaller batch of nq queries
+ * uses node_visits * sqrt(nq / 2^20), at least 64, since its time is its
+ * longest single-thread search.  0 keeps every query on one thread.
+ * Process-wide tuning knob; the autotuner sets it. */
 void m2s_set_query_budget(uint32_t node_visits);
 uint32_t m2s_query_budget(void);
 
 /* The query autotuner (no counterpart in the reference): times the resident
- * mesh's LBVH query on the caller's device queries d_q[0..nq) at each node
- * budget of {0, 256, 512, 768, 1024, 1536, 2048, 4096} (the point where a
- * query moves from one thread to one warp) and sets the process-wide budget
- * to the fastest.  Results do not depend on the budget.  out_budget (may be
+ * mesh's LBVH query on the caller's device queries d_q[0..nq) with each
+ * base budget of {0, 256, 512, 768, 1024, 1536, 2048, 4096} (see
+ * m2s_set_query_budget: where a query moves from one thread to one warp,
+ * scaled down for batches under 2^20 queries) and sets the fastest.  Results do not depend on the budget.  out_budget (may be
  * NULL) receives the choice, out_ms (may be NULL, 8 entries) each
  * candidate's time.  Synchronous; meshes built with AccelerationMethod::None
  * have no traversal to tune (M2S_ERR_INVALID_ARGUMENT). */

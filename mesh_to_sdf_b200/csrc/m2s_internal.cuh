@@ -3,7 +3,9 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
+#include <cmath>
 #include <memory>
 #include <string>
 #include <vector>
@@ -125,6 +127,14 @@ int query_points(const MeshView& m, int accel, int sign, const float* d_q, uint6
 // Node visits a query may spend in the one-thread-per-query pass before it is
 // continued one warp per query (0 disables the second pass).
 extern uint32_t g_query_budget;
+// The budget a batch of nq queries uses: `base` from 2^20 queries up, and
+// base * sqrt(nq / 2^20), at least 64, below (0 stays 0: no warp pass).
+inline uint32_t effective_query_budget(uint32_t base, uint64_t nq) {
+  if (base == 0) return 0;
+  const double f = nq >= (1ull << 20) ? 1.0 : std::sqrt((double)nq / (double)(1ull << 20));
+  const uint32_t b = (uint32_t)(base * f + 0.5);
+  return b < 64 ? std::min<uint32_t>(64, base) : b;
+}
 // Node budgets the query autotuner tries.
 constexpr int kQueryBudgetCandidates = 8;
 constexpr uint32_t kQueryBudgets[kQueryBudgetCandidates] = {0, 256, 512, 768, 1024, 1536, 2048, 4096};

@@ -759,7 +759,9 @@ int query_points(const MeshView& m, int accel, int sign, const float* d_q, uint6
     if ((st = hard.alloc(nq, s)) || (st = hard_count.alloc(1, s))) return st;
     M2S_CUDA(cudaMemsetAsync(hard_count.p, 0, 4, s));
   }
-  const uint32_t budget = g_query_budget;
+  // Smaller batches hand long searches to the warp pass sooner: their time is
+  // the longest single-thread search, not the throughput of many.
+  const uint32_t budget = effective_query_budget(g_query_budget, nq);
   HardQuery* hp = two_pass ? hard.p : nullptr;
   uint32_t* hc = two_pass ? hard_count.p : nullptr;
   // With profiling on, the counting instantiations run and their totals are
