@@ -525,10 +525,41 @@ def other_workload(args):
     torch.cuda.synchronize()
     qms = e0.elapsed_time(e1)
     assert int(status.item()) == 0, int(status.item())
+    accuracy = None
+    if not args.no_cpu_baseline:
+        accuracy = workload_accuracy(v, idx, args.workload == "c3", grid, sign, out.cpu().numpy(), q,
+                                     qo.cpu().numpy(), am)
     print(json.dumps({"workload": args.workload, "triangles": mesh.triangle_count, "grid": list(grid.cell_count),
                       "sign": sign.name, "grid_ms": gms, "cells_per_s": N / (gms / 1e3), "grid_stats": stats,
-                      "points": npts, "method": repr(am), "points_ms": qms, "pts_per_s": npts / (qms / 1e3)}),
+                      "points": npts, "method": repr(am), "points_ms": qms, "pts_per_s": npts / (qms / 1e3),
+                      "accuracy": accuracy}),
           flush=True)
+
+
+def workload_accuracy(v, idx, strip, grid, sign, gpu_grid, q, gpu_pts, am, n_sample=50_000):
+    """The c1 / c3 lines' accuracy (reported, not timed).  Grid: the
+    restatement on all host threads; cells whose sign differs are split into
+    tie-ambiguous ones (the same distance bits from a differently oriented
+    triangle, so the sign follows the tie order) and the rest.  Points: the
+    oracle on a seeded sample (the same lowest-index tie rule, so bit-exact)."""
+    import oracle
+
+    threads = os.cpu_count() or 1
+    ref = oracle.generate_grid_sdf(v, idx, grid.first_cell, grid.cell_size, grid.cell_count,
+                                   "raycast" if int(sign) == 0 else "normal", strip=strip, n_threads=threads)
+    ga, ra = np.abs(gpu_grid), np.abs(ref)
+    flip = np.signbit(gpu_grid) != np.signbit(ref)
+    tie = flip & (ga.view(np.uint32) == ra.view(np.uint32))
+    rng = np.random.default_rng(SEED + 11)
+    pick = rng.choice(len(q), min(n_sample, len(q)), replace=False)
+    codes = {0: "none", 1: "bvh", 2: "rtree", 3: "rtree_bvh"}
+    opts = oracle.generate_sdf(v, idx, q[pick], codes[am.kind], int(am.sign), strip=strip, n_threads=threads)
+    return {"grid_vs_restatement": {"cells": int(len(gpu_grid)),
+                                    "value_differs_frac": float(np.mean(ga.view(np.uint32) != ra.view(np.uint32))),
+                                    "sign_differs": int(flip.sum()), "sign_differs_tie_ambiguous": int(tie.sum()),
+                                    "threads": threads},
+            "points_vs_oracle": {"sample": int(len(pick)),
+                                 "bits_differ": int(np.sum(gpu_pts[pick].view(np.uint32) != opts.view(np.uint32)))}}
 
 
 def batch_workload(args):
