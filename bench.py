@@ -256,6 +256,7 @@ def main():
     ap.add_argument("--requests", type=int, default=200, help="c5 requests per rate")
     ap.add_argument("--batch", type=int, default=256, help="meshes of the c4 batch")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--wave-cells", type=int, default=0, help="c4: cells per batched job (0 = the library default)")
     args = ap.parse_args()
     if args.small:
         return small_case(args.grid)
@@ -618,6 +619,8 @@ def batch_workload(args):
     plain_ms = timed(plain_pass, max(1, min(args.steps, 3)))
     per_edge = plain_by_edge()
     batched = torch.empty(N, dtype=torch.float32, device="cuda")
+    if args.wave_cells:
+        m2s.set_grid_tuning(wave_cells=args.wave_cells)
     plan = m2s.GridPlan(meshes, grids, S.Raycast, batched, status)
     blocks0 = plan.blocks
     plan.run()

@@ -93,8 +93,9 @@ uint64_t upload_bytes(uint64_t tris, uint64_t nv, uint64_t ni, int bits, int acc
 // with their sort buffers, and the continuation list of the two-pass query.
 uint64_t point_bytes(uint64_t nq) { return 64 * nq + (1u << 20); }
 
-// Largest grid batch, in waves of the batched job.
+// Largest grid batch, in waves of the batched job, and the serving wave size.
 constexpr uint64_t kBatchWaves = 4;
+constexpr uint64_t kServeWaveCells = 4ull << 20;
 
 }  // namespace
 
@@ -334,8 +335,10 @@ void m2s_server::grid_loop() {
   for (;;) {
     std::vector<RequestP> batch;
     std::vector<MeshView> views;
-    const GridTuning tune = g_grid_tuning;
-    const uint64_t wave_cells = tune.wave_cells ? tune.wave_cells : (4ull << 20);
+    // Serving keeps waves small: a wave's requests complete together.
+    GridTuning tune = g_grid_tuning;
+    tune.wave_cells = std::min<uint64_t>(tune.wave_cells ? tune.wave_cells : kServeWaveCells, kServeWaveCells);
+    const uint64_t wave_cells = tune.wave_cells;
     {
       std::unique_lock<std::mutex> lk(mu);
       cv_work.wait(lk, [&] { return stop || head_ready(kGrid); });
