@@ -212,6 +212,73 @@ def synth_bbox(v):
     return v.min(axis=0), v.max(axis=0)
 
 
+def reference_workloads(args):
+    """The CPU baseline of the other configurations: the oracle port (the
+    reference's decomposition: parallel seeding, per-thread heaps and rays for
+    grids; queries in parallel, RtreeBvh serially as the reference does) on the
+    host cores, on bounded samples of each configuration.  One JSON line."""
+    import oracle
+
+    import mesh_to_sdf_b200 as m2s
+    from mesh_to_sdf_b200 import synth
+
+    cores = os.cpu_count() or 1
+
+    def grid_rate(v, idx, g, sign, strip=False):
+        t = time.perf_counter()
+        oracle.generate_grid_sdf(v, idx, g.first_cell, g.cell_size, g.cell_count, sign, strip=strip, n_threads=cores)
+        return g.get_total_cell_count() / (time.perf_counter() - t)
+
+    def point_rate(v, idx, q, accel, sign="raycast", strip=False, threads=cores):
+        t = time.perf_counter()
+        oracle.generate_sdf(v, idx, q, accel, sign, strip=strip, n_threads=threads)
+        return len(q) / (time.perf_counter() - t)
+
+    out = {"impl": "reference", "workload": args.workload, "cores": cores, "kind": "port"}
+    if args.workload == "c1":
+        v, idx = synth.icosphere(3)
+        g = m2s.Grid.from_bounding_box([-1.2] * 3, [1.2] * 3, [32, 32, 32])
+        q = synth.uniform_points(10_000, [-1.2] * 3, [1.2] * 3, seed=SEED)
+        out["grid_cells_per_s"] = grid_rate(v, idx, g, "raycast")
+        out["rtree_bvh_points_per_s"] = point_rate(v, idx, q, "rtree_bvh", threads=1)  # serial in the reference
+        out["sample"] = "the whole configuration"
+    elif args.workload == "c3":
+        v, idx = synth.terrain(512, seed=SEED)
+        lo, hi = synth.padded_bbox(v, 0.1)
+        g = m2s.Grid.from_bounding_box(lo, hi, [384, 384, 128])
+        q = synth.uniform_points(200_000, lo, hi, seed=SEED)
+        out["grid_cells_per_s"] = grid_rate(v, idx, g, "normal", strip=True)
+        out["rtree_points_per_s"] = point_rate(v, idx, q, "rtree", "normal", strip=True)
+        out["sample"] = "the whole grid; 200,000 of the 4M points"
+    else:
+        items = synth.batch_meshes(args.batch, seed=SEED)[::16]
+        cells, t = 0, time.perf_counter()
+        for v, i, lo, hi, e in items:
+            g = m2s.Grid.from_bounding_box(lo, hi, [e, e, e])
+            oracle.generate_grid_sdf(v, i, g.first_cell, g.cell_size, g.cell_count, "raycast", n_threads=cores)
+            cells += g.get_total_cell_count()
+        out["grid_cells_per_s"] = cells / (time.perf_counter() - t)
+        out["sample"] = f"every 16th of the {args.batch} meshes ({len(items)} grids, {cells} cells), one call each"
+    print(json.dumps(out), flush=True)
+
+
+def c2_point_baseline(cores):
+    """The C2 point methods on the host cores (oracle port; samples)."""
+    import oracle
+
+    from mesh_to_sdf_b200 import synth
+
+    v, idx, lo, hi = workload()
+    q = synth.mixed_points(v, idx, 100_000, seed=SEED)
+    res = {}
+    for name, accel, sign, n in (("bvh_raycast", "bvh", "raycast", 100_000), ("rtree", "rtree", "normal", 100_000),
+                                 ("none_raycast", "none", "raycast", 1_000), ("none_normal", "none", "normal", 1_000)):
+        t = time.perf_counter()
+        oracle.generate_sdf(v, idx, q[:n], accel, sign, n_threads=cores)
+        res[name] = {"points": n, "points_per_s": n / (time.perf_counter() - t)}
+    return res
+
+
 def reference_arm(args, world, rank):
     """The reference's CPU path (its C++ restatement; cargo is not on this image), all host cores."""
     if rank != 0:
@@ -220,6 +287,7 @@ def reference_arm(args, world, rank):
     grid = grid_for(lo, hi)
     slab = cpu_slab(grid)
     cores = os.cpu_count() or 1
+    points = c2_point_baseline(cores)
     for _ in range(args.warmup):
         run_cpu_grid(v, idx, slab, cores)
     ts = [run_cpu_grid(v, idx, slab, cores) for _ in range(args.steps)]
@@ -232,7 +300,8 @@ def reference_arm(args, world, rank):
             "config": {"workload": "star_s6_grid256_raycast", "sample": "256x256x32 middle slab of the 256^3 grid"},
             "cpu_baseline": {"value": value, "unit": "cells/s", "cores": cores, "kind": "port",
                              "sample": "256x256x32 middle z-slab (2.1M cells) of the 256^3 grid, per step"},
-            "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "points": points}
     print(json.dumps(line), flush=True)
 
 
@@ -260,6 +329,8 @@ def main():
     args = ap.parse_args()
     if args.small:
         return small_case(args.grid)
+    if args.impl == "reference" and args.workload in ("c1", "c3", "c4"):
+        return reference_workloads(args)
     if args.workload == "c4":
         return batch_workload(args)
     if args.workload == "c5":
