@@ -480,6 +480,18 @@ int m2s_server_create(uint64_t hbm_budget_bytes, uint32_t point_streams, m2s_ser
     delete S;
     return st;
   }
+  {
+    // Grow the device memory pool once, up front: growing it while requests
+    // run (new physical memory for a larger working set) stalled every worker
+    // for tens to hundreds of milliseconds now and then.  The pool keeps what
+    // it reserved, so later allocations are carved from this.
+    const uint64_t reserve = std::min<uint64_t>(hbm_budget_bytes / 2, 16ull << 30);
+    void* p = nullptr;
+    if (reserve && dev_alloc(&p, reserve, S->s_upload) == M2S_OK) {
+      dev_free(p, S->s_upload);
+      cudaStreamSynchronize(S->s_upload);
+    }
+  }
   S->th[kUpload] = std::thread([S] { S->upload_loop(); });
   S->th[kPoints] = std::thread([S] { S->points_loop(); });
   S->th[kGrid] = std::thread([S] { S->grid_loop(); });
