@@ -394,7 +394,7 @@ def main():
     value = world * N * args.steps / (total_ms / 1e3)
     assert int(status.item()) == 0
 
-    # ---- roofline of the dominant phase: propagation (k_relax rounds), profiled on the same stream
+    # ---- roofline of the dominant phase: propagation (k_propagate), profiled on the same stream
     m2s.set_profiling(True)
     flush.fill_(1)
     step()
@@ -418,7 +418,7 @@ def main():
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                 "frac": achieved / hbm_peak, "traffic": PROPAGATE_DRAM_BYTES,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one 256^3 launch",
-                "kernel": "k_relax (propagation rounds)", "peak_source": "measured" if peaks else "fallback",
+                "kernel": "k_propagate (propagation rounds)", "peak_source": "measured" if peaks else "fallback",
                 "phase_ms": phases, "stats": stats}
 
     # ---- e2e: the host-pointer C ABI with pinned buffers, H2D + D2H inside the timed region
