@@ -219,7 +219,7 @@ def test_query_autotune_keeps_results():
 
 
 def test_fp64_error_report(orc):
-    # north_star error report: distance error against an FP64 brute force
+    # error report: distance error against an FP64 brute force
     v, idx = synth.star(4, seed=9)
     q = synth.mixed_points(v, idx, 4000, seed=10)
     gpu = m2s.generate_sdf(v, T.TriangleList(idx), q, A.rtree_bvh())
