@@ -516,49 +516,51 @@ constexpr int kUnroll = 2;  // proposals per thread in flight
 
 enum { kRelax = 0, kRedistribute = 1, kDone = 2, kLimit = 3 };
 
-// Next step of the schedule, computed by thread 0 of every block from the
+// Next step of the schedule, computed by warp 0 of every block from the
 // global list counts (final at this point: the last grid barrier ordered every
-// push before it).  All counts it may need are loaded together, one round trip.
-// Block 0 also empties the list relaxed last round, which no block reads here
-// and which receives pushes only after the next barrier.
-__device__ __forceinline__ int next_step(Sched& sh, const Counters& ct, uint32_t spill_overflow, PropState* st,
-                                         bool leader) {
+// push before it): lane k reads the count of the list of bucket b + k, all in
+// one round trip, and the lanes rotate the ring by shuffles.  Block 0 also
+// empties the list relaxed last round, which no block reads here and which
+// receives pushes only after the next barrier.  Every lane returns the action.
+__device__ __forceinline__ int next_step(Sched& sh, const Counters& ct, uint32_t spill_overflow, bool leader) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t my_slot = lane < kRing ? sh.slot[lane] : 0u;
+  const uint32_t c = lane < kRing ? *(volatile uint32_t*)&ct.count[my_slot] : 0u;
   // Bit k: the list of bucket b + k holds states (bits past the window's end cleared).
-  uint32_t nonempty = 0;
-#pragma unroll
-  for (int k = 0; k < kRing; ++k) nonempty |= (*(volatile uint32_t*)&ct.count[sh.slot[k]] != 0u ? 1u : 0u) << k;
-  const uint32_t left = sh.B + kRing - sh.b;  // buckets b .. B + kRing - 1 lie in the window
+  uint32_t nonempty = __ballot_sync(0xFFFFFFFFu, lane < kRing && c != 0u);
+  const uint32_t b = sh.b, B = sh.B, fp = sh.fp, cur = sh.cur;
+  const uint32_t left = B + kRing - b;  // buckets b .. B + kRing - 1 lie in the window
   if (left < kRing) nonempty &= (1u << left) - 1u;
   // Only values no block can change before every block has passed this step:
   // list counts (pushes come after the next barrier), the push overflow flag
   // and the spill overflow flag of the round just finished (the next propose
   // phase writes the other parity).
   const uint32_t overflow = *(volatile uint32_t*)ct.overflow | spill_overflow;
-  const uint32_t far_n = *(volatile uint32_t*)&ct.count[kFar0 + sh.fp];
-  const uint32_t far_b = *(volatile uint32_t*)&ct.far_min[sh.fp];
+  const uint32_t far_n = *(volatile uint32_t*)&ct.count[kFar0 + fp];
+  const uint32_t far_b = *(volatile uint32_t*)&ct.far_min[fp];
+  __syncwarp();  // every lane has read the schedule before it changes
   if (overflow) return kDone;
-  // slot[q] holds bucket b + q; the window ends at bucket B + kRing - 1.
   if (nonempty) {
+    // slot[k] holds bucket b + k; advance b to the first non-empty bucket q.
     const int q = __ffs(nonempty) - 1;
-    const uint32_t nq = *(volatile uint32_t*)&ct.count[sh.slot[q]];
-    uint32_t rot[kRing];
-#pragma unroll
-    for (int k = 0; k < kRing; ++k) rot[k] = sh.slot[(k + q) % kRing];  // advance b by q
-    const uint32_t consumed = sh.cur;
-    sh.cur = rot[0];
-    rot[0] = consumed;  // becomes the list of states re-queued at bucket b
-#pragma unroll
-    for (int k = 0; k < kRing; ++k) sh.slot[k] = rot[k];
-    sh.b += q;
-    sh.n = nq;
-    sh.round += 1;
-    if (leader) ct.count[consumed] = 0;
+    const uint32_t nq = __shfl_sync(0xFFFFFFFFu, c, q);
+    const uint32_t moved = __shfl_sync(0xFFFFFFFFu, my_slot, (lane + q) & (kRing - 1));
+    if (lane < kRing) sh.slot[lane] = lane == 0 ? cur : moved;  // slot 0: the consumed list, re-queued at b
+    if (lane == 0) {
+      sh.cur = moved;
+      sh.b = b + q;
+      sh.n = nq;
+      sh.round += 1;
+      if (leader) ct.count[cur] = 0;
+    }
+    __syncwarp();
     return kRelax;
   }
   // Every window list is empty.  Far states all lie at or beyond B + kRing, so
   // the new window starts at the lowest of them.
   if (far_n == 0) return kDone;
-  sh.B = sh.b = far_b;
+  if (lane == 0) sh.B = sh.b = far_b;
+  __syncwarp();
   return kRedistribute;
 }
 
@@ -901,13 +903,19 @@ __global__ void __launch_bounds__(256, 4) k_propagate(const __grid_constant__ Gr
   uint32_t far_phases = 0, logged = 0, max_list = 0, solo_rounds = 0;
   const uint64_t t_start = (lead_block && threadIdx.x == 0 && round_log) ? global_ns() : 0;
   bool aborted = false;
-  // Thread 0: the next step (unless a solo run already chose it), logged by
+  // Warp 0: the next step (unless a solo run already chose it), logged by
   // block 0 when profiling: the relaxed list's size, or (top bit) the far list's.
   auto step = [&]() {
-    s_ntouch = 0;  // every thread read it in the last commit, before the last barrier
     const bool in_run = lead_block && s_solo_run;
     const uint32_t spill_ov = in_run ? 0u : *(volatile uint32_t*)&st->overflow2[sh.round & 1u];
-    sh.action = sh.steps >= max_steps ? kLimit : next_step(sh, counters(in_run), spill_ov, st, lead_block);
+    const bool limit = sh.steps >= max_steps;
+    const int action = limit ? kLimit : next_step(sh, counters(in_run), spill_ov, lead_block);
+    if (threadIdx.x != 0) {
+      __syncwarp();
+      return;
+    }
+    s_ntouch = 0;  // every thread read it in the last commit, before the last barrier
+    sh.action = action;
     ++sh.steps;
     if (sh.action == kRelax) max_list = max(max_list, sh.n);
     // Profiling: block 0 records each step — the relaxed list's size (bit 30:
@@ -921,13 +929,16 @@ __global__ void __launch_bounds__(256, 4) k_propagate(const __grid_constant__ Gr
       round_log[2 * logged + 1] = (uint32_t)(global_ns() - t_start);
       ++logged;
     }
+    __syncwarp();
   };
   bool chosen = false;  // a solo round's tail chose this step already (block-uniform)
   for (;;) {
     if (!chosen) {
-      if (threadIdx.x == 0) {
-        if (s_pending) s_pending = 0;
-        else step();
+      if (threadIdx.x < 32) {
+        const bool pending = s_pending;
+        __syncwarp();
+        if (!pending) step();
+        else if (threadIdx.x == 0) s_pending = 0;
       }
       __syncthreads();
     }
@@ -1062,8 +1073,8 @@ __global__ void __launch_bounds__(256, 4) k_propagate(const __grid_constant__ Gr
     // rounds stay small, else hands the schedule (next action included) to the
     // other blocks at the barrier they wait at.
     __syncthreads();
+    if (threadIdx.x < 32) step();
     if (threadIdx.x == 0) {
-      step();
       ++s_runs;
       ++solo_rounds;
       s_more = sh.action == kRelax && sh.n <= solo_max && s_runs < kSoloRounds;
