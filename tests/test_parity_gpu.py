@@ -382,6 +382,22 @@ def test_grid_negative_and_anisotropic_sizes(orc):
     assert np.all(np.abs(gpu) >= nn)
 
 
+def test_grid_tiny_and_flat_shapes(orc):
+    # one cell, lines and planes of cells, a grid with a zero extent
+    v, idx = synth.icosphere(2)
+    for count in ([1, 1, 1], [1, 1, 40], [40, 1, 1], [1, 37, 1], [2, 2, 2], [33, 29, 1]):
+        grid = m2s.Grid.from_bounding_box([-1.3] * 3, [1.3] * 3, count)
+        for sign in (S.Raycast, S.Normal):
+            gpu, ref1, ref8, nn = grid_report(orc, v, idx, grid, sign)
+            label = f"{count} {sign!r}"
+            check_grid(gpu, ref1, ref8, nn, float(np.linalg.norm(grid.cell_size)), sign, label)
+    # a zero cell count with triangles: the crate's seeding clamp (`clamp(0, n - 1)`,
+    # generate/grid.rs:400-426) panics; the ABI refuses the grid instead
+    empty = m2s.Grid.new([-1.3] * 3, [0.1] * 3, [0, 8, 8])
+    with pytest.raises(m2s.M2SError):
+        m2s.generate_grid_sdf(v, T.TriangleList(idx), empty, S.Raycast)
+
+
 def test_grid_coarse_mesh_far_states(orc):
     # a coarse sphere in a fine grid: seeds lie many buckets from the surface and
     # wait in the far list; the result keeps the same envelope as the others
