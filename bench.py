@@ -587,6 +587,7 @@ def other_workload(args):
     stats = m2s.last_grid_stats()
     qd = torch.from_numpy(q).cuda()
     qo = torch.empty(npts, dtype=torch.float32, device="cuda")
+    budget, _ = mesh.autotune_queries(qd)  # the library's query autotuner, on these points
     for _ in range(2):
         mesh.query_device(qd, qo, status)
     torch.cuda.synchronize()
@@ -604,7 +605,7 @@ def other_workload(args):
     print(json.dumps({"workload": args.workload, "triangles": mesh.triangle_count, "grid": list(grid.cell_count),
                       "sign": sign.name, "grid_ms": gms, "cells_per_s": N / (gms / 1e3), "grid_stats": stats,
                       "points": npts, "method": repr(am), "points_ms": qms, "pts_per_s": npts / (qms / 1e3),
-                      "accuracy": accuracy}),
+                      "node_budget": budget, "accuracy": accuracy}),
           flush=True)
 
 
