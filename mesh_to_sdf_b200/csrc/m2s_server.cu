@@ -230,6 +230,8 @@ void m2s_server::points_loop() {
   uint32_t* d_status = nullptr;
   if (cudaHostAlloc((void**)&h_status, kSlots * 4, cudaHostAllocPortable) != cudaSuccess ||
       cudaMalloc((void**)&d_status, kSlots * 4) != cudaSuccess) {
+    cudaGetLastError();
+    if (h_status) cudaFreeHost(h_status);
     std::lock_guard<std::mutex> lk(mu);
     stop = true;
     cv_work.notify_all();
