@@ -110,3 +110,40 @@ def test_acceleration_method_list():
     assert names == ["AccelerationMethod.None(Raycast)", "AccelerationMethod.None(Normal)",
                      "AccelerationMethod.Bvh(Raycast)", "AccelerationMethod.Bvh(Normal)", "AccelerationMethod.Rtree",
                      "AccelerationMethod.RtreeBvh"]
+
+
+def test_header_compiles_and_links_from_cpp(tmp_path):
+    # a C++ caller of include/m2s.h, linked against the library: the boundary
+    # as a non-Python host sees it (no device work: status strings, argument
+    # checks and, without a GPU, the no-device status)
+    import shutil
+    import subprocess
+
+    gxx = shutil.which("g++")
+    if not gxx:
+        pytest.skip("no g++")
+    lib_path = _lib.lib()._name
+    src = tmp_path / "caller.cpp"
+    src.write_text(r'''
+#include <cstdio>
+#include <cstring>
+#include "m2s.h"
+int main() {
+  if (std::strcmp(m2s_status_string(M2S_OK), "ok") != 0) return 1;
+  const float v[12] = {0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0, -1};
+  const uint32_t idx[4] = {0, 1, 2, 0};  // not a multiple of 3: the crate panics (lib.rs:203)
+  const float q[3] = {0.2f, 0.2f, 0.05f};
+  float out[1];
+  uint64_t n = 0;
+  int st = m2s_generate_sdf(v, 4, idx, 4, M2S_INDEX_U32, M2S_TOPOLOGY_TRIANGLE_LIST, q, 1, M2S_ACCEL_BVH,
+                            M2S_SIGN_RAYCAST, out, &n, nullptr);
+  std::printf("%d %s\n", st, m2s_status_string(st));
+  return st == M2S_ERR_INDEX_COUNT ? 0 : 2;
+}
+''')
+    exe = tmp_path / "caller"
+    r = subprocess.run([gxx, "-std=c++17", "-I", os.path.join(ROOT, "include"), str(src), lib_path, "-o", str(exe),
+                        f"-Wl,-rpath,{os.path.dirname(lib_path)}"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, (r.stdout, r.stderr)
