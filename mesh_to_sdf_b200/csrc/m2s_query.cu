@@ -4,7 +4,8 @@
 //    every triangle.  Triangle tiles are staged in shared memory by the bulk
 //    copy engine (cp.async.bulk + mbarrier, double-buffered); each thread owns
 //    one query and folds the tile in triangle order, exactly the reference's
-//    fold order.
+//    fold order.  Normal batches of fewer than 2^17 queries take
+//    k_brute_normal_warp: a warp per query, the same fold in the same order.
 //  * Bvh(Raycast) / RtreeBvh (bvh.rs:256-332, rtree_bvh.rs:143-201): exact
 //    nearest triangle on the LBVH, then the 3-axis ray vote.
 //  * Rtree (rtree.rs:306-326): the nearest triangle's signed distance.
@@ -134,6 +135,79 @@ __global__ void k_brute_finish(const uint2* __restrict__ part, uint64_t nq, floa
     const float d = fminf(F32_MAX, fsqrt(__uint_as_float(pp.x)));
     out[i] = pp.y ? -d : d;
   }
+}
+
+// Normal sign, one warp per query: lane k evaluates triangle t0 + k of each
+// group of 32, then the warp folds the group's distances into `best` in
+// triangle order — the first lane whose distance compare_distances puts
+// before `best` replaces it, and only the lanes after it are tested again,
+// against the new value, until none is before it.  That is the reference's
+// sequential fold (default.rs:63-70) step for step, with 32 triangles
+// evaluated at a time, so a batch of few queries still fills the GPU.
+constexpr int kBwThreads = 256;                 // 8 queries per block
+constexpr uint64_t kBruteWarpMaxQueries = 1u << 17;  // below: one warp per query
+__global__ void __launch_bounds__(kBwThreads) k_brute_normal_warp(const TriRec* __restrict__ tris, uint32_t T,
+                                                                  const float* __restrict__ q, uint64_t nq,
+                                                                  float* __restrict__ out, uint32_t* status) {
+  __shared__ __align__(128) TriRec tile[2][kBfTile];
+  __shared__ __align__(8) uint64_t bar[2];
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t qi = (uint64_t)blockIdx.x * (kBwThreads / 32) + (threadIdx.x >> 5);
+  const bool valid = qi < nq;  // warp-uniform
+  const P3 p = valid ? load_query(q, qi) : P3{0.0f, 0.0f, 0.0f};
+  const uint32_t ntile = (T + kBfTile - 1) / kBfTile;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  auto issue = [&](uint32_t i) {
+    uint32_t cnt = min((uint32_t)kBfTile, T - i * kBfTile);
+    uint32_t bytes = cnt * (uint32_t)sizeof(TriRec);
+    mbar_arrive_expect_tx(&bar[i & 1], bytes);
+    bulk_g2s(&tile[i & 1][0], tris + (uint64_t)i * kBfTile, bytes, &bar[i & 1]);
+  };
+  if (threadIdx.x == 0) {
+    if (ntile > 0) issue(0);
+    if (ntile > 1) issue(1);
+  }
+  float best = F32_MAX;
+  bool nan = false, lost = false;
+  for (uint32_t i = 0; i < ntile; ++i) {
+    const int buf = i & 1;
+    if (!mbar_wait_bounded(&bar[buf], (i >> 1) & 1)) lost = true;
+    const uint32_t cnt = min((uint32_t)kBfTile, T - i * kBfTile);
+    const TriRec* tl = tile[buf];
+    if (valid && !__any_sync(0xFFFFFFFFu, lost)) {
+      for (uint32_t j0 = 0; j0 < cnt; j0 += 32u) {
+        const uint32_t j = j0 + lane;
+        const bool have = j < cnt;
+        float d = 0.0f;
+        if (have) {
+          const float4 ra = tl[j].a, rb = tl[j].b, rc = tl[j].c;
+          d = point_triangle_signed_distance(p, p3(ra), p3(rb), p3(rc), __float_as_int(ra.w));
+        }
+        uint32_t todo = __ballot_sync(0xFFFFFFFFu, have);  // lanes not folded yet
+        while (todo) {
+          const bool before = ((todo >> lane) & 1u) && compare_distances(d, best, &nan) == -1;
+          const uint32_t m = __ballot_sync(0xFFFFFFFFu, before);
+          if (!m) break;
+          const int w = __ffs(m) - 1;
+          best = __shfl_sync(0xFFFFFFFFu, d, w);
+          todo &= ~((2u << w) - 1u);  // lanes up to w are folded (w = 31 clears all)
+        }
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && i + 2 < ntile) {
+      fence_proxy_async_smem();
+      issue(i + 2);
+    }
+  }
+  if (lost) atomicOr(status, bit(M2S_ERR_LIMIT));
+  if (nan) atomicOr(status, bit(M2S_ERR_NAN_DISTANCE));
+  if (valid && lane == 0) out[qi] = best;
 }
 
 // ---------------------------------------------------------------------------
@@ -688,6 +762,13 @@ int brute_force_sdf(const MeshView& m, int sign, const float* d_q, uint64_t nq, 
       k_brute<0><<<dim3(blocks, chunks), kBfThreads, 0, s>>>(m.tris, m.n_tris, d_q, nq, d_out, d_status, part.p);
       k_brute_finish<<<(unsigned)std::min<uint64_t>((nq + 255) / 256, 148u * 16u), 256, 0, s>>>(part.p, nq, d_out);
     }
+  } else if (nq < kBruteWarpMaxQueries) {
+    // Too few queries for one thread each to fill the GPU (the thread kernel
+    // needs about 150k): a warp per query (8,192 queries x 81,920 triangles:
+    // 26.7 -> 4.4 ms; 65,536: 37.6 -> 31.0 ms; at 262,144 the thread kernel
+    // is ahead, 109 against 122 ms).
+    const unsigned wblocks = (unsigned)((nq + kBwThreads / 32 - 1) / (kBwThreads / 32));
+    k_brute_normal_warp<<<wblocks, kBwThreads, 0, s>>>(m.tris, m.n_tris, d_q, nq, d_out, d_status);
   } else {
     k_brute<1><<<blocks, kBfThreads, 0, s>>>(m.tris, m.n_tris, d_q, nq, d_out, d_status, nullptr);
   }

@@ -127,6 +127,43 @@ def test_every_method_bit_exact(orc, mesh):
         assert_bit_equal(gpu, orc_sdf(orc, v, idx, q, am, strip=strip), f"{mesh} {am!r}")
 
 
+def _tie_fan(n_rim, seed):
+    # A fan around the origin whose triangles all share vertex 0, half of them
+    # wound the other way, plus exact duplicates with the opposite winding:
+    # a point above the hub is equally far (the shared vertex) from many
+    # triangles of both signs, and nearly so from its jittered neighbours, so
+    # compare_distances' ties and sign rule decide the fold at every step.
+    rng = np.random.default_rng(seed)
+    ang = np.sort(rng.uniform(0, 2 * np.pi, n_rim))
+    rim = np.stack([np.cos(ang), np.sin(ang), rng.normal(0, 1e-3, n_rim)], 1) * rng.uniform(0.9, 1.1, (n_rim, 1))
+    v = np.vstack([[[0, 0, 0]], rim]).astype(np.float32)
+    tris = []
+    for k in range(n_rim):
+        t = [0, 1 + k, 1 + (k + 1) % n_rim]
+        tris.append(t if rng.random() < 0.5 else t[::-1])
+        if rng.random() < 0.3:
+            tris.append(tris[-1][::-1])
+    idx = np.array(tris, np.uint32).reshape(-1)
+    hub = np.concatenate([rng.normal(0, 1e-6, (600, 2)), rng.choice([-1, 1], (600, 1)) *
+                          rng.uniform(1e-5, 0.3, (600, 1))], 1)
+    q = np.vstack([hub, rng.uniform(-1.2, 1.2, (400, 3))]).astype(np.float32)
+    return v, idx, q
+
+
+@pytest.mark.parametrize("n_rim", [70, 333])
+def test_none_normal_fold_ties(orc, n_rim):
+    # default.rs:63-70: the compare_distances fold in triangle order, on both
+    # brute-force kernels (a warp per query below 2^17 queries, a thread per
+    # query from there); one tile and ragged groups of 32 (n_rim 70), several
+    # tiles (n_rim 333)
+    v, idx, q = _tie_fan(n_rim, seed=n_rim)
+    ref = orc.generate_sdf(v, idx, q, "none", int(S.Normal))
+    assert_bit_equal(m2s.generate_sdf(v, T.TriangleList(idx), q, A.none(S.Normal)), ref, "warp per query")
+    big = np.tile(q, ((1 << 17) // len(q) + 1, 1))
+    gpu = m2s.generate_sdf(v, T.TriangleList(idx), big, A.none(S.Normal))
+    assert_bit_equal(gpu, np.tile(ref, (1 << 17) // len(q) + 1), "thread per query")
+
+
 def test_topology_encodings(orc):
     # generate/grid.rs:844-901 and lib.rs:193-215: u16, u32, no-index list, strips
     v, idx = synth.icosphere(2)
