@@ -415,41 +415,34 @@ __global__ void k_collect(const __grid_constant__ GridSet gs, const unsigned lon
 // and advances it from the global list counts after each grid barrier, so no
 // block waits for a scheduler.
 //
-// Two-level arrival counters (groups of kBarrierFan blocks, then the group
-// leaders) keep the atomics of a barrier from queueing on one address.  Each
-// counter lives in its own 128-byte line.
-constexpr int kBarrierFan = 16;
-constexpr int kBarrierGroups = 128;  // supports up to 2048 co-resident blocks
+// One arrival counter for every barrier of a launch: a block adds 1 when it
+// arrives at its g-th barrier and passes once the counter has reached
+// g x blocks.  The counter is never reset, so nothing but the last arrival
+// stands between the blocks and the release (arrival and wait are a
+// fire-and-forget add and polls of one word), and comparisons are by signed
+// difference, which stays right when the counter wraps: while a block waits
+// at barrier g, barrier g - 1 is complete and no block is past g + 1, so
+// its difference stays inside (-blocks, blocks).
+constexpr unsigned int kMaxBarrierBlocks = 2048;
 struct GridBarrier {
-  unsigned int gen;
+  unsigned int arrivals;
   unsigned int abort;
   unsigned int pad0[30];
-  unsigned int top[32];
-  unsigned int group[kBarrierGroups][32];
 };
 
-__device__ __forceinline__ unsigned int atom_add_acq_rel(unsigned int* p, unsigned int v) {
-  unsigned int old;
-  asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
-  return old;
-}
 __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
   unsigned int v;
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
-__device__ __forceinline__ void st_release(unsigned int* p, unsigned int v) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
 
 // Barrier over the co-resident blocks of a cooperative launch.  Every block
-// passes the same sequence of barriers, so each keeps the generation count in
-// shared memory and waits for the global one to reach its next value: an
-// arrival costs the group atomic, the top atomic for the last of a group, and
-// the wait.  A wait spins briefly, then backs off with __nanosleep so waiting
-// blocks leave the memory system to the ones working (block 0 alone during a
-// solo run).  It is bounded in time: after kBarrierTimeoutNs it raises
-// `abort`, which makes every block leave the kernel at its next barrier.
+// passes the same sequence of barriers, so each keeps its barrier count g in
+// shared memory and waits for the arrivals to reach g x blocks.  A wait spins
+// briefly, then backs off with __nanosleep so waiting blocks leave the memory
+// system to the ones working (block 0 alone during a solo run).  It is bounded
+// in time: after kBarrierTimeoutNs it gives up, and every block leaves the
+// kernel at its next barrier (kAbortOffset below).
 constexpr uint64_t kBarrierTimeoutNs = 2000000000ull;  // two seconds
 constexpr uint32_t kBarrierSpins = 64;
 
@@ -459,38 +452,40 @@ __device__ __forceinline__ uint64_t global_ns() {
   return t;
 }
 
+__device__ __forceinline__ void red_add_release(unsigned int* p, unsigned int v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// The first block to give up adds kAbortOffset to the counter once (the
+// abort word picks that block): every later wait, in any barrier of the
+// launch, then sees a difference of about 2^30 and leaves as well.
+constexpr unsigned int kAbortOffset = 1u << 30;
 __device__ __forceinline__ bool grid_barrier(GridBarrier* bar, unsigned int nblocks, unsigned int* gen) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    const unsigned int target = *gen + 1;
-    const unsigned int grp = blockIdx.x / kBarrierFan;
-    const unsigned int ngroups = (nblocks + kBarrierFan - 1) / kBarrierFan;
-    const unsigned int in_grp = min((unsigned)kBarrierFan, nblocks - grp * kBarrierFan);
-    bool last = false;
-    if (atom_add_acq_rel(&bar->group[grp][0], 1u) == in_grp - 1) {
-      bar->group[grp][0] = 0;  // nobody touches this counter again before the release below
-      last = atom_add_acq_rel(&bar->top[0], 1u) == ngroups - 1;
-    }
-    if (last) {
-      bar->top[0] = 0;
-      st_release(&bar->gen, target);
-    } else {
-      uint32_t polls = 0;
-      uint64_t t0 = 0;
-      while (ld_acquire(&bar->gen) != target) {
-        if (ld_acquire(&bar->abort)) break;
-        if (++polls < kBarrierSpins) continue;
-        if (polls == kBarrierSpins) t0 = global_ns();
-        __nanosleep(256);
-        if (global_ns() - t0 > kBarrierTimeoutNs) {
-          atomicExch(&bar->abort, 1u);
-          break;
-        }
+    const unsigned int target = (*gen + 1u) * nblocks;
+    red_add_release(&bar->arrivals, 1u);
+    uint32_t polls = 0;
+    uint64_t t0 = 0;
+    int pass = 1;
+    for (;;) {
+      const int diff = (int)(ld_acquire(&bar->arrivals) - target);
+      if (diff >= (int)(kAbortOffset >> 2)) {
+        pass = 0;
+        break;
+      }
+      if (diff >= 0) break;
+      if (++polls < kBarrierSpins) continue;
+      if (polls == kBarrierSpins) t0 = global_ns();
+      __nanosleep(256);
+      if (global_ns() - t0 > kBarrierTimeoutNs) {
+        if (atomicExch(&bar->abort, 1u) == 0u) atomicAdd(&bar->arrivals, kAbortOffset);
+        pass = 0;
+        break;
       }
     }
-    *gen = target;
-    ok = ld_acquire(&bar->abort) ? 0 : 1;
+    *gen = *gen + 1u;
+    ok = pass;
   }
   __syncthreads();
   return ok != 0;
@@ -1438,7 +1433,7 @@ int GridJob::prepare(const MeshView* meshes, uint32_t n, const GridDesc* gds, in
     return M2S_ERR_CUDA;
   }
   J.coop_max = (unsigned)std::min<unsigned long long>((unsigned long long)sms * per_sm,
-                                                     (unsigned long long)kBarrierFan * kBarrierGroups);
+                                                     (unsigned long long)kMaxBarrierBlocks);
   if (tune.blocks_per_sm > 0) per_sm = std::min(per_sm, tune.blocks_per_sm);
   const unsigned long long cpb = std::max<uint32_t>(tune.cells_per_block, 1);
   // At least one block per SM: a round's proposals are chains of dependent
