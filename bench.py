@@ -36,7 +36,7 @@ SEED = 0
 
 # DRAM bytes (read + write) of one propagation launch of this workload, from an
 # ncu capture of dram__bytes_read.sum and dram__bytes_write.sum (one launch).
-PROPAGATE_DRAM_BYTES = 326_975_744 + 438_171_136
+PROPAGATE_DRAM_BYTES = 324_104_960 + 438_122_752
 
 
 def workload():
