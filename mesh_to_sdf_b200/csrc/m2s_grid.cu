@@ -155,7 +155,8 @@ struct Sched {
   uint32_t b, B;
   uint32_t slot[kRing];
   uint32_t cur, fp, round, n;
-  uint32_t steps;  // rounds + redistributions so far
+  uint32_t prev_n;  // states of the relax round before this one
+  uint32_t steps;   // rounds + redistributions so far
   int action;
 };
 
@@ -544,6 +545,7 @@ __device__ __forceinline__ int next_step(Sched& sh, const Counters& ct, uint32_t
     if (lane == 0) {
       sh.cur = moved;
       sh.b = b + q;
+      sh.prev_n = sh.n;
       sh.n = nq;
       sh.round += 1;
       if (leader) ct.count[cur] = 0;
@@ -568,6 +570,15 @@ __device__ __forceinline__ int next_step(Sched& sh, const Counters& ct, uint32_t
 // depend on which threads do it: results are the same either way.
 constexpr uint32_t kSoloRounds = 1024;  // the threshold (default 64 states) is GridTuning::solo_max
 constexpr uint32_t kSoloCap = 64;  // largest solo_max
+// A run starts at the second small round in a row: an isolated small round
+// (a lull between large ones) costs more as a run of one, which adds a
+// barrier's wait for the other blocks and the schedule handoff, than on every
+// block (star s6 256^3: 10.12 -> 9.94 ms; star s4 96^3: 1.72 -> 1.57 ms),
+// while chains of small rounds still run alone (terrain 384x384x128 Normal:
+// 23.7 -> 23.3 ms).  Every block decides from the same schedule.
+__device__ __forceinline__ bool solo_round(const Sched& sh, uint32_t solo_max) {
+  return sh.n <= solo_max && sh.prev_n <= solo_max;
+}
 
 // Queue of one warp's proposals that need a distance evaluation (Normal sign).
 constexpr uint32_t kQueue = 64;
@@ -892,6 +903,7 @@ __global__ void __launch_bounds__(256, 4) k_propagate(const __grid_constant__ Gr
     sh.fp = st->fp;
     sh.round = 0;
     sh.steps = 0;
+    sh.n = 0xFFFFFFFFu;  // no relax round yet: the first is never solo
   }
   bool nan = false;
   unsigned long long evals = 0;
@@ -917,7 +929,7 @@ __global__ void __launch_bounds__(256, 4) k_propagate(const __grid_constant__ Gr
     // a solo round) or the far list's size (bit 31) — and when it was chosen.
     if (lead_block && round_log && logged < log_cap) {
       uint32_t v = 0;
-      if (sh.action == kRelax) v = sh.n | (sh.n <= solo_max ? 0x40000000u : 0u);
+      if (sh.action == kRelax) v = sh.n | (solo_round(sh, solo_max) ? 0x40000000u : 0u);
       else if (sh.action == kRedistribute) v = 0x80000000u | counters(in_run).count[kFar0 + sh.fp];
       else v = 0xC0000000u;  // the end
       round_log[2 * logged] = v;
@@ -989,7 +1001,7 @@ __global__ void __launch_bounds__(256, 4) k_propagate(const __grid_constant__ Gr
       continue;
     }
     // ---- a relax round: by every block, or by block 0 alone when it is small
-    const bool solo = sh.n <= solo_max;
+    const bool solo = solo_round(sh, solo_max);
     if (solo && !s_solo_run) {
       // A solo run starts.  Block 0 will change list counts at once (pushes,
       // and emptying the list it relaxes at its next step), so every block
@@ -1072,7 +1084,7 @@ __global__ void __launch_bounds__(256, 4) k_propagate(const __grid_constant__ Gr
     if (threadIdx.x == 0) {
       ++s_runs;
       ++solo_rounds;
-      s_more = sh.action == kRelax && sh.n <= solo_max && s_runs < kSoloRounds;
+      s_more = sh.action == kRelax && solo_round(sh, solo_max) && s_runs < kSoloRounds;
       if (!s_more) {
         for (int k = 0; k < kLists; ++k) st->count[k] = s_count[k];
         st->far_min[0] = s_far_min[0];

@@ -454,10 +454,12 @@ def test_grid_solo_rounds_do_not_change_results():
             lo, hi = synth.padded_bbox(v)
             grid = m2s.Grid.from_bounding_box(lo, hi, [40, 44, 36])
             topo = T.TriangleStrip(idx) if strip else T.TriangleList(idx)
-            outs = []
+            outs, solo_rounds = [], []
             for solo in (0, 64, 4096):
                 m2s.set_grid_tuning(solo_max=solo)
                 outs.append(m2s.generate_grid_sdf(v, topo, grid, sign))
+                solo_rounds.append(m2s.last_grid_stats()["solo_rounds"])
             assert np.array_equal(bits(outs[0]), bits(outs[1])) and np.array_equal(bits(outs[0]), bits(outs[2]))
+            assert solo_rounds[0] == 0 and solo_rounds[1] > 0, solo_rounds
     finally:
         m2s.set_grid_tuning()
