@@ -314,13 +314,20 @@ __global__ void k_seed(const __grid_constant__ GridSet gs, const TriRec* __restr
   long long total = ex * ey * ez;
   bool nan = false;
   uint32_t updates = 0;
-  for (long long k = lane; k < total; k += 32) {
-    int z = mn[2] + (int)(k % ez);
-    int y = mn[1] + (int)((k / ez) % ey);
-    int x = mn[0] + (int)(k / (ez * ey));
+  auto visit = [&](int x, int y, int z) {
     float d = cell_distance<SIGN>(center(g, x, y, z), a, b, c, kind);
     if (isnan(d)) nan = true;
     if (update_min<SIGN>(&keys[g.cell_off + local_index(g, x, y, z)], pack(d, t), &nan)) ++updates;
+  };
+  if (total <= 0x7FFFFFFFll) {  // 32-bit division (64-bit costs ~4x the instructions)
+    const uint32_t uez = (uint32_t)ez, uey = (uint32_t)ey, utotal = (uint32_t)total;
+    for (uint32_t k = lane; k < utotal; k += 32) {
+      const uint32_t q = k / uez, xq = q / uey;
+      visit(mn[0] + (int)xq, mn[1] + (int)(q - xq * uey), mn[2] + (int)(k - q * uez));
+    }
+  } else {
+    for (long long k = lane; k < total; k += 32)
+      visit(mn[0] + (int)(k / (ez * ey)), mn[1] + (int)((k / ez) % ey), mn[2] + (int)(k % ez));
   }
   if (nan) atomicOr(status, bit(M2S_ERR_NAN_DISTANCE));
   for (int o = 16; o; o >>= 1) updates += __shfl_xor_sync(0xFFFFFFFFu, updates, o);
@@ -1166,11 +1173,18 @@ __global__ void k_rays(const __grid_constant__ GridSet gs, const TriRec* __restr
   uint32_t* bitsA = bits + g.bits_off[AXIS];
   const uint32_t W = g.words[AXIS];
   uint32_t hits = 0;
+  const bool small = total <= 0x7FFFFFFFll;  // 32-bit division (64-bit costs ~4x the instructions)
   for (long long q = lane; q < total; q += 32) {
     int c3[3];
     c3[AXIS] = 0;
-    c3[IY] = j0 + (int)(q / nk);
-    c3[IZ] = k0 + (int)(q % nk);
+    if (small) {
+      const uint32_t uq = (uint32_t)q, row = uq / (uint32_t)nk;
+      c3[IY] = j0 + (int)row;
+      c3[IZ] = k0 + (int)(uq - row * (uint32_t)nk);
+    } else {
+      c3[IY] = j0 + (int)(q / nk);
+      c3[IZ] = k0 + (int)(q % nk);
+    }
     P3 o = center(g, c3[0], c3[1], c3[2]);  // ray origin: a low-face cell centre (grid.rs:580)
     float tt;
     if (!ray_hit_aligned<AXIS>(o, a, b, c, &tt)) continue;

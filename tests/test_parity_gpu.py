@@ -279,6 +279,9 @@ def test_error_statuses():
     q = [[0.1, 0.2, 0.3], [1, 1, 1]]
     out = m2s.generate_sdf(TETRA_V, T.TriangleList(empty), q, A.none(S.Raycast))
     assert out.tolist() == [np.finfo(np.float32).max] * 2  # default.rs:56
+    for n in (2, 1 << 17):  # Normal folds from f32::MAX too, on both brute-force kernels
+        qn = np.tile(np.asarray(q, np.float32), (n // 2, 1))
+        assert np.all(m2s.generate_sdf(TETRA_V, T.TriangleList(empty), qn, A.none(S.Normal)) == np.finfo(np.float32).max)
     assert len(m2s.generate_sdf(TETRA_V, T.TriangleList(empty), q, A.rtree_bvh())) == 0  # rtree_bvh.rs:96-97
     assert m2s.build_sdf_acceleration(TETRA_V, T.TriangleList(empty), A.rtree_bvh()) is None
     with pytest.raises(m2s.M2SError) as e:  # rtree.rs:317
