@@ -329,6 +329,101 @@ __device__ Nearest nearest_triangle(const MeshView& m, P3 p, bool* overflow, Nea
   return best;
 }
 
+// The same search for the 32 queries of a warp at once (Morton-adjacent
+// queries reach mostly the same nodes): the warp walks one node sequence,
+// every node fetched once for all lanes, and each lane takes a node only
+// while its own box distance is within its own best; the order of the two
+// children follows the majority of lanes.  A lane's result is the one the
+// single-thread search gives (exhaustive under its own bound, ties to the
+// lowest triangle index); `budget` counts the nodes a lane took, and a lane
+// over it stops taking nodes and clears *finished.
+template <bool STATS = false>
+__device__ Nearest nearest_triangle_packet(const MeshView& m, P3 p, bool active, bool* overflow, uint32_t budget,
+                                           bool* finished, QCount* qc = nullptr) {
+  Nearest best{INFINITY, 0xFFFFFFFFu, 0};
+  auto eval = [&](uint32_t leaf) {
+    if constexpr (STATS) ++qc->tests;
+    TriRec r = load_tri(m.stris, leaf);
+    float d2 = point_triangle_distance2(p, p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
+    uint32_t idx = __float_as_uint(r.b.w);
+    if (d2 < best.d2 || (d2 == best.d2 && idx < best.tri)) best = {d2, idx, leaf};
+  };
+  *finished = true;
+  bool live = active;  // still taking nodes
+  if (m.root & LEAF_BIT) {
+    if (live) eval(m.root & ~LEAF_BIT);
+    return best;
+  }
+  uint32_t st_node[kStack];
+  float st_dist[kStack];
+  int sp = 0;
+  uint32_t node = 0;
+  uint32_t visits = 0;
+  bool take = live;  // this lane wants `node`
+  while (true) {
+    if (take) {
+      if (++visits > budget) {
+        *finished = false;
+        live = false;
+      } else if constexpr (STATS) {
+        ++qc->visits;
+      }
+    }
+    take = take && live;
+    if (__any_sync(0xFFFFFFFFu, take)) {
+      BvhNode nd = load_node(m.nodes, node);
+      float dl = box_dist2(p, nd.l_lo, nd.l_hi), dr = box_dist2(p, nd.r_lo, nd.r_hi);
+      uint32_t L = __float_as_uint(nd.l_lo.w), R = __float_as_uint(nd.l_hi.w);
+      bool goL = take && dl <= best.d2, goR = take && dr <= best.d2;
+      if (L & LEAF_BIT) {
+        if (goL) eval(L & ~LEAF_BIT);
+        goL = false;
+      }
+      if (R & LEAF_BIT) {
+        if (goR) eval(R & ~LEAF_BIT);
+        goR = false;
+      }
+      goL = goL && dl <= best.d2;
+      goR = goR && dr <= best.d2;
+      const bool anyL = __any_sync(0xFFFFFFFFu, goL), anyR = __any_sync(0xFFFFFFFFu, goR);
+      if (anyL && anyR) {
+        const uint32_t nl = __popc(__ballot_sync(0xFFFFFFFFu, goL && (!goR || dl <= dr)));
+        const uint32_t nr = __popc(__ballot_sync(0xFFFFFFFFu, goR && (!goL || dr < dl)));
+        const bool lfirst = nl >= nr;
+        if (sp < kStack) {
+          st_node[sp] = lfirst ? R : L;
+          st_dist[sp] = (lfirst ? goR : goL) ? (lfirst ? dr : dl) : INFINITY;
+          ++sp;
+        } else if (lfirst ? goR : goL) {
+          *overflow = true;
+        }
+        node = lfirst ? L : R;
+        take = lfirst ? goL : goR;
+        continue;
+      }
+      if (anyL || anyR) {
+        node = anyL ? L : R;
+        take = anyL ? goL : goR;
+        continue;
+      }
+    }
+    // pop the next entry some lane still wants
+    bool found = false;
+    while (sp > 0) {
+      --sp;
+      const bool want = live && st_dist[sp] <= best.d2;
+      if (__any_sync(0xFFFFFFFFu, want)) {
+        node = st_node[sp];
+        take = want;
+        found = true;
+        break;
+      }
+    }
+    if (!found) break;
+  }
+  return best;
+}
+
 // (d2, triangle) packed so that the unsigned order is the search order.
 __device__ __forceinline__ unsigned long long nn_key(float d2, uint32_t tri) {
   return ((unsigned long long)__float_as_uint(d2) << 32) | tri;
@@ -653,19 +748,26 @@ __global__ void __launch_bounds__(128) k_query(MeshView m, const float* __restri
                                                const uint32_t* __restrict__ order, uint64_t nq,
                                                float* __restrict__ out, float* __restrict__ vec,
                                                uint8_t* __restrict__ inside_out, uint32_t* status, uint32_t budget,
-                                               HardQuery* hard, uint32_t* hard_count,
+                                               HardQuery* hard, uint32_t* hard_count, bool packet,
                                                unsigned long long* qstats = nullptr) {
   uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= nq) return;
-  uint64_t i = order ? order[k] : k;
-  P3 p = load_query(q, i);
+  if (!packet && k >= nq) return;  // a packet search needs every lane of the warp
+  const bool active = k < nq;
+  uint64_t i = active ? (order ? order[k] : k) : 0;
+  P3 p = active ? load_query(q, i) : P3{0.0f, 0.0f, 0.0f};
   bool overflow = false, nan = false;
   bool inside = false;
   QCount qc;
-  if (MODE == Q_BVH_RAYCAST || MODE == Q_VECTOR) inside = vote_inside<STATS>(m, p, &overflow, &qc);
   bool finished = true;
-  Nearest nn = nearest_triangle<STATS>(m, p, &overflow, Nearest{INFINITY, 0xFFFFFFFFu, 0},
-                                       (MODE == Q_BVH_NORMAL || !hard) ? 0xFFFFFFFFu : budget, &finished, &qc);
+  const uint32_t bud = (MODE == Q_BVH_NORMAL || !hard) ? 0xFFFFFFFFu : budget;
+  Nearest nn;
+  if (packet) {
+    nn = nearest_triangle_packet<STATS>(m, p, active, &overflow, bud, &finished, &qc);
+    if (!active) return;
+  } else {
+    nn = nearest_triangle<STATS>(m, p, &overflow, Nearest{INFINITY, 0xFFFFFFFFu, 0}, bud, &finished, &qc);
+  }
+  if (MODE == Q_BVH_RAYCAST || MODE == Q_VECTOR) inside = vote_inside<STATS>(m, p, &overflow, &qc);
   if (finished) {
     finish_query<MODE, STATS>(m, i, p, nn, inside, out, vec, inside_out, &nan, &overflow, &qc);
   } else {
@@ -743,6 +845,12 @@ __global__ void k_query_keys(const float* __restrict__ q, uint64_t nq, MeshView 
 // Node-visit budget of the single-thread search (0: single pass only).
 uint32_t g_query_budget = 768;
 
+// Batch size from which Raycast, Rtree and vector queries search a warp at a
+// time (measured crossover: star s6 and the 512^2 terrain are even at 400k to
+// 600k queries; 1M star points 8.0 -> 7.1 ms, 4M terrain points 15.2 -> 10.7 ms;
+// 100k star points 2.4 -> 2.9 ms).
+constexpr uint64_t kPacketMinQueries = 1u << 19;
+
 int brute_force_sdf(const MeshView& m, int sign, const float* d_q, uint64_t nq, float* d_out, uint32_t* d_status,
                     cudaStream_t s, bool allow_alloc) {
   if (nq == 0) return M2S_OK;
@@ -780,29 +888,30 @@ namespace {
 template <bool ST>
 void launch_queries(int mode, const MeshView& m, const float* d_q, const uint32_t* ord, uint64_t nq, float* d_out,
                     float* d_vec, uint8_t* d_inside, uint32_t* d_status, uint32_t budget, HardQuery* hp, uint32_t* hc,
-                    bool two_pass, unsigned blocks, unsigned long long* qs, cudaStream_t s) {
+                    bool two_pass, bool packet, unsigned blocks, unsigned long long* qs, cudaStream_t s) {
   const unsigned hard_blocks = 148u * 32u;
   switch (mode) {
     case Q_BVH_RAYCAST:
       k_query<Q_BVH_RAYCAST, ST><<<blocks, 128, 0, s>>>(m, d_q, ord, nq, d_out, nullptr, nullptr, d_status, budget, hp,
-                                                        hc, qs);
+                                                        hc, packet, qs);
       if (two_pass)
         k_query_hard<Q_BVH_RAYCAST, ST><<<hard_blocks, 32 * kHardWarps, 0, s>>>(m, d_q, hp, hc, d_out, nullptr,
                                                                                   nullptr, d_status, qs);
       break;
     case Q_BVH_NORMAL:
       k_query<Q_BVH_NORMAL, ST><<<blocks, 128, 0, s>>>(m, d_q, ord, nq, d_out, nullptr, nullptr, d_status, budget,
-                                                       nullptr, nullptr, qs);
+                                                       nullptr, nullptr, packet, qs);
       break;
     case Q_RTREE:
-      k_query<Q_RTREE, ST><<<blocks, 128, 0, s>>>(m, d_q, ord, nq, d_out, nullptr, nullptr, d_status, budget, hp, hc, qs);
+      k_query<Q_RTREE, ST><<<blocks, 128, 0, s>>>(m, d_q, ord, nq, d_out, nullptr, nullptr, d_status, budget, hp, hc,
+                                                  packet, qs);
       if (two_pass)
         k_query_hard<Q_RTREE, ST><<<hard_blocks, 32 * kHardWarps, 0, s>>>(m, d_q, hp, hc, d_out, nullptr, nullptr,
                                                                             d_status, qs);
       break;
     default:
       k_query<Q_VECTOR, ST><<<blocks, 128, 0, s>>>(m, d_q, ord, nq, nullptr, d_vec, d_inside, d_status, budget, hp, hc,
-                                                   qs);
+                                                   packet, qs);
       if (two_pass)
         k_query_hard<Q_VECTOR, ST><<<hard_blocks, 32 * kHardWarps, 0, s>>>(m, d_q, hp, hc, nullptr, d_vec, d_inside,
                                                                              d_status, qs);
@@ -853,12 +962,17 @@ int query_points(const MeshView& m, int accel, int sign, const float* d_q, uint6
     if ((st = qs.alloc(4, s))) return st;
     M2S_CUDA(cudaMemsetAsync(qs.p, 0, 32, s));
   }
+  // Morton-ordered warps search together (nearest_triangle_packet): always
+  // for Bvh(Normal), whose searches have no budget, and for the others from
+  // kPacketMinQueries on, where throughput rather than the longest warp sets
+  // the time.
+  const bool packet = ord != nullptr && (mode == Q_BVH_NORMAL || nq >= kPacketMinQueries);
   if (counting)
-    launch_queries<true>(mode, m, d_q, ord, nq, d_out, d_vec, d_inside, d_status, budget, hp, hc, two_pass, blocks,
-                         qs.p, s);
+    launch_queries<true>(mode, m, d_q, ord, nq, d_out, d_vec, d_inside, d_status, budget, hp, hc, two_pass, packet,
+                         blocks, qs.p, s);
   else
-    launch_queries<false>(mode, m, d_q, ord, nq, d_out, d_vec, d_inside, d_status, budget, hp, hc, two_pass, blocks,
-                          nullptr, s);
+    launch_queries<false>(mode, m, d_q, ord, nq, d_out, d_vec, d_inside, d_status, budget, hp, hc, two_pass, packet,
+                          blocks, nullptr, s);
   M2S_CUDA(cudaGetLastError());
   if (counting) {
     unsigned long long h[4];

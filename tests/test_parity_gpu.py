@@ -211,6 +211,31 @@ def test_large_batch_morton_order(orc):
         assert_bit_equal(m2s.generate_sdf(v, T.TriangleList(idx), q, am), orc_sdf(orc, v, idx, q, am), repr(am))
 
 
+def test_packet_search_bit_exact(orc):
+    # Morton-ordered batches search a warp at a time (always for Bvh(Normal),
+    # from 2^19 queries for the others): the same bits as the oracle, with a
+    # ragged last warp; the hard pass still takes over-budget lanes
+    v, idx = synth.star(3, seed=5)
+    q = synth.mixed_points(v, idx, (1 << 19) + 777, seed=9)
+    topo = T.TriangleList(idx)
+    for am in (A.bvh(S.Raycast), A.rtree(), A.rtree_bvh(), A.bvh(S.Normal)):
+        assert_bit_equal(m2s.generate_sdf(v, topo, q, am), orc_sdf(orc, v, idx, q, am), repr(am))
+    assert_bit_equal(m2s.generate_sdf(v, topo, q[:5000], A.bvh(S.Normal)),
+                     orc_sdf(orc, v, idx, q[:5000], A.bvh(S.Normal)), "Bvh(Normal) 5000")
+    acc = m2s.build_sdf_acceleration(v, topo, A.rtree_bvh())
+    vec, inside = m2s.query_vector_to_closest_point_rtree_bvh(acc, q)
+    ov, oi = orc.query_vector_to_closest_point(v, idx, q)
+    assert_bit_equal(vec.reshape(-1), ov.reshape(-1), "vectors")
+    assert np.array_equal(inside, oi)
+    L = m2s._lib.lib()
+    saved = L.m2s_query_budget()
+    try:  # a small budget sends many lanes of each warp to the hard pass
+        L.m2s_set_query_budget(64)
+        assert_bit_equal(m2s.generate_sdf(v, topo, q, A.rtree()), orc_sdf(orc, v, idx, q, A.rtree()), "budget 64")
+    finally:
+        L.m2s_set_query_budget(saved)
+
+
 def test_query_counting_changes_no_result():
     # profiling runs the counting kernel instantiations: same bits, sane counts
     v, idx = synth.star(4, seed=5)
