@@ -317,6 +317,7 @@ def main():
     ap.add_argument("--small", action="store_true",
                     help="one short pass for profilers: one grid, 100k Rtree / RtreeBvh points, 8k brute-force points")
     ap.add_argument("--grid", type=int, default=128, help="grid edge of the --small pass")
+    ap.add_argument("--points", type=int, default=100_000, help="query points of the --small pass")
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
                     help="c2 (default): the headline line; c1 / c3: the small and the terrain configurations; "
                          "c4: 256 grids batched in one plan against 256 single-grid calls; "
@@ -328,7 +329,7 @@ def main():
     ap.add_argument("--wave-cells", type=int, default=0, help="c4: cells per batched job (0 = the library default)")
     args = ap.parse_args()
     if args.small:
-        return small_case(args.grid)
+        return small_case(args.grid, args.points)
     if args.impl == "reference" and args.workload in ("c1", "c3", "c4"):
         return reference_workloads(args)
     if args.workload == "c4":
@@ -836,8 +837,9 @@ def serving_workload(args):
                       "server_stats": stats}), flush=True)
 
 
-def small_case(edge=128):
-    """A short, fixed workload for ncu captures (at most ~1.5 GB on the device)."""
+def small_case(edge=128, points=100_000):
+    """A short, fixed workload for ncu captures (at most ~1.5 GB on the device);
+    from 2^19 points the queries take the warp-packet search."""
     import torch
 
     import mesh_to_sdf_b200 as m2s
@@ -850,13 +852,13 @@ def small_case(edge=128):
     out = torch.empty(grid.get_total_cell_count(), dtype=torch.float32, device="cuda")
     status = torch.zeros(1, dtype=torch.int32, device="cuda")
     mesh.grid_device(grid, S.Raycast, out, status)
-    q = torch.from_numpy(synth.mixed_points(v, idx, 100_000, seed=SEED)).cuda()
-    qo = torch.empty(100_000, dtype=torch.float32, device="cuda")
+    q = torch.from_numpy(synth.mixed_points(v, idx, points, seed=SEED)).cuda()
+    qo = torch.empty(points, dtype=torch.float32, device="cuda")
     mesh.query_device(q, qo, status)
     rt = m2s.build_sdf_acceleration(v, m2s.Topology.TriangleList(idx), A.rtree())
     rt.query_device(q, qo, status)
     bf = m2s.build_sdf_acceleration(v, m2s.Topology.TriangleList(idx), A.none(S.Raycast))
-    bf.query_device(q[:8192].contiguous(), qo, status)
+    bf.query_device(q[:8192].contiguous(), qo[:8192], status)
     torch.cuda.synchronize()
     assert int(status.item()) == 0
     print("small ok", m2s.last_grid_stats())
