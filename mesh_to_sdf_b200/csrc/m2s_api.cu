@@ -187,7 +187,7 @@ void record_query_stats(const uint64_t stats[5]) {
 void record_round_log(const std::vector<uint32_t>& log) { t_round_log = log; }
 
 int dev_alloc(void** p, size_t bytes, cudaStream_t s) {
-  cudaMemPool_t pool;
+  cudaMemPool_t pool = nullptr;
   int st = current_pool(&pool);
   if (st) return st;
   cudaError_t e = cudaMallocFromPoolAsync(p, bytes, pool, s);
