@@ -166,7 +166,8 @@ void m2s_grid_plan_free(m2s_grid_plan* plan);
 void m2s_clear_grid_autotune(void);
 
 /* Process-wide grid knobs; they change speed, never results.  blocks_per_sm:
- * cooperative propagation blocks per SM (0 = occupancy limit);
+ * cooperative propagation blocks per SM (0 = occupancy limit; the server's
+ * grid waves then run 3 per SM, leaving room for point queries);
  * cells_per_block: the propagation launch uses ceil(cells / this) blocks, at
  * least one per SM (0 = 1024); wave_cells: a batch runs as jobs of at most this many
  * cells, largest grids first (a larger grid alone); grids in one job share its
