@@ -4,8 +4,9 @@
 //    every triangle.  Triangle tiles are staged in shared memory by the bulk
 //    copy engine (cp.async.bulk + mbarrier, double-buffered); each thread owns
 //    one query and folds the tile in triangle order, exactly the reference's
-//    fold order.  Normal batches of fewer than 2^17 queries take
-//    k_brute_normal_warp: a warp per query, the same fold in the same order.
+//    fold order; batches of 4096 queries or more are visited in Morton order.
+//    Normal batches of fewer than 2^17 queries take k_brute_normal_warp: a
+//    warp per query, the same fold in the same order.
 //  * Bvh(Raycast) / RtreeBvh (bvh.rs:256-332, rtree_bvh.rs:143-201): exact
 //    nearest triangle on the LBVH, then the 3-axis ray vote.
 //  * Rtree (rtree.rs:306-326): the nearest triangle's signed distance.
@@ -40,12 +41,13 @@ template <int SIGN>
 __global__ void __launch_bounds__(kBfThreads) k_brute(const TriRec* __restrict__ tris, uint32_t T,
                                                       const float* __restrict__ q, uint64_t nq,
                                                       float* __restrict__ out, uint32_t* status,
-                                                      uint2* __restrict__ part) {
+                                                      uint2* __restrict__ part, const uint32_t* __restrict__ order) {
   __shared__ __align__(128) TriRec tile[2][kBfTile];
   __shared__ __align__(8) uint64_t bar[2];
   const int tid = threadIdx.x;
-  const uint64_t qi = (uint64_t)blockIdx.x * kBfThreads + tid;
-  const bool valid = qi < nq;
+  const uint64_t k = (uint64_t)blockIdx.x * kBfThreads + tid;
+  const bool valid = k < nq;
+  const uint64_t qi = valid && order ? order[k] : k;  // Morton order: a warp's queries share region branches
   const P3 p = valid ? load_query(q, qi) : P3{0.0f, 0.0f, 0.0f};
   // this block's chunk of triangles: whole tiles [t_begin, t_end)
   const uint32_t all_tiles = (T + kBfTile - 1) / kBfTile;
@@ -851,23 +853,89 @@ uint32_t g_query_budget = 768;
 // 100k star points 2.4 -> 2.9 ms).
 constexpr uint64_t kPacketMinQueries = 1u << 19;
 
+namespace {
+// Order-preserving int image of a float (for atomic min / max).
+__device__ __forceinline__ int f2o(float f) {
+  const int i = __float_as_int(f);
+  return i >= 0 ? i : i ^ 0x7FFFFFFF;
+}
+__device__ __forceinline__ float o2f(int i) { return __int_as_float(i >= 0 ? i : i ^ 0x7FFFFFFF); }
+__global__ void k_bf_bounds_init(int* b) {
+  if (threadIdx.x < 3) b[threadIdx.x] = 0x7FFFFFFF;
+  else if (threadIdx.x < 6) b[threadIdx.x] = (int)0x80000000;
+}
+__global__ void k_bf_bounds(const float* __restrict__ q, uint64_t nq, int* b) {
+  int lo[3] = {0x7FFFFFFF, 0x7FFFFFFF, 0x7FFFFFFF}, hi[3] = {(int)0x80000000, (int)0x80000000, (int)0x80000000};
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += (uint64_t)gridDim.x * blockDim.x)
+    for (int d = 0; d < 3; ++d) {
+      const int v = f2o(q[3 * i + d]);
+      lo[d] = min(lo[d], v);
+      hi[d] = max(hi[d], v);
+    }
+  for (int d = 0; d < 3; ++d) {
+    for (int o = 16; o; o >>= 1) {
+      lo[d] = min(lo[d], __shfl_xor_sync(0xFFFFFFFFu, lo[d], o));
+      hi[d] = max(hi[d], __shfl_xor_sync(0xFFFFFFFFu, hi[d], o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicMin(&b[d], lo[d]);
+      atomicMax(&b[3 + d], hi[d]);
+    }
+  }
+}
+__global__ void k_bf_keys(const float* __restrict__ q, uint64_t nq, const int* __restrict__ b, uint32_t* keys,
+                          uint32_t* vals) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nq) return;
+  uint32_t key = 0;
+  for (int d = 0; d < 3; ++d) {
+    const float l = o2f(b[d]), h = o2f(b[3 + d]);
+    const float ext = h - l;
+    const float u = ext > 0.0f ? (q[3 * i + d] - l) / ext : 0.0f;
+    const uint32_t v = (uint32_t)fminf(fmaxf(u * 1024.0f, 0.0f), 1023.0f);  // NaN -> 0
+    for (int bt = 0; bt < 10; ++bt) key |= ((v >> bt) & 1u) << (3 * bt + (2 - d));
+  }
+  keys[i] = key;
+  vals[i] = (uint32_t)i;
+}
+}  // namespace
+
 int brute_force_sdf(const MeshView& m, int sign, const float* d_q, uint64_t nq, float* d_out, uint32_t* d_status,
                     cudaStream_t s, bool allow_alloc) {
   if (nq == 0) return M2S_OK;
   unsigned blocks = (unsigned)((nq + kBfThreads - 1) / kBfThreads);
+  // Thread-per-query kernels visit large batches in Morton order (of the
+  // queries' own bounding box): the lanes of a warp then mostly fall in the
+  // same Voronoi regions of a triangle and take the same branches (65,536
+  // points x 81,920 triangles Raycast 24.3 -> 21.2 ms, 262,144 Normal 108.5
+  // -> 88.9 ms).  Results are per query, so the order changes none.
+  DevBuf<uint32_t> keys, order;
+  DevBuf<int> bounds;
+  const uint32_t* ord = nullptr;
+  const bool thread_kernel = sign == M2S_SIGN_RAYCAST || nq >= kBruteWarpMaxQueries;
+  if (allow_alloc && thread_kernel && nq >= 4096 && nq <= 0xFFFFFFFFull) {
+    int st;
+    if ((st = keys.alloc(nq, s)) || (st = order.alloc(nq, s)) || (st = bounds.alloc(6, s))) return st;
+    k_bf_bounds_init<<<1, 32, 0, s>>>(bounds.p);
+    k_bf_bounds<<<(unsigned)std::min<uint64_t>((nq + 255) / 256, 148u * 8u), 256, 0, s>>>(d_q, nq, bounds.p);
+    k_bf_keys<<<(unsigned)((nq + 255) / 256), 256, 0, s>>>(d_q, nq, bounds.p, keys.p, order.p);
+    M2S_CUDA(cudaGetLastError());
+    if ((st = radix_sort_pairs(keys.p, order.p, nq, 30, s))) return st;
+    ord = order.p;
+  }
   if (sign == M2S_SIGN_RAYCAST) {
     // Enough (query, triangle chunk) blocks to fill the GPU ~4 deep.
     const uint32_t tiles = (m.n_tris + kBfTile - 1) / kBfTile;
     uint32_t chunks = (uint32_t)std::max<uint64_t>(1, (148ull * 16ull + blocks - 1) / blocks);
     chunks = std::max(1u, std::min(chunks, std::min(tiles, 64u)));
     if (chunks == 1 || !allow_alloc) {
-      k_brute<0><<<blocks, kBfThreads, 0, s>>>(m.tris, m.n_tris, d_q, nq, d_out, d_status, nullptr);
+      k_brute<0><<<blocks, kBfThreads, 0, s>>>(m.tris, m.n_tris, d_q, nq, d_out, d_status, nullptr, ord);
     } else {
       DevBuf<uint2> part;
       int st = part.alloc(nq, s);
       if (st) return st;
       k_brute_init<<<(unsigned)std::min<uint64_t>((nq + 255) / 256, 148u * 16u), 256, 0, s>>>(part.p, nq);
-      k_brute<0><<<dim3(blocks, chunks), kBfThreads, 0, s>>>(m.tris, m.n_tris, d_q, nq, d_out, d_status, part.p);
+      k_brute<0><<<dim3(blocks, chunks), kBfThreads, 0, s>>>(m.tris, m.n_tris, d_q, nq, d_out, d_status, part.p, ord);
       k_brute_finish<<<(unsigned)std::min<uint64_t>((nq + 255) / 256, 148u * 16u), 256, 0, s>>>(part.p, nq, d_out);
     }
   } else if (nq < kBruteWarpMaxQueries) {
@@ -878,7 +946,7 @@ int brute_force_sdf(const MeshView& m, int sign, const float* d_q, uint64_t nq, 
     const unsigned wblocks = (unsigned)((nq + kBwThreads / 32 - 1) / (kBwThreads / 32));
     k_brute_normal_warp<<<wblocks, kBwThreads, 0, s>>>(m.tris, m.n_tris, d_q, nq, d_out, d_status);
   } else {
-    k_brute<1><<<blocks, kBfThreads, 0, s>>>(m.tris, m.n_tris, d_q, nq, d_out, d_status, nullptr);
+    k_brute<1><<<blocks, kBfThreads, 0, s>>>(m.tris, m.n_tris, d_q, nq, d_out, d_status, nullptr, ord);
   }
   M2S_CUDA(cudaGetLastError());
   return M2S_OK;

@@ -236,6 +236,15 @@ def test_packet_search_bit_exact(orc):
         L.m2s_set_query_budget(saved)
 
 
+def test_brute_force_morton_order(orc):
+    # None visits batches of 4096 or more queries in Morton order (Raycast:
+    # chunked over triangles too); results stay in input order, bit-exact
+    v, idx = synth.star(3, seed=6)
+    q = synth.mixed_points(v, idx, 6001, seed=12)
+    for am in (A.none(S.Raycast), A.none(S.Normal)):
+        assert_bit_equal(m2s.generate_sdf(v, T.TriangleList(idx), q, am), orc_sdf(orc, v, idx, q, am), repr(am))
+
+
 def test_query_counting_changes_no_result():
     # profiling runs the counting kernel instantiations: same bits, sane counts
     v, idx = synth.star(4, seed=5)
