@@ -859,6 +859,8 @@ def small_case(edge=128, points=100_000):
     rt.query_device(q, qo, status)
     bf = m2s.build_sdf_acceleration(v, m2s.Topology.TriangleList(idx), A.none(S.Raycast))
     bf.query_device(q[:8192].contiguous(), qo[:8192], status)
+    bn = m2s.build_sdf_acceleration(v, m2s.Topology.TriangleList(idx), A.none(S.Normal))
+    bn.query_device(q[:8192].contiguous(), qo[:8192], status)
     torch.cuda.synchronize()
     assert int(status.item()) == 0
     print("small ok", m2s.last_grid_stats())
