@@ -195,40 +195,72 @@ __global__ void k_hist(const uint32_t* __restrict__ keys, uint64_t n, int shift,
   hist[(uint64_t)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
 }
 
-// Stable scatter: within a tile, keys keep their input order per digit.
+// Stable scatter: within a tile, keys keep their input order per digit.  The
+// tile is first ordered by digit in shared memory (a key's place: the tile's
+// start of its digit, from the scanned offsets, plus the same-digit keys
+// before it), then each digit's run is written out contiguously, so
+// neighbouring threads write neighbouring addresses.
 __global__ void k_scatter(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint32_t* kout,
                           uint32_t* vout, uint64_t n, int shift, const uint32_t* offsets, uint32_t nblocks) {
   __shared__ uint32_t run[kDigits];
   __shared__ uint32_t wcnt[kThreads / 32][kDigits];
   __shared__ uint32_t base_off[kDigits];
+  __shared__ uint32_t tile_start[kDigits];
+  __shared__ uint32_t s_key[kSortTile], s_val[kSortTile];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  run[threadIdx.x] = 0;
-  base_off[threadIdx.x] = offsets[(uint64_t)threadIdx.x * nblocks + blockIdx.x];
+  const uint64_t base = (uint64_t)blockIdx.x * kSortTile;
+  const uint32_t tile_n = (uint32_t)(n - base < (uint64_t)kSortTile ? n - base : (uint64_t)kSortTile);
+  {
+    // this tile's count of digit d: the next offset (digit-major) minus its own
+    const uint64_t idx = (uint64_t)threadIdx.x * nblocks + blockIdx.x;
+    const uint32_t off = offsets[idx];
+    const uint32_t next = idx + 1 < (uint64_t)kDigits * nblocks ? offsets[idx + 1] : (uint32_t)n;
+    base_off[threadIdx.x] = off;
+    // exclusive scan of the counts over the 256 digits (one per thread)
+    uint32_t c = next - off, incl = c;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) wcnt[0][warp] = incl;
+    __syncthreads();
+    uint32_t wbase = 0;
+    for (int w = 0; w < warp; ++w) wbase += wcnt[0][w];
+    tile_start[threadIdx.x] = wbase + incl - c;
+    run[threadIdx.x] = 0;
+    __syncthreads();
+  }
   const uint32_t lt_mask = (1u << lane) - 1u;
-  uint64_t base = (uint64_t)blockIdx.x * kSortTile;
   for (int it = 0; it < kSortItems; ++it) {
     for (int w = 0; w < kThreads / 32; ++w) wcnt[w][threadIdx.x] = 0;
     __syncthreads();
-    uint64_t k = base + (uint64_t)it * kThreads + threadIdx.x;
-    bool valid = k < n;
-    uint32_t key = valid ? kin[k] : 0, val = valid ? vin[k] : 0;
-    uint32_t digit = valid ? (key >> shift) & 0xFFu : 0x100u;
-    uint32_t peers = __match_any_sync(0xFFFFFFFFu, digit);
-    uint32_t lrank = __popc(peers & lt_mask);
+    const uint32_t t = (uint32_t)it * kThreads + threadIdx.x;
+    const bool valid = t < tile_n;
+    const uint32_t key = valid ? kin[base + t] : 0, val = valid ? vin[base + t] : 0;
+    const uint32_t digit = valid ? (key >> shift) & 0xFFu : 0x100u;
+    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, digit);
+    const uint32_t lrank = __popc(peers & lt_mask);
     if (valid && lrank == 0) wcnt[warp][digit] = __popc(peers);
     __syncthreads();
     if (valid) {
       uint32_t before = run[digit];
       for (int w = 0; w < warp; ++w) before += wcnt[w][digit];
-      uint32_t dst = base_off[digit] + before + lrank;
-      kout[dst] = key;
-      vout[dst] = val;
+      const uint32_t pos = tile_start[digit] + before + lrank;  // < tile_n
+      s_key[pos] = key;
+      s_val[pos] = val;
     }
     __syncthreads();
     uint32_t add = 0;
     for (int w = 0; w < kThreads / 32; ++w) add += wcnt[w][threadIdx.x];
     run[threadIdx.x] += add;
     __syncthreads();
+  }
+  for (uint32_t t = threadIdx.x; t < tile_n; t += kThreads) {
+    const uint32_t key = s_key[t];
+    const uint32_t d = (key >> shift) & 0xFFu;
+    const uint32_t dst = base_off[d] + (t - tile_start[d]);
+    kout[dst] = key;
+    vout[dst] = s_val[t];
   }
 }
 

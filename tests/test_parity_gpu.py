@@ -227,6 +227,11 @@ def test_packet_search_bit_exact(orc):
     ov, oi = orc.query_vector_to_closest_point(v, idx, q)
     assert_bit_equal(vec.reshape(-1), ov.reshape(-1), "vectors")
     assert np.array_equal(inside, oi)
+    tv, ti = synth.terrain(40, seed=2)  # a strip of long flat triangles, uniform points
+    tq = synth.uniform_points((1 << 19) + 33, *synth.padded_bbox(tv), seed=3)
+    for am in (A.rtree(), A.bvh(S.Normal), A.bvh(S.Raycast)):
+        assert_bit_equal(m2s.generate_sdf(tv, T.TriangleStrip(ti), tq, am),
+                         orc_sdf(orc, tv, ti, tq, am, strip=True), "terrain " + repr(am))
     L = m2s._lib.lib()
     saved = L.m2s_query_budget()
     try:  # a small budget sends many lanes of each warp to the hard pass
