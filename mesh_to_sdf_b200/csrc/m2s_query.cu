@@ -852,6 +852,7 @@ uint32_t g_query_budget = 768;
 // 600k queries; 1M star points 8.0 -> 7.1 ms, 4M terrain points 15.2 -> 10.7 ms;
 // 100k star points 2.4 -> 2.9 ms).
 constexpr uint64_t kPacketMinQueries = 1u << 19;
+constexpr uint64_t kMortonMinQueries = 1u << 17;  // batch size from which queries run in Morton order
 
 namespace {
 // Order-preserving int image of a float (for atomic min / max).
@@ -993,11 +994,19 @@ int query_points(const MeshView& m, int accel, int sign, const float* d_q, uint6
   if (accel == M2S_ACCEL_NONE && !d_vec) return brute_force_sdf(m, sign, d_q, nq, d_out, d_status, s);
   if (m.n_tris == 0) return M2S_ERR_EMPTY_MESH;
   if (nq > 0xFFFFFFFFull) return M2S_ERR_INVALID_ARGUMENT;
-  // Morton-ordered launch for large batches.
+  const int mode = d_vec ? Q_VECTOR
+                         : (accel == M2S_ACCEL_RTREE
+                                ? Q_RTREE
+                                : ((accel == M2S_ACCEL_BVH && sign == M2S_SIGN_NORMAL) ? Q_BVH_NORMAL : Q_BVH_RAYCAST));
+  // Morton-ordered launch for large batches: from 2^17 queries (below, the
+  // sort's launches cost more than coherent warps save: 10k RtreeBvh points
+  // on icosphere s3 0.33 -> 0.21 ms unsorted, star s6 50k 1.84 -> 1.65 ms; at
+  // 200k sorting wins, 3.75 -> 3.20 ms), and from 4096 for Bvh(Normal), whose
+  // packet search needs the order.
   DevBuf<uint32_t> keys, order;
   const uint32_t* ord = nullptr;
   int st;
-  if (nq >= 4096) {
+  if (nq >= (mode == Q_BVH_NORMAL ? 4096u : kMortonMinQueries)) {
     if ((st = keys.alloc(nq, s)) || (st = order.alloc(nq, s))) return st;
     k_query_keys<<<(unsigned)((nq + 255) / 256), 256, 0, s>>>(d_q, nq, m, keys.p, order.p);
     M2S_CUDA(cudaGetLastError());
@@ -1005,10 +1014,6 @@ int query_points(const MeshView& m, int accel, int sign, const float* d_q, uint6
     ord = order.p;
   }
   unsigned blocks = (unsigned)((nq + 127) / 128);
-  int mode = d_vec ? Q_VECTOR
-                   : (accel == M2S_ACCEL_RTREE ? Q_RTREE
-                                               : ((accel == M2S_ACCEL_BVH && sign == M2S_SIGN_NORMAL) ? Q_BVH_NORMAL
-                                                                                                      : Q_BVH_RAYCAST));
   // Queries over the node budget continue one warp per query.
   DevBuf<HardQuery> hard;
   DevBuf<uint32_t> hard_count;

@@ -204,11 +204,14 @@ def test_vector_query_matches_oracle(orc):
 
 
 def test_large_batch_morton_order(orc):
-    # >= 4096 queries take the Morton-sorted launch; results stay in input order
+    # from 2^17 queries the per-thread search runs in Morton order (Bvh(Normal)
+    # from 4096); results stay in input order, and an unsorted 20k batch agrees
     v, idx = synth.star(5, seed=2)
-    q = synth.mixed_points(v, idx, 20000, seed=4)
-    for am in (A.bvh(S.Raycast), A.rtree(), A.rtree_bvh()):
-        assert_bit_equal(m2s.generate_sdf(v, T.TriangleList(idx), q, am), orc_sdf(orc, v, idx, q, am), repr(am))
+    q = synth.mixed_points(v, idx, (1 << 17) + 500, seed=4)
+    for n in (20000, len(q)):
+        for am in (A.bvh(S.Raycast), A.rtree(), A.rtree_bvh(), A.bvh(S.Normal)):
+            assert_bit_equal(m2s.generate_sdf(v, T.TriangleList(idx), q[:n], am), orc_sdf(orc, v, idx, q[:n], am),
+                             f"{am!r} {n}")
 
 
 def test_packet_search_bit_exact(orc):
