@@ -4,7 +4,7 @@
 //    every triangle.  Triangle tiles are staged in shared memory by the bulk
 //    copy engine (cp.async.bulk + mbarrier, double-buffered); each thread owns
 //    one query and folds the tile in triangle order, exactly the reference's
-//    fold order; batches of 4096 queries or more are visited in Morton order.
+//    fold order; batches of 2^28 pairs or more are visited in Morton order.
 //    Normal batches of fewer than 2^17 queries take k_brute_normal_warp: a
 //    warp per query, the same fold in the same order.
 //  * Bvh(Raycast) / RtreeBvh (bvh.rs:256-332, rtree_bvh.rs:143-201): exact
@@ -148,6 +148,7 @@ __global__ void k_brute_finish(const uint2* __restrict__ part, uint64_t nq, floa
 // evaluated at a time, so a batch of few queries still fills the GPU.
 constexpr int kBwThreads = 256;                 // 8 queries per block
 constexpr uint64_t kBruteWarpMaxQueries = 1u << 17;  // below: one warp per query
+constexpr uint64_t kBruteSortMinPairs = 1ull << 28;  // from here the thread kernels visit queries in Morton order
 __global__ void __launch_bounds__(kBwThreads) k_brute_normal_warp(const TriRec* __restrict__ tris, uint32_t T,
                                                                   const float* __restrict__ q, uint64_t nq,
                                                                   float* __restrict__ out, uint32_t* status) {
@@ -905,7 +906,9 @@ int brute_force_sdf(const MeshView& m, int sign, const float* d_q, uint64_t nq, 
                     cudaStream_t s, bool allow_alloc) {
   if (nq == 0) return M2S_OK;
   unsigned blocks = (unsigned)((nq + kBfThreads - 1) / kBfThreads);
-  // Thread-per-query kernels visit large batches in Morton order (of the
+  // Thread-per-query kernels visit large batches (2^28 pairs or more: the
+  // sort's ~20 launches take ~0.1 ms, the order saves ~13 % of the kernel)
+  // in Morton order (of the
   // queries' own bounding box): the lanes of a warp then mostly fall in the
   // same Voronoi regions of a triangle and take the same branches (65,536
   // points x 81,920 triangles Raycast 24.3 -> 21.2 ms, 262,144 Normal 108.5
@@ -914,7 +917,7 @@ int brute_force_sdf(const MeshView& m, int sign, const float* d_q, uint64_t nq, 
   DevBuf<int> bounds;
   const uint32_t* ord = nullptr;
   const bool thread_kernel = sign == M2S_SIGN_RAYCAST || nq >= kBruteWarpMaxQueries;
-  if (allow_alloc && thread_kernel && nq >= 4096 && nq <= 0xFFFFFFFFull) {
+  if (allow_alloc && thread_kernel && nq >= 4096 && nq <= 0xFFFFFFFFull && nq * m.n_tris >= kBruteSortMinPairs) {
     int st;
     if ((st = keys.alloc(nq, s)) || (st = order.alloc(nq, s)) || (st = bounds.alloc(6, s))) return st;
     k_bf_bounds_init<<<1, 32, 0, s>>>(bounds.p);

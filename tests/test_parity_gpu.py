@@ -245,10 +245,16 @@ def test_packet_search_bit_exact(orc):
 
 
 def test_brute_force_morton_order(orc):
-    # None visits batches of 4096 or more queries in Morton order (Raycast:
-    # chunked over triangles too); results stay in input order, bit-exact
-    v, idx = synth.star(3, seed=6)
-    q = synth.mixed_points(v, idx, 6001, seed=12)
+    # None visits batches of 2^28 (query, triangle) pairs or more in Morton
+    # order (Raycast: chunked over triangles too; Normal here on one warp per
+    # query); results stay in input order, bit-exact
+    v, idx = synth.star(5, seed=6)
+    q = synth.mixed_points(v, idx, 13200, seed=12)
+    assert len(q) * (len(idx) // 3) >= 1 << 28
+    v4, i4 = synth.star(4, seed=7)  # Normal on the thread kernel, sorted: 2^17+ queries, 2^28+ pairs
+    q4 = synth.mixed_points(v4, i4, (1 << 17) + 100, seed=13)
+    assert_bit_equal(m2s.generate_sdf(v4, T.TriangleList(i4), q4, A.none(S.Normal)),
+                     orc_sdf(orc, v4, i4, q4, A.none(S.Normal)), "Normal, thread kernel")
     for am in (A.none(S.Raycast), A.none(S.Normal)):
         assert_bit_equal(m2s.generate_sdf(v, T.TriangleList(idx), q, am), orc_sdf(orc, v, idx, q, am), repr(am))
 
