@@ -193,7 +193,7 @@ int m2s_grid_sdf_batch_device(const m2s_mesh* const* meshes, uint32_t n_grids, c
   }
   uint64_t stats[kGridStats] = {};
   st = grid_sdf_batch(views.data(), n_grids, grids.data(), sign, d_out, d_status, s, stats, grid_phase_slot(),
-                      g_grid_tuning);
+                      grid_tuning());
   record_grid_stats(stats);
   return st;
 }
@@ -225,7 +225,7 @@ int m2s_grid_plan_create(const m2s_mesh* const* meshes, uint32_t n_grids, const 
     cudaStreamDestroy(own);
     return code;
   };
-  if ((st = prepare_waves(views.data(), n_grids, grids.data(), sign, d_out, d_status, P->own, g_grid_tuning,
+  if ((st = prepare_waves(views.data(), n_grids, grids.data(), sign, d_out, d_status, P->own, grid_tuning(),
                           &P->jobs)))
     return fail(st);
   for (auto& j : P->jobs) {
@@ -342,10 +342,12 @@ void m2s_grid_plan_free(m2s_grid_plan* plan) {
 }
 
 void m2s_set_grid_tuning(int blocks_per_sm, uint32_t cells_per_block, uint64_t wave_cells, int solo_max) {
-  g_grid_tuning.blocks_per_sm = blocks_per_sm > 0 ? blocks_per_sm : 0;
-  g_grid_tuning.cells_per_block = cells_per_block ? cells_per_block : 1024;
-  g_grid_tuning.wave_cells = wave_cells ? wave_cells : (1ull << 26);
-  g_grid_tuning.solo_max = solo_max < 0 ? 64u : (uint32_t)solo_max;
+  GridTuning t = grid_tuning();
+  t.blocks_per_sm = blocks_per_sm > 0 ? blocks_per_sm : 0;
+  t.cells_per_block = cells_per_block ? cells_per_block : 1024;
+  t.wave_cells = wave_cells ? wave_cells : (1ull << 26);
+  t.solo_max = solo_max < 0 ? 64u : (uint32_t)solo_max;
+  set_grid_tuning(t);
 }
 
 void m2s_clear_grid_autotune(void) {

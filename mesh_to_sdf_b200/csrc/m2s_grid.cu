@@ -42,6 +42,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <vector>
 
 #include "m2s_internal.cuh"
@@ -1724,12 +1725,25 @@ int grid_sdf_batch(const MeshView* meshes, uint32_t n, const GridDesc* gds, int 
   return M2S_OK;
 }
 
+namespace {
+std::mutex g_grid_tuning_mu;
 GridTuning g_grid_tuning;
+}  // namespace
+
+GridTuning grid_tuning() {
+  std::lock_guard<std::mutex> lk(g_grid_tuning_mu);
+  return g_grid_tuning;
+}
+
+void set_grid_tuning(const GridTuning& t) {
+  std::lock_guard<std::mutex> lk(g_grid_tuning_mu);
+  g_grid_tuning = t;
+}
 
 int grid_sdf(const MeshView& m, const GridDesc& gd, int sign, float* d_out, uint32_t* d_status, cudaStream_t s,
              uint64_t stats[kGridStats], float phase_ms[4]) {
   if (gd.cells() == 0) return M2S_OK;
-  return grid_sdf_batch(&m, 1, &gd, sign, d_out, d_status, s, stats, phase_ms, g_grid_tuning);
+  return grid_sdf_batch(&m, 1, &gd, sign, d_out, d_status, s, stats, phase_ms, grid_tuning());
 }
 
 }  // namespace m2s

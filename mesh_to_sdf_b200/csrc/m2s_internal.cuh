@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <cmath>
 #include <memory>
@@ -126,7 +127,7 @@ int query_points(const MeshView& m, int accel, int sign, const float* d_q, uint6
 
 // Node visits a query may spend in the one-thread-per-query pass before it is
 // continued one warp per query (0 disables the second pass).
-extern uint32_t g_query_budget;
+extern std::atomic<uint32_t> g_query_budget;
 // The budget a batch of nq queries uses: `base` from 2^20 queries up, and
 // base * sqrt(nq / 2^20), at least 64, below (0 stays 0: no warp pass).
 inline uint32_t effective_query_budget(uint32_t base, uint64_t nq) {
@@ -257,8 +258,10 @@ int check_grid(const GridDesc& g);
 uint32_t default_list_capacity(uint64_t cells);
 uint64_t grid_job_bytes(uint64_t cells);
 
-// Process-wide grid knobs (m2s_set_grid_tuning).
-extern GridTuning g_grid_tuning;
+// Process-wide grid knobs (m2s_set_grid_tuning), read as a copy under a lock:
+// a caller may change them while other threads (the server's) run grids.
+GridTuning grid_tuning();
+void set_grid_tuning(const GridTuning& t);
 
 // ---- host API helpers (m2s_api.cu) -------------------------------------------
 

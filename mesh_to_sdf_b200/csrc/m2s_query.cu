@@ -846,7 +846,7 @@ __global__ void k_query_keys(const float* __restrict__ q, uint64_t nq, MeshView 
 }  // namespace
 
 // Node-visit budget of the single-thread search (0: single pass only).
-uint32_t g_query_budget = 768;
+std::atomic<uint32_t> g_query_budget{768};
 
 // Batch size from which Raycast, Rtree and vector queries search a warp at a
 // time (measured crossover: star s6 and the 512^2 terrain are even at 400k to
@@ -1020,14 +1020,15 @@ int query_points(const MeshView& m, int accel, int sign, const float* d_q, uint6
   // Queries over the node budget continue one warp per query.
   DevBuf<HardQuery> hard;
   DevBuf<uint32_t> hard_count;
-  const bool two_pass = mode != Q_BVH_NORMAL && g_query_budget > 0;
+  const uint32_t base_budget = g_query_budget.load(std::memory_order_relaxed);
+  const bool two_pass = mode != Q_BVH_NORMAL && base_budget > 0;
   if (two_pass) {
     if ((st = hard.alloc(nq, s)) || (st = hard_count.alloc(1, s))) return st;
     M2S_CUDA(cudaMemsetAsync(hard_count.p, 0, 4, s));
   }
   // Smaller batches hand long searches to the warp pass sooner: their time is
   // the longest single-thread search, not the throughput of many.
-  const uint32_t budget = effective_query_budget(g_query_budget, nq);
+  const uint32_t budget = effective_query_budget(base_budget, nq);
   HardQuery* hp = two_pass ? hard.p : nullptr;
   uint32_t* hc = two_pass ? hard_count.p : nullptr;
   // With profiling on, the counting instantiations run and their totals are

@@ -345,7 +345,7 @@ void m2s_server::grid_loop() {
     std::vector<RequestP> batch;
     std::vector<MeshView> views;
     // Serving keeps waves small: a wave's requests complete together.
-    GridTuning tune = g_grid_tuning;
+    GridTuning tune = grid_tuning();
     tune.wave_cells = std::min<uint64_t>(tune.wave_cells ? tune.wave_cells : kServeWaveCells, kServeWaveCells);
     if (tune.blocks_per_sm <= 0) tune.blocks_per_sm = kServeBlocksPerSm;
     const uint64_t wave_cells = tune.wave_cells;
