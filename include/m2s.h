@@ -324,8 +324,10 @@ int m2s_last_grid_phase_ms(float out[4]);
  * copying up to `capacity` steps (2 * capacity words) to `out` (may be NULL). */
 uint32_t m2s_last_grid_round_log(uint32_t* out, uint32_t capacity);
 
-/* Point queries run one thread per query; a query that visits more than its
- * node budget is continued by a whole warp (points deep inside a closed mesh
+/* Point queries run one thread per query (from 2^19 queries the 32 queries of
+ * a warp walk the tree together, the budget still counted per query); a
+ * query that visits more than its node budget is continued by a whole warp
+ * (points deep inside a closed mesh
  * see most triangles at nearly the same distance).  `node_visits` is the
  * budget of batches of 2^20 queries and more; a smaller batch of nq queries
  * uses node_visits * sqrt(nq / 2^20), at least 64, since its time is its
