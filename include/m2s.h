@@ -40,7 +40,7 @@ enum m2s_status {
   M2S_ERR_INDEX_COUNT = 3,     /* lib.rs:203, lib.rs:207 list length % 3 != 0 */
   M2S_ERR_INDEX_RANGE = 4,     /* slice indexing panic (test at lib.rs:557-566) */
   M2S_ERR_NAN_DISTANCE = 5,    /* lib.rs:330 expect("NaN distance") */
-  M2S_ERR_EMPTY_MESH = 6,      /* rtree.rs:317 nearest.unwrap() on an empty tree */
+  M2S_ERR_EMPTY_MESH = 6,      /* rtree.rs:148 nearest.unwrap() on an empty tree */
   M2S_ERR_CUDA = 7,
   M2S_ERR_OUT_OF_MEMORY = 8,
   M2S_ERR_LIMIT = 9, /* a bounded device loop (stack, worklist, rounds) hit its limit */
@@ -64,7 +64,7 @@ enum {                                              /* lib.rs:272-286 */
 typedef struct m2s_mesh m2s_mesh;
 
 /* generate_sdf (lib.rs:364-391).  `sign` is ignored for RTREE (always the
- * normal sign, rtree.rs:306-326) and RTREE_BVH (always the 3-ray vote,
+ * normal sign, rtree.rs:137-157) and RTREE_BVH (always the 3-ray vote,
  * rtree_bvh.rs:143-201).  out: n_queries floats. */
 int m2s_generate_sdf(const float* vertices, uint64_t n_vertices, const void* indices,
                      uint64_t n_indices, int index_bits, int topology, const float* query_points,
@@ -175,6 +175,13 @@ void m2s_clear_grid_autotune(void);
  * many states run on one block with block barriers only (0 = never, negative
  * = the default 64, at most 64). */
 void m2s_set_grid_tuning(int blocks_per_sm, uint32_t cells_per_block, uint64_t wave_cells, int solo_max);
+/* Process-wide (no counterpart in the reference): with enable != 0 (the
+ * default) grid propagation drops, before their closest-point evaluation, the
+ * proposals that a per-triangle distance bound (the triangle's plane and edge
+ * lines, with a slack far above f32 rounding) proves cannot beat the cell's
+ * value; 0 keeps only the same-triangle test.  Results are identical either
+ * way; the switch exists so that tests can show it. */
+void m2s_set_grid_bound_filter(int enable);
 
 /* generate_sdf with AccelerationMethod::None for callers that cannot allocate
  * device memory.  No counterpart in the reference: the crate allocates freely.
@@ -286,11 +293,15 @@ int m2s_radix_sort_pairs_device(uint32_t* d_keys, uint32_t* d_values, uint64_t n
 
 /* Diagnostics of the last grid call on this thread: [seed updates, relax
  * rounds, states relaxed, neighbour proposals (the on-grid cells of the 26
- * around each relaxed state; a Normal proposal to a cell that already holds
- * its triangle is counted but not evaluated), ray hits, propagation
+ * around each relaxed state; a proposal dropped unevaluated, see
+ * m2s_last_grid_filter_stats, is counted too), ray hits, propagation
  * restarts, kernel launches, far-list redistributions, rounds relaxed by one
  * block alone, largest bucket list relaxed in one round]. */
 int m2s_last_grid_stats(uint64_t out[10]);
+/* Of the neighbour proposals of the last grid call on this thread: [dropped
+ * because the neighbour already holds the proposing triangle, dropped by the
+ * distance bound (m2s_set_grid_bound_filter)]; the rest were evaluated. */
+int m2s_last_grid_filter_stats(uint64_t out[2]);
 
 /* When enabled (per thread), grid calls time their phases with CUDA events on
  * their stream — the points the crate logs at generate/grid.rs:303-307,

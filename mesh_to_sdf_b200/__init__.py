@@ -26,7 +26,7 @@ __all__ = [
     "SignMethod", "AccelerationMethod", "Topology", "Grid", "SnapResult", "SdfAccelerationMesh", "M2SError",
     "generate_sdf", "generate_grid_sdf", "build_sdf_acceleration", "query_sdf",
     "query_vector_to_closest_point_rtree_bvh", "ALL_SDF_ACCELERATION_METHODS", "device_available",
-    "grid_sdf_batch_device", "GridPlan", "grid_offsets", "set_grid_tuning", "clear_grid_autotune", "Server",
+    "grid_sdf_batch_device", "GridPlan", "grid_offsets", "set_grid_tuning", "set_grid_bound_filter", "clear_grid_autotune", "Server",
     "sort_cells_by_distance", "sort_cells_by_distance_device", "check_mesh_triangle_list",
 ]
 
@@ -282,10 +282,26 @@ GRID_STATS = ("seed_updates", "rounds", "states_relaxed", "neighbour_evals", "ra
 
 
 def last_grid_stats():
-    """Counters of the last grid call on this thread (names in GRID_STATS)."""
+    """Counters of the last grid call on this thread (names in GRID_STATS),
+    plus how many neighbour proposals were dropped unevaluated: `dropped_same`
+    (the neighbour held the proposing triangle) and `dropped_bound` (the
+    distance bound proved they cannot win)."""
+    L = _lib.lib()
     a = np.zeros(len(GRID_STATS), np.uint64)
-    _lib.lib().m2s_last_grid_stats(_vp(a))
-    return dict(zip(GRID_STATS, (int(x) for x in a)))
+    L.m2s_last_grid_stats(_vp(a))
+    d = dict(zip(GRID_STATS, (int(x) for x in a)))
+    f = np.zeros(2, np.uint64)
+    L.m2s_last_grid_filter_stats(_vp(f))
+    d["dropped_same"], d["dropped_bound"] = int(f[0]), int(f[1])
+    return d
+
+
+def set_grid_bound_filter(enable: bool):
+    """Process-wide: drop grid-propagation proposals that a per-triangle
+    distance bound proves cannot win (the default), or evaluate every proposal
+    but those to a cell already holding the proposing triangle.  Results are
+    identical either way."""
+    _lib.lib().m2s_set_grid_bound_filter(1 if enable else 0)
 
 
 QUERY_STATS = ("queries", "search_node_fetches", "search_triangle_tests", "sign_node_fetches", "sign_triangle_tests")

@@ -40,6 +40,8 @@ SIGNATURES = {
     "m2s_grid_plan_free": (None, [P]),
     "m2s_clear_grid_autotune": (None, []),
     "m2s_set_grid_tuning": (None, [I, ctypes.c_uint32, U64, I]),
+    "m2s_set_grid_bound_filter": (None, [I]),
+    "m2s_last_grid_filter_stats": (I, [P]),
     "m2s_grid_plan_waves": (ctypes.c_uint32, [P]),
     "m2s_radix_sort_pairs_device": (I, [P, P, U64, I, P]),
     "m2s_sort_cells_by_distance_device": (I, [P, U64, P, P, P]),

@@ -251,7 +251,14 @@ uint32_t m2s_query_budget(void) { return g_query_budget; }
 
 int m2s_last_grid_stats(uint64_t out[10]) {
   if (!out) return M2S_ERR_INVALID_ARGUMENT;
-  for (int i = 0; i < kGridStats; ++i) out[i] = t_grid_stats[i];
+  for (int i = 0; i < 10; ++i) out[i] = t_grid_stats[i];
+  return M2S_OK;
+}
+
+int m2s_last_grid_filter_stats(uint64_t out[2]) {
+  if (!out) return M2S_ERR_INVALID_ARGUMENT;
+  out[0] = t_grid_stats[10];
+  out[1] = t_grid_stats[11];
   return M2S_OK;
 }
 

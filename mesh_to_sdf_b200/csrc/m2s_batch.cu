@@ -145,6 +145,8 @@ struct m2s_grid_plan {
         sum[7] += info.far_phases;
         sum[8] += info.solo_rounds;
         sum[9] = std::max<uint64_t>(sum[9], info.max_list);
+        sum[10] += info.filter_same;
+        sum[11] += info.filter_bound;
         if (!info.overflow) continue;
         if (attempt >= 6 || j->capacity() >= 0x40000000u) {
           set_error("grid propagation lists overflowed at the largest capacity");
@@ -347,6 +349,12 @@ void m2s_set_grid_tuning(int blocks_per_sm, uint32_t cells_per_block, uint64_t w
   t.cells_per_block = cells_per_block ? cells_per_block : 1024;
   t.wave_cells = wave_cells ? wave_cells : (1ull << 26);
   t.solo_max = solo_max < 0 ? 64u : (uint32_t)solo_max;
+  set_grid_tuning(t);
+}
+
+void m2s_set_grid_bound_filter(int enable) {
+  GridTuning t = grid_tuning();
+  t.bound_filter = enable != 0;
   set_grid_tuning(t);
 }
 

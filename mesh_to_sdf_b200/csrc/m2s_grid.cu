@@ -180,6 +180,8 @@ struct PropState {
   uint32_t log_n;         // steps recorded in the round log
   uint32_t solo_rounds;   // rounds relaxed by block 0 alone
   unsigned long long entries, evals, seeds, ray_hits;
+  unsigned long long filter_same;   // proposals dropped: the neighbour holds the proposing triangle
+  unsigned long long filter_bound;  // proposals dropped by the distance bound
 };
 
 __device__ __forceinline__ P3 center(const GridK& g, int x, int y, int z) {
@@ -266,6 +268,92 @@ __device__ __forceinline__ bool update_min(unsigned long long* slot, unsigned lo
     old = prev;
   }
   return false;
+}
+
+// ---- the propagation's proposal filter -------------------------------------
+// Most proposals cannot win (on the star s6 256^3 grid under 5 % beat the
+// snapshot), and a proposal's closest-point evaluation is most of its cost.
+// A triangle lies in its plane and, inside that plane, on the inner side of
+// each of its three edge lines, so the distance from p to the triangle is at
+// least sqrt(h^2 + o^2), where h is p's distance to the plane and o the
+// largest distance of p's projection outside an edge line.  A proposal whose
+// bound already exceeds the snapshot's distance by a slack far above the
+// rounding of both computations cannot beat the snapshot (for Normal: not
+// even enter compare_distances' tie band), so it is dropped unevaluated.
+// Results are unchanged; the filter only skips work whose outcome is known.
+//
+// TriBound: n = unit normal, n.w = n . a; e0, e1, e2 = unit in-plane normals
+// of the edges ab, bc, ca pointing into the triangle, .w = e . (the edge's
+// first vertex).  Built in double from the exact f32 vertices.
+struct __align__(16) TriBound {
+  float4 n, e0, e1, e2;
+};
+// Slack of the test, relative to the snapshot distance and per unit of the
+// largest coordinate magnitude involved (the point's and the triangle's: the
+// f32 closest-point arithmetic errs by a few ulps of these; the slack is
+// about a thousand times that).
+constexpr float kBoundRel = 1.0f / 65536.0f;
+constexpr double kBoundAbs = 1.0 / 16384.0;
+// Triangles whose area is tiny against their longest edge (slivers: the
+// reference's region tests lose accuracy there) and degenerate ones are never
+// filtered: their record is zero and their slack infinite.
+constexpr double kBoundMinShape = 1e-4;
+
+__global__ void k_bounds(const TriRec* __restrict__ tris, uint32_t T, TriBound* __restrict__ out,
+                         float* __restrict__ slack) {
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
+    const TriRec r = tris[t];
+    const double ax = r.a.x, ay = r.a.y, az = r.a.z, bx = r.b.x, by = r.b.y, bz = r.b.z;
+    const double cx = r.c.x, cy = r.c.y, cz = r.c.z;
+    const double abx = bx - ax, aby = by - ay, abz = bz - az, acx = cx - ax, acy = cy - ay, acz = cz - az;
+    const double bcx = cx - bx, bcy = cy - by, bcz = cz - bz;
+    const double nx = aby * acz - abz * acy, ny = abz * acx - abx * acz, nz = abx * acy - aby * acx;
+    const double nn = sqrt(nx * nx + ny * ny + nz * nz);
+    const double lab = sqrt(abx * abx + aby * aby + abz * abz), lac = sqrt(acx * acx + acy * acy + acz * acz);
+    const double lbc = sqrt(bcx * bcx + bcy * bcy + bcz * bcz);
+    const double emax = fmax(lab, fmax(lac, lbc));
+    const double vmax = fmax(fmax(fmax(fabs(ax), fabs(ay)), fmax(fabs(az), fabs(bx))),
+                             fmax(fmax(fabs(by), fabs(bz)), fmax(fmax(fabs(cx), fabs(cy)), fabs(cz))));
+    const double scale = vmax + emax;
+    const bool ok = __float_as_int(r.a.w) == 0 && isfinite(scale) && scale < 1e18 && emax > 0.0 &&
+                    nn > kBoundMinShape * emax * emax;
+    if (!ok) {
+      const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+      out[t] = TriBound{z, z, z, z};
+      slack[t] = __int_as_float(0x7F800000);  // +inf: never filtered
+      continue;
+    }
+    const double ux = nx / nn, uy = ny / nn, uz = nz / nn;
+    // In-plane normal of edge (p, q) toward the third vertex: u x (q - p) / |q - p|
+    // (u = ab x ac / |ab x ac|, so u x ab points from ab toward c, and so on).
+    auto edge = [&](double px, double py, double pz, double dx, double dy, double dz, double len) {
+      const double mx = (uy * dz - uz * dy) / len, my = (uz * dx - ux * dz) / len, mz = (ux * dy - uy * dx) / len;
+      return make_float4((float)mx, (float)my, (float)mz, (float)(mx * px + my * py + mz * pz));
+    };
+    TriBound b;
+    b.n = make_float4((float)ux, (float)uy, (float)uz, (float)(ux * ax + uy * ay + uz * az));
+    b.e0 = edge(ax, ay, az, abx, aby, abz, lab);
+    b.e1 = edge(bx, by, bz, bcx, bcy, bcz, lbc);
+    b.e2 = edge(cx, cy, cz, -acx, -acy, -acz, lac);
+    out[t] = b;
+    slack[t] = (float)(kBoundAbs * scale);
+  }
+}
+
+// True when triangle `tb` (slack `sl`) provably cannot beat the snapshot key
+// at the cell centre p.
+template <int SIGN>
+__device__ __forceinline__ bool bound_rejects(const TriBound& tb, float sl, P3 p, unsigned long long snap) {
+  const float h = fmaf(tb.n.x, p.x, fmaf(tb.n.y, p.y, fmaf(tb.n.z, p.z, -tb.n.w)));
+  const float s0 = fmaf(tb.e0.x, p.x, fmaf(tb.e0.y, p.y, fmaf(tb.e0.z, p.z, -tb.e0.w)));
+  const float s1 = fmaf(tb.e1.x, p.x, fmaf(tb.e1.y, p.y, fmaf(tb.e1.z, p.z, -tb.e1.w)));
+  const float s2 = fmaf(tb.e2.x, p.x, fmaf(tb.e2.y, p.y, fmaf(tb.e2.z, p.z, -tb.e2.w)));
+  const float o = fmaxf(0.0f, -fminf(s0, fminf(s1, s2)));
+  const float lb2 = fmaf(h, h, o * o);
+  const float pm = fmaxf(fabsf(p.x), fmaxf(fabsf(p.y), fabsf(p.z)));
+  float thr = fmaf(fabsf(key_dist(snap)), 1.0f + kBoundRel, fmaf((float)kBoundAbs, pm, sl));
+  if (SIGN == M2S_SIGN_NORMAL) thr += 1e-6f;  // compare_distances' absolute tie band (lib.rs:321)
+  return lb2 > thr * thr;                     // false when thr is infinite or anything is NaN
 }
 
 __global__ void k_fill_u64(unsigned long long* p, unsigned long long n, unsigned long long v) {
@@ -591,7 +679,8 @@ __device__ __forceinline__ bool solo_round(const Sched& sh, uint32_t solo_max) {
 // Queue of one warp's proposals that need a distance evaluation (Normal sign).
 constexpr uint32_t kQueue = 64;
 struct WarpQueue {
-  uint32_t tri[kQueue], j[kQueue], x[kQueue], y[kQueue], z[kQueue];
+  uint32_t tri[kQueue], j[kQueue];
+  float px[kQueue], py[kQueue], pz[kQueue];  // the neighbour's cell centre
   unsigned long long snap[kQueue];
 };
 constexpr int kWarps = 8;  // k_propagate runs 256 threads per block
@@ -629,14 +718,13 @@ __device__ __forceinline__ bool neighbour_cell(const GridSet& gs, uint2 ent, uin
   return true;
 }
 
-// Distance of triangle tri (record r) at cell (X, Y, Z) = j against the
+// Distance of triangle tri (record r) at cell j, centre pos, against the
 // cell's snapshot key; true when this proposal moved the cell off the
 // snapshot (it is then the cell's one staging proposal of the round).
-template <int SIGN, bool MULTI>
-__device__ __forceinline__ bool propose_at(const GridSet& gs, const TriRec& r, uint32_t tri, uint32_t j, int X, int Y,
-                                           int Z, unsigned long long snap, unsigned long long* work_keys, bool& nan) {
-  const GridK& g = grid_of_tri<MULTI>(gs, tri);
-  const float d = cell_distance<SIGN>(center(g, X, Y, Z), p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
+template <int SIGN>
+__device__ __forceinline__ bool propose_at(const TriRec& r, uint32_t tri, uint32_t j, P3 pos, unsigned long long snap,
+                                           unsigned long long* work_keys, bool& nan) {
+  const float d = cell_distance<SIGN>(pos, p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
   if (isnan(d)) nan = true;
   const unsigned long long cand = pack(d, tri);
   return beats<SIGN>(cand, snap, &nan) && improve_first<SIGN>(&work_keys[j], cand, snap, &nan);
@@ -691,7 +779,8 @@ template <int SIGN, bool MULTI>
 __device__ __forceinline__ void relax_propose_solo(const GridSet& gs, const TriRec* __restrict__ tris,
                                                    const unsigned long long* snap_keys, const uint2* list, uint32_t n,
                                                    uint32_t* HJ, unsigned long long* HK, uint16_t* taken,
-                                                   uint32_t* ntaken, bool& nan, unsigned long long& evals) {
+                                                   uint32_t* ntaken, bool& nan, unsigned long long& evals,
+                                                   uint32_t& dropped_same) {
   const uint32_t P = 26u * n;
   for (uint32_t p = threadIdx.x; p < P; p += blockDim.x) {
     const uint2 ent = __ldcg(&list[p / 26u]);  // written by other blocks in earlier rounds
@@ -701,7 +790,10 @@ __device__ __forceinline__ void relax_propose_solo(const GridSet& gs, const TriR
     ++evals;
     const unsigned long long snap = __ldcg(&snap_keys[j]);
     const TriRec r = tris[ent.y];
-    if (key_tri(snap) == ent.y) continue;
+    if (key_tri(snap) == ent.y) {
+      ++dropped_same;
+      continue;
+    }
     const GridK& g = grid_of_tri<MULTI>(gs, ent.y);
     const float d = cell_distance<SIGN>(center(g, X, Y, Z), p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
     if (isnan(d)) nan = true;
@@ -743,19 +835,24 @@ __device__ __forceinline__ void relax_commit_solo(const GridSet& gs, unsigned lo
 // consecutive threads share a state, so its entry and triangle loads are warp
 // broadcasts.
 //
-// Raycast: each thread evaluates its proposals, kUnroll at a time.  Normal:
-// a proposal whose neighbour already holds the same triangle cannot gain (the
-// distance of a (cell, triangle) pair is one deterministic value), and the
-// signed distance costs more, so the warp first filters its proposals and
-// queues the rest in shared memory, then evaluates them 32 at a time with
-// every lane busy.  Results do not depend on the order of proposals.
+// With the filter (the default), a proposal is dropped unevaluated when the
+// neighbour already holds the same triangle (the distance of a (cell,
+// triangle) pair is one deterministic value, so it cannot gain) or when the
+// triangle's distance bound proves it cannot beat the snapshot; each warp
+// queues the rest in shared memory and evaluates them 32 at a time with every
+// lane busy.  Without it, Raycast proposals are evaluated where they arise,
+// kUnroll per thread at a time, and Normal ones pass the same-triangle test
+// and the queue only.  Results do not depend on the filter or on the order of
+// proposals.
 template <int SIGN, bool MULTI>
 __device__ __forceinline__ void relax_propose(const GridSet& gs, const TriRec* __restrict__ tris,
-                                              const unsigned long long* snap_keys, unsigned long long* work_keys,
-                                              const uint2* list, uint32_t n, uint32_t T, uint32_t t0,
-                                              uint32_t* s_touch, uint32_t* s_ntouch, PropState* st, uint32_t parity,
-                                              uint32_t* spill, uint32_t cap, bool& nan, unsigned long long& evals,
-                                              WarpQueue* q) {
+                                              const TriBound* __restrict__ bounds, const float* __restrict__ slack,
+                                              bool filter, const unsigned long long* snap_keys,
+                                              unsigned long long* work_keys, const uint2* list, uint32_t n,
+                                              uint32_t T, uint32_t t0, uint32_t* s_touch, uint32_t* s_ntouch,
+                                              PropState* st, uint32_t parity, uint32_t* spill, uint32_t cap,
+                                              bool& nan, unsigned long long& evals, uint32_t& dropped_same,
+                                              uint32_t& dropped_bound, WarpQueue* q) {
   const uint32_t dE = T / 26u, dK = T % 26u;
   uint32_t e = t0 / 26u, k = t0 % 26u;
   // The neighbour of state e for proposal k: false when it lies off the grid.
@@ -763,11 +860,6 @@ __device__ __forceinline__ void relax_propose(const GridSet& gs, const TriRec* _
     const uint2 ent = __ldcg(&list[eu]);  // written by other blocks in earlier rounds
     tri = ent.y;
     return neighbour_cell<MULTI>(gs, ent, kk, j, X, Y, Z);
-  };
-  // Distance of triangle tri at cell (X, Y, Z) = j against its snapshot key;
-  // true when this proposal moved the cell off the snapshot.
-  auto evaluate = [&](uint32_t tri, uint32_t j, int X, int Y, int Z, unsigned long long snap) {
-    return propose_at<SIGN, MULTI>(gs, tris[tri], tri, j, X, Y, Z, snap, work_keys, nan);
   };
   auto step = [&]() {
     k += dK;
@@ -777,7 +869,7 @@ __device__ __forceinline__ void relax_propose(const GridSet& gs, const TriRec* _
       ++e;
     }
   };
-  if constexpr (SIGN == M2S_SIGN_RAYCAST) {
+  if (SIGN == M2S_SIGN_RAYCAST && !filter) {
     while (e < n) {
       bool first[kUnroll];
       uint32_t jj[kUnroll];
@@ -791,54 +883,64 @@ __device__ __forceinline__ void relax_propose(const GridSet& gs, const TriRec* _
         int X, Y, Z;
         if (eu >= n || !neighbour(eu, ku, tri, j, X, Y, Z)) continue;
         ++evals;
-        first[u] = evaluate(tri, j, X, Y, Z, __ldcg(&snap_keys[j]));
+        const P3 pos = center(grid_of_tri<MULTI>(gs, tri), X, Y, Z);
+        first[u] = propose_at<SIGN>(tris[tri], tri, j, pos, __ldcg(&snap_keys[j]), work_keys, nan);
         jj[u] = j;
       }
 #pragma unroll
       for (int u = 0; u < kUnroll; ++u)
         if (first[u]) stage_touch(jj[u], s_touch, s_ntouch, st, parity, spill, cap);
     }
-  } else {
-    const uint32_t lane = threadIdx.x & 31u;
-    uint32_t qn = 0;  // warp-uniform queue length, < 32 between iterations
-    auto run = [&](uint32_t i) {
-      if (evaluate(q->tri[i], q->j[i], (int)q->x[i], (int)q->y[i], (int)q->z[i], q->snap[i]))
-        stage_touch(q->j[i], s_touch, s_ntouch, st, parity, spill, cap);
-    };
-    while (__any_sync(0xFFFFFFFFu, e < n)) {
-      const uint32_t eu = e, ku = k;
-      step();
-      uint32_t tri = 0, j = 0;
-      int X = 0, Y = 0, Z = 0;
-      unsigned long long snap = 0;
-      bool keep = false;
-      if (eu < n && neighbour(eu, ku, tri, j, X, Y, Z)) {
-        ++evals;
-        snap = __ldcg(&snap_keys[j]);
-        keep = key_tri(snap) != tri;
-      }
-      const unsigned m = __ballot_sync(0xFFFFFFFFu, keep);
-      if (keep) {
-        const uint32_t w = qn + __popc(m & ((1u << lane) - 1u));  // qn + 31 at most
-        q->tri[w] = tri;
-        q->j[w] = j;
-        q->x[w] = (uint32_t)X;
-        q->y[w] = (uint32_t)Y;
-        q->z[w] = (uint32_t)Z;
-        q->snap[w] = snap;
-      }
-      qn += __popc(m);
-      if (qn >= 32u) {
-        __syncwarp();
-        run(qn - 32u + lane);
-        __syncwarp();  // the slots are written again next iteration
-        qn -= 32u;
+    return;
+  }
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t qn = 0;  // warp-uniform queue length, < 32 between iterations
+  auto run = [&](uint32_t i) {
+    const uint32_t tri = q->tri[i], j = q->j[i];
+    if (propose_at<SIGN>(tris[tri], tri, j, P3{q->px[i], q->py[i], q->pz[i]}, q->snap[i], work_keys, nan))
+      stage_touch(j, s_touch, s_ntouch, st, parity, spill, cap);
+  };
+  while (__any_sync(0xFFFFFFFFu, e < n)) {
+    const uint32_t eu = e, ku = k;
+    step();
+    uint32_t tri = 0, j = 0;
+    int X = 0, Y = 0, Z = 0;
+    P3 pos{0.f, 0.f, 0.f};
+    unsigned long long snap = 0;
+    bool keep = false;
+    if (eu < n && neighbour(eu, ku, tri, j, X, Y, Z)) {
+      ++evals;
+      snap = __ldcg(&snap_keys[j]);
+      pos = center(grid_of_tri<MULTI>(gs, tri), X, Y, Z);
+      if (key_tri(snap) == tri) {
+        ++dropped_same;
+      } else if (filter && bound_rejects<SIGN>(bounds[tri], slack[tri], pos, snap)) {
+        ++dropped_bound;
+      } else {
+        keep = true;
       }
     }
-    __syncwarp();
-    if (lane < qn) run(lane);
-    __syncwarp();
+    const unsigned m = __ballot_sync(0xFFFFFFFFu, keep);
+    if (keep) {
+      const uint32_t w = qn + __popc(m & ((1u << lane) - 1u));  // qn + 31 at most
+      q->tri[w] = tri;
+      q->j[w] = j;
+      q->px[w] = pos.x;
+      q->py[w] = pos.y;
+      q->pz[w] = pos.z;
+      q->snap[w] = snap;
+    }
+    qn += __popc(m);
+    if (qn >= 32u) {
+      __syncwarp();
+      run(qn - 32u + lane);
+      __syncwarp();  // the slots are written again next iteration
+      qn -= 32u;
+    }
   }
+  __syncwarp();
+  if (lane < qn) run(lane);
+  __syncwarp();
 }
 
 // Commit phase: publish each touched cell's round winner to the snapshot and
@@ -884,11 +986,12 @@ __global__ void __launch_bounds__(256, 4) k_propagate(const __grid_constant__ Gr
                                                    uint2* lists, uint32_t cap, uint32_t* spill_lists,
                                                    PropState* st, GridBarrier* bar, uint32_t max_steps,
                                                    uint32_t* status, uint32_t* round_log, uint32_t log_cap,
-                                                   uint32_t solo_max) {
+                                                   uint32_t solo_max, const TriBound* __restrict__ bounds,
+                                                   const float* __restrict__ slack, uint32_t filter) {
   __shared__ Sched sh;
   __shared__ __align__(16) uint32_t s_touch[kTouchStage];  // also a solo run's min table
   __shared__ uint16_t s_taken[26 * kSoloCap];              // a solo round's taken table slots
-  __shared__ WarpQueue s_queue[SIGN == M2S_SIGN_NORMAL ? kWarps : 1];
+  __shared__ WarpQueue s_queue[kWarps];
   __shared__ uint32_t s_ntouch, s_gen, s_pending, s_more, s_runs, s_solo_run;
   __shared__ uint32_t s_count[kLists], s_far_min[2], s_overflow;  // block 0's counters during a solo run
   // (built where used, so no pointer stays live across the propose loop)
@@ -915,6 +1018,7 @@ __global__ void __launch_bounds__(256, 4) k_propagate(const __grid_constant__ Gr
   }
   bool nan = false;
   unsigned long long evals = 0;
+  uint32_t dropped_same = 0, dropped_bound = 0;
   uint32_t far_phases = 0, logged = 0, max_list = 0, solo_rounds = 0;
   const uint64_t t_start = (lead_block && threadIdx.x == 0 && round_log) ? global_ns() : 0;
   bool aborted = false;
@@ -1056,11 +1160,11 @@ __global__ void __launch_bounds__(256, 4) k_propagate(const __grid_constant__ Gr
     unsigned long long* HK = reinterpret_cast<unsigned long long*>(s_touch + kHash);
     if (solo)
       relax_propose_solo<SIGN, MULTI>(gs, tris, snap_keys, lists + (unsigned long long)sh.cur * cap, n, HJ, HK,
-                                      s_taken, &s_ntouch, nan, evals);
+                                      s_taken, &s_ntouch, nan, evals, dropped_same);
     else
-      relax_propose<SIGN, MULTI>(gs, tris, snap_keys, work_keys, lists + (unsigned long long)sh.cur * cap, n, T, t0,
-                                 s_touch, &s_ntouch, st, parity, spill, cap, nan, evals,
-                                 &s_queue[SIGN == M2S_SIGN_NORMAL ? threadIdx.x >> 5 : 0]);
+      relax_propose<SIGN, MULTI>(gs, tris, bounds, slack, filter != 0u, snap_keys, work_keys,
+                                 lists + (unsigned long long)sh.cur * cap, n, T, t0, s_touch, &s_ntouch, st, parity,
+                                 spill, cap, nan, evals, dropped_same, dropped_bound, &s_queue[threadIdx.x >> 5]);
     if (lead_block && threadIdx.x == 0) atomicAdd(&st->entries, (unsigned long long)n);
     if (solo) {
       __syncthreads();
@@ -1119,6 +1223,13 @@ __global__ void __launch_bounds__(256, 4) k_propagate(const __grid_constant__ Gr
   if (nan) atomicOr(status, bit(M2S_ERR_NAN_DISTANCE));
   for (int o = 16; o; o >>= 1) evals += __shfl_xor_sync(0xFFFFFFFFu, evals, o);
   if (lane == 0 && evals) atomicAdd(&st->evals, evals);
+  unsigned long long ds = dropped_same, db = dropped_bound;
+  for (int o = 16; o; o >>= 1) {
+    ds += __shfl_xor_sync(0xFFFFFFFFu, ds, o);
+    db += __shfl_xor_sync(0xFFFFFFFFu, db, o);
+  }
+  if (lane == 0 && ds) atomicAdd(&st->filter_same, ds);
+  if (lane == 0 && db) atomicAdd(&st->filter_bound, db);
   if (aborted && lead_block && threadIdx.x == 0) atomicOr(status, bit(M2S_ERR_LIMIT));
   if (lead_block && threadIdx.x == 0) {
     st->round = sh.round;
@@ -1305,6 +1416,9 @@ struct GridJob::Impl {
   DevBuf<uint2> lists;
   DevBuf<uint32_t> touched;
   DevBuf<uint32_t> round_log;  // profiling only
+  DevBuf<TriBound> bounds;     // the proposal filter's per-triangle records
+  DevBuf<float> slack;
+  bool filter = true;
 };
 
 GridJob::GridJob() : p(new Impl) {}
@@ -1328,6 +1442,7 @@ uint32_t GridJob::grids() const { return p->gs.ngrids; }
 uint64_t GridJob::device_bytes() const {
   const Impl& J = *p;
   return J.comb_tris.n * sizeof(TriRec) + J.tri_grid.n * 4 + (J.snap.n + J.work.n) * 8 + J.bits.n * 4 +
+         J.bounds.n * sizeof(TriBound) + J.slack.n * 4 +
          (uint64_t)kLists * J.cap * 8 + 2ull * J.cap * 4 + J.table.n * sizeof(GridK);
 }
 
@@ -1339,7 +1454,7 @@ uint32_t default_list_capacity(uint64_t cells) {
 uint64_t grid_job_bytes(uint64_t cells) {
   const uint64_t cap = default_list_capacity(cells);
   const uint64_t ray_words = 3 * (cells / 32 + 3 * std::cbrt((double)cells) * std::cbrt((double)cells));
-  return 16 * cells + (uint64_t)kLists * 8 * cap + 8 * cap + 4 * ray_words + (1u << 20);
+  return 16 * cells + (uint64_t)kLists * 8 * cap + 8 * cap + 4 * ray_words + (1u << 20);  // + 68 B per triangle
 }
 
 int check_grid(const GridDesc& g) {
@@ -1444,6 +1559,8 @@ int GridJob::prepare(const MeshView* meshes, uint32_t n, const GridDesc* gds, in
   if ((st = J.snap.alloc(N, s)) || (st = J.work.alloc(N, s)) || (st = J.state.alloc(1, s)) ||
       (st = J.bar.alloc(1, s)))
     return st;
+  J.filter = tune.bound_filter;
+  if (tris && ((st = J.bounds.alloc(tris, s)) || (st = J.slack.alloc(tris, s)))) return st;
   if (sign == M2S_SIGN_RAYCAST && (st = J.bits.alloc(woff, s))) return st;
   J.cap = tune.list_capacity ? tune.list_capacity : default_list_capacity(N);
   J.solo_max = std::min<uint32_t>(tune.solo_max, kSoloCap);  // a solo round never spills
@@ -1511,6 +1628,10 @@ int GridJob::enqueue(cudaStream_t s, cudaEvent_t* ev) {
   if (J.T > 0) {
     M2S_CUDA(cudaMemsetAsync(J.bar.p, 0, sizeof(GridBarrier), s));
     M2S_CUDA(cudaMemcpyAsync(J.work.p, J.snap.p, N * 8, cudaMemcpyDeviceToDevice, s));
+    if (J.filter) {
+      k_bounds<<<blocks_for(J.T, 256), 256, 0, s>>>(J.tris, J.T, J.bounds.p, J.slack.p);
+      ++J.launches;
+    }
     if (multi) k_collect<true><<<blocks_for(N, 256), 256, 0, s>>>(J.gs, J.snap.p, J.state.p, J.lists.p, J.cap);
     else k_collect<false><<<blocks_for(N, 256), 256, 0, s>>>(J.gs, J.snap.p, J.state.p, J.lists.p, J.cap);
     M2S_CUDA(cudaGetLastError());
@@ -1519,8 +1640,10 @@ int GridJob::enqueue(cudaStream_t s, cudaEvent_t* ev) {
     const TriRec* tris = J.tris;
     uint32_t* log = J.round_log.p;
     uint32_t log_cap = (uint32_t)(J.round_log.n / 2);
+    uint32_t filter = J.filter ? 1u : 0u;
     void* args[] = {&J.gs,     &tris,   &J.snap.p,  &J.work.p,    &J.lists.p, &J.cap,     &J.touched.p,
-                    &J.state.p, &J.bar.p, &max_steps, &J.d_status, &log,       &log_cap, &J.solo_max};
+                    &J.state.p, &J.bar.p, &max_steps, &J.d_status, &log,       &log_cap, &J.solo_max,
+                    &J.bounds.p, &J.slack.p, &filter};
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(J.coop_blocks);
     cfg.blockDim = dim3(256);
@@ -1586,6 +1709,8 @@ int GridJob::read_state(cudaStream_t s, GridRunInfo* info) {
   info->solo_rounds = h->solo_rounds;
   info->max_list = h->max_list;
   info->log_n = h->log_n;
+  info->filter_same = h->filter_same;
+  info->filter_bound = h->filter_bound;
   info->launches = J.launches;
   return M2S_OK;
 }
@@ -1627,6 +1752,8 @@ int run_grid_job(GridJob& job, cudaStream_t s, uint64_t stats[kGridStats], float
     stats[7] = info.far_phases;
     stats[8] = info.solo_rounds;
     stats[9] = info.max_list;
+    stats[10] = info.filter_same;
+    stats[11] = info.filter_bound;
   }
   if (phase_ms) {
     for (int i = 0; i < 4; ++i) M2S_CUDA(cudaEventElapsedTime(&phase_ms[i], ev[i], ev[i + 1]));

@@ -168,9 +168,11 @@ struct GridDesc {
 
 // stats: [seed updates, relax rounds, states relaxed, neighbour proposals,
 // ray hits, overflow restarts, kernel launches, far-list redistributions,
-// rounds relaxed by one block alone, largest list relaxed in one round].  phase_ms (may be NULL) receives device time of
-// [seeding, propagation, rays, finalize].
-constexpr int kGridStats = 10;
+// rounds relaxed by one block alone, largest list relaxed in one round,
+// proposals dropped because the neighbour holds the proposing triangle,
+// proposals dropped by the distance bound].  phase_ms (may be NULL) receives
+// device time of [seeding, propagation, rays, finalize].
+constexpr int kGridStats = 12;
 int grid_sdf(const MeshView& m, const GridDesc& g, int sign, float* d_out, uint32_t* d_status, cudaStream_t s,
              uint64_t stats[kGridStats], float phase_ms[4]);
 
@@ -185,12 +187,15 @@ struct GridTuning {
   // Relax rounds of at most this many states run on one block, with block
   // barriers only (0: every round on every block).
   uint32_t solo_max = 64;
+  // Drop proposals that a per-triangle distance bound proves cannot win
+  // before their closest-point evaluation (false: only the same-triangle test).
+  bool bound_filter = true;
 };
 
 struct GridRunInfo {
   bool overflow = false;
   uint64_t seeds = 0, rounds = 0, entries = 0, evals = 0, ray_hits = 0, far_phases = 0, launches = 0, solo_rounds = 0,
-           max_list = 0, log_n = 0;
+           max_list = 0, log_n = 0, filter_same = 0, filter_bound = 0;
 };
 
 // A set of (mesh, grid) pairs computed together: one cell index space (grid k

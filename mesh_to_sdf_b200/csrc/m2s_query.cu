@@ -7,10 +7,10 @@
 //    fold order; batches of 2^28 pairs or more are visited in Morton order.
 //    Normal batches of fewer than 2^17 queries take k_brute_normal_warp: a
 //    warp per query, the same fold in the same order.
-//  * Bvh(Raycast) / RtreeBvh (bvh.rs:256-332, rtree_bvh.rs:143-201): exact
+//  * Bvh(Raycast) / RtreeBvh (bvh.rs:104-180, rtree_bvh.rs:143-201): exact
 //    nearest triangle on the LBVH, then the 3-axis ray vote.
-//  * Rtree (rtree.rs:306-326): the nearest triangle's signed distance.
-//  * Bvh(Normal) (bvh.rs:268-281): compare_distances folded over the near-tie
+//  * Rtree (rtree.rs:137-157): the nearest triangle's signed distance.
+//  * Bvh(Normal) (bvh.rs:117-129): compare_distances folded over the near-tie
 //    band of the nearest distance, in triangle order.
 //  * query_vector_to_closest_point_rtree_bvh (rtree_bvh.rs:217-276).
 #include <cuda_runtime.h>
@@ -608,7 +608,7 @@ __device__ __forceinline__ bool vote_inside(const MeshView& m, P3 p, bool* overf
 
 // Bvh(Normal): compare_distances over every triangle whose |signed distance|
 // lies in the near-tie band of the nearest distance, folded in triangle order
-// from f32::MAX with the rule of bvh.rs:277-279.
+// from f32::MAX with the rule of bvh.rs:125-127.
 constexpr int kBand = 32;
 
 template <bool STATS = false>
@@ -719,7 +719,7 @@ __device__ __forceinline__ void finish_query(const MeshView& m, uint64_t i, P3 p
     float d = fminf(F32_MAX, fsqrt(nn.d2));
     out[i] = inside ? -d : d;
   } else if (MODE == Q_RTREE) {
-    // rtree.rs:316-323: signed distance of the nearest triangle.
+    // rtree.rs:149-154: signed distance of the nearest triangle.
     TriRec r = load_tri(m.tris, nn.tri);
     out[i] = point_triangle_signed_distance(p, p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
   } else if (MODE == Q_BVH_NORMAL) {

@@ -429,7 +429,7 @@ int orc_generate_sdf(const float* v, uint64_t nv, const void* idx, uint64_t ni, 
       if (out_len) *out_len = 0;
       return ST_OK;
     }
-    return ST_EMPTY_MESH;  // rtree.rs:317 unwrap on None; bvh has no root node
+    return ST_EMPTY_MESH;  // rtree.rs:148 unwrap on None; bvh has no root node
   }
   CpuBvh bvh;
   bvh.build(m);
@@ -446,7 +446,7 @@ int orc_generate_sdf(const float* v, uint64_t nv, const void* idx, uint64_t ni, 
       float d2;
       long t = bvh.nearest(m, p, &d2);
       if (accel == 2) {
-        // query_sdf_rtree (rtree.rs:313-325)
+        // query_sdf_rtree (rtree.rs:137-157)
         r = point_triangle_signed_distance(p, m.a[t], m.b[t], m.c[t]);
       } else {
         // query_sdf_bvh Raycast (bvh.rs:283-328), query_sdf_rtree_bvh (rtree_bvh.rs:150-199)

@@ -11,8 +11,16 @@ properties that hold at any size:
     cell diagonal above it (grid.rs:495-558 relaxes the 3x3x3 block);
   * Raycast: every sign equals the restatement's on all host threads (signs
     come from ray parities, independent of the propagation order) and values
-    differ from it in under 15 % of cells (the reference's own 1- vs
-    8-thread drift is 1-15 % on the test meshes, generate/grid.rs:318-339).
+    differ from it in under 7.5 % of cells (measured: 6.03 %; the reference's
+    own 1- vs 8-thread drift is 1-15 % on the test meshes,
+    generate/grid.rs:318-339);
+  * Normal (terrain): values differ from the restatement's in under 1 % of
+    cells, and every sign difference is accounted for: the two sides hold
+    different triangles there (the same triangle gives the same signed value),
+    either at exactly the same distance, or within compare_distances' tie
+    band (lib.rs:315-332), or — where the propagation order let a different
+    triangle win — at most a cell diagonal apart, in a bounded number of cells;
+  * the proposal filter (m2s_set_grid_bound_filter) changes no bit.
 """
 import os
 
@@ -83,7 +91,13 @@ def test_bench_grid_full_size(orc):
     ref = orc.generate_grid_sdf(v, idx, grid.first_cell, grid.cell_size, grid.cell_count, "raycast",
                                 n_threads=os.cpu_count() or 1)
     assert np.array_equal(np.signbit(d), np.signbit(ref))
-    assert np.mean(bits(np.abs(d)) != bits(np.abs(ref))) < 0.15
+    assert np.mean(bits(np.abs(d)) != bits(np.abs(ref))) < 0.075
+    m2s.set_grid_bound_filter(False)
+    try:
+        unfiltered = run_grid(v, topo, grid, S.Raycast)
+    finally:
+        m2s.set_grid_bound_filter(True)
+    assert np.array_equal(bits(unfiltered), bits(d)), "the proposal filter changed the bench grid"
     # the batched job gives the same bits: with one wave for both grids the
     # 256^3 grid runs through the MULTI kernels beside a small one
     import torch
@@ -100,10 +114,48 @@ def test_bench_grid_full_size(orc):
     assert np.array_equal(bits(out[: len(d)].cpu().numpy()), bits(d))
 
 
-def test_terrain_grid_full_size():
+def approx_eq_band(a, b):
+    """float-cmp's approx_eq!(f32, a, b, ulps = 2, epsilon = 1e-6) on
+    non-negative magnitudes (lib.rs:321): within 1e-6, or at most 2 ulps apart."""
+    a = np.asarray(a, np.float32)
+    b = np.asarray(b, np.float32)
+    ulps = np.abs(bits(a).astype(np.int64) - bits(b).astype(np.int64))
+    return (np.abs(a.astype(np.float64) - b.astype(np.float64)) <= np.float32(1e-6)) | (ulps <= 2)
+
+
+def sign_breakdown(gpu, ref, cell_diag):
+    """Cells whose Normal sign differs, by cause (see the module docstring)."""
+    flip = np.signbit(gpu) != np.signbit(ref)
+    ga, ra = np.abs(gpu[flip]), np.abs(ref[flip])
+    same = bits(ga) == bits(ra)
+    band = ~same & approx_eq_band(ga, ra)
+    order = ~same & ~band
+    gap = np.abs(ga[order].astype(np.float64) - ra[order]) / cell_diag
+    return {"sign_differs": int(flip.sum()), "same_distance": int(same.sum()), "tie_band": int(band.sum()),
+            "order": int(order.sum()), "order_max_gap_cell_diagonals": float(gap.max()) if len(gap) else 0.0}
+
+
+def test_terrain_grid_full_size(orc):
     v, idx = synth.terrain(512, seed=0)
     lo, hi = synth.padded_bbox(v, 0.1)
     grid = m2s.Grid.from_bounding_box(lo, hi, [384, 384, 128])
     topo = T.TriangleStrip(idx)
     d = run_grid(v, topo, grid, S.Normal)
     check_real_triangle(d, exact_nearest(v, topo, grid, A.rtree()), grid, "terrain 384x384x128")
+    ref = orc.generate_grid_sdf(v, idx, grid.first_cell, grid.cell_size, grid.cell_count, "normal", strip=True,
+                                n_threads=os.cpu_count() or 1)
+    differ = float(np.mean(bits(np.abs(d)) != bits(np.abs(ref))))
+    cell = float(np.linalg.norm(grid.cell_size.astype(np.float64)))
+    br = sign_breakdown(d, ref, cell)
+    print("terrain vs restatement:", {"value_differs_frac": differ, **br})
+    # measured on B200 against the restatement on 16 host threads: values
+    # 0.77 %, signs 90,539 (0.48 %: 34,275 at the same distance, 8,464 in the
+    # tie band, 47,800 by order, at most 0.039 cell diagonals apart); the
+    # restatement's own multi-thread run varies from run to run, so the bars
+    # keep some room
+    assert differ < 0.012, differ
+    # a different winning triangle at a distinct distance stays close (both
+    # are propagated values of real triangles) and is rare
+    assert br["order_max_gap_cell_diagonals"] <= 0.25, br
+    assert br["order"] <= 0.004 * len(d), br
+    assert br["sign_differs"] <= 0.007 * len(d), br

@@ -182,7 +182,7 @@ def test_topology_encodings(orc):
 
 
 def test_build_query_equals_generate():
-    # default.rs:146-150, bvh.rs:383-387, rtree.rs:374-378, rtree_bvh.rs:330-334
+    # default.rs:131-150, bvh.rs:216-232, rtree.rs:191-206, rtree_bvh.rs:314-331
     v, idx = synth.star(3, seed=7)
     q = synth.mixed_points(v, idx, 2000, seed=8)
     for am in m2s.ALL_SDF_ACCELERATION_METHODS:
@@ -332,7 +332,7 @@ def test_error_statuses():
         assert np.all(m2s.generate_sdf(TETRA_V, T.TriangleList(empty), qn, A.none(S.Normal)) == np.finfo(np.float32).max)
     assert len(m2s.generate_sdf(TETRA_V, T.TriangleList(empty), q, A.rtree_bvh())) == 0  # rtree_bvh.rs:96-97
     assert m2s.build_sdf_acceleration(TETRA_V, T.TriangleList(empty), A.rtree_bvh()) is None
-    with pytest.raises(m2s.M2SError) as e:  # rtree.rs:317
+    with pytest.raises(m2s.M2SError) as e:  # rtree.rs:148
         m2s.generate_sdf(TETRA_V, T.TriangleList(empty), q, A.rtree())
     assert e.value.status == 6
     # a single triangle (the LBVH root is a leaf)
