@@ -34,9 +34,46 @@ N_BRUTE = 65_536
 SEED = 0
 
 
-# DRAM bytes (read + write) of one propagation launch of this workload, from an
-# ncu capture of dram__bytes_read.sum and dram__bytes_write.sum (one launch).
+# DRAM bytes (read + write) of one propagation launch of the bench grid, from
+# an ncu capture of dram__bytes_read.sum and dram__bytes_write.sum (one launch).
 PROPAGATE_DRAM_BYTES = 324_104_960 + 438_122_752
+PROPAGATE_DRAM_SOURCE = "profiles/k_propagate_star_s6_grid256.md (ncu, one 256^3 launch)"
+
+
+# FP32 operations of one propagation evaluation, counting every add, sub, mul,
+# div and sqrt as one: the closest point on the interior path (67), the
+# squared distance (8) and its square root (1); Normal adds the sign's dot
+# product (5).  The strict build issues no fused multiply-add.
+EVAL_OPS = {"raycast": 76, "normal": 81}
+
+
+def grid_roofline(cells, n_vertices, n_tris, phases, stats, hbm_peak, peak_source, sm_mhz, sign):
+    """Roofline of the dominant kernel of a grid (propagation).  Algorithmic
+    bytes: 4 B per output cell plus the mesh once (12 B per vertex, 12 B of
+    u32 indices per triangle) — the HBM bytes the result itself needs.
+    `implementation_bytes` counts what the kernel's own data structures move
+    (per relaxed state its 8 B entry and 48 B triangle record, per proposal
+    the neighbour's 8 B snapshot and 8 B working key), mostly L2 hits.
+    `traffic` is the ncu DRAM count of one launch of the bench grid and
+    `traffic_ratio` its multiple of the algorithmic bytes.  `fp32` sets the
+    evaluated proposals' FP32 operations against the FP32 peak (148 SMs x
+    128 lanes x the SM clock, one operation per lane and cycle: no FMA)."""
+    prop_s = phases["propagation"] / 1e3
+    algo = 4 * cells + 12 * n_vertices + 12 * n_tris
+    achieved = algo / prop_s / 1e9 if prop_s > 0 else 0.0
+    impl = stats["states_relaxed"] * 56 + stats["neighbour_evals"] * 16
+    evaluated = stats["neighbour_evals"] - stats.get("dropped_same", 0) - stats.get("dropped_bound", 0)
+    peak_tops = 148 * 128 * sm_mhz * 1e6 / 1e12
+    tops = evaluated * EVAL_OPS[sign] / prop_s / 1e12 if prop_s > 0 else 0.0
+    return {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+            "traffic": PROPAGATE_DRAM_BYTES, "traffic_ratio": PROPAGATE_DRAM_BYTES / algo,
+            "traffic_source": PROPAGATE_DRAM_SOURCE, "algorithmic_bytes": algo,
+            "implementation_bytes": impl, "implementation_gbs": impl / prop_s / 1e9 if prop_s > 0 else 0.0,
+            "kernel": "k_propagate (propagation rounds)", "peak_source": peak_source,
+            "fp32": {"proposals": stats["neighbour_evals"], "evaluated": evaluated,
+                     "ops_per_evaluation": EVAL_OPS[sign], "achieved_tops": tops, "peak_tops": peak_tops,
+                     "frac": tops / peak_tops, "proposals_per_s": stats["neighbour_evals"] / prop_s},
+            "phase_ms": phases, "stats": stats}
 
 
 def workload():
@@ -172,39 +209,128 @@ def run_cpu_grid(v, idx, g, threads):
     return time.perf_counter() - t
 
 
-def grid_accuracy(v, idx, grid, gpu, threads, n_sample=10_000):
-    """Accuracy of the GPU grid against the oracle (reported, not timed): the
-    restatement's own grid on all host threads (cells whose value or sign
-    differ; the reference's propagation is order-dependent, so values may
-    differ where triangles tie), and an FP64 brute force on seeded sample cells
-    (max / RMS distance error, sign mismatches, those at cells within 1e-5 of
-    the bbox diagonal of the surface counted apart as ambiguous)."""
+def fp64_report(v, idx, points, values, threads, strip=False, raycast_sign=True, diag=None, ref64=None):
+    """Error of f32 results against an FP64 brute force at the same points
+    (reported, not timed): max / RMS of | |value| - d64 |, the max relative to
+    the bounding-box diagonal, and — for Raycast-signed results — sign
+    mismatches against the FP64 3-ray vote, those within 1e-5 of the diagonal
+    of the surface counted apart as ambiguous."""
     import oracle
 
-    ref = oracle.generate_grid_sdf(v, idx, grid.first_cell, grid.cell_size, grid.cell_count, "raycast",
-                                   n_threads=threads)
-    ga, ra = np.abs(gpu), np.abs(ref)
-    differ = ga.view(np.uint32) != ra.view(np.uint32)
-    cell_diag = float(np.linalg.norm(grid.cell_size.astype(np.float64)))
+    d64, inside64 = ref64 if ref64 is not None else oracle.generate_sdf_f64(v, idx, points, strip=strip,
+                                                                             n_threads=threads)
+    if diag is None:
+        lo, hi = synth_bbox(v)
+        diag = float(np.linalg.norm(hi - lo))
+    vals = np.asarray(values, np.float32)
+    err = np.abs(np.abs(vals.astype(np.float64)) - d64)
+    out = {"sample": int(len(points)), "max_err": float(err.max()) if len(err) else 0.0,
+           "rms_err": float(np.sqrt(np.mean(err ** 2))) if len(err) else 0.0,
+           "max_err_rel_bbox_diag": float(err.max() / diag) if len(err) else 0.0}
+    if raycast_sign:
+        flip = np.signbit(vals) != inside64
+        near = d64 <= 1e-5 * diag
+        out["sign_mismatch"] = int((flip & ~near).sum())
+        out["sign_mismatch_ambiguous"] = int((flip & near).sum())
+    return out
+
+
+def sample_cells(grid, n, seed):
+    """n seeded distinct cells of the grid and their centres (grid.rs:135-141 arithmetic)."""
     nx, ny, nz = (int(c) for c in grid.cell_count)
-    rng = np.random.default_rng(SEED + 3)
-    cells = rng.choice(len(gpu), n_sample, replace=False)
+    rng = np.random.default_rng(seed)
+    cells = rng.choice(nx * ny * nz, min(n, nx * ny * nz), replace=False)
     ijk = np.stack([cells // (ny * nz), (cells // nz) % ny, cells % nz], axis=1)
     centres = (grid.first_cell.astype(np.float32) + ijk.astype(np.float32) * grid.cell_size.astype(np.float32))
-    d64, inside64 = oracle.generate_sdf_f64(v, idx, centres.astype(np.float32), n_threads=threads)
-    lo, hi = synth_bbox(v)
-    diag = float(np.linalg.norm(hi - lo))
-    err = np.abs(np.abs(gpu[cells].astype(np.float64)) - d64)
-    flip = np.signbit(gpu[cells]) != inside64.astype(bool)
-    near = d64 <= 1e-5 * diag
-    return {"restatement": {"cells": int(len(gpu)), "value_differs": int(differ.sum()),
-                            "value_differs_frac": float(differ.mean()),
-                            "sign_differs": int((np.signbit(gpu) != np.signbit(ref)).sum()),
-                            "max_value_diff_cell_diagonals": float((np.abs(ga.astype(np.float64) - ra)).max() / cell_diag),
-                            "threads": threads},
-            "fp64": {"sample_cells": n_sample, "max_err": float(err.max()), "rms_err": float(np.sqrt(np.mean(err ** 2))),
-                     "max_err_rel_bbox_diag": float(err.max() / diag),
-                     "sign_mismatch": int((flip & ~near).sum()), "sign_mismatch_ambiguous": int((flip & near).sum())}}
+    return cells, centres.astype(np.float32)
+
+
+def approx_eq_band(a, b):
+    """float-cmp's approx_eq!(f32, a, b, ulps = 2, epsilon = 1e-6) on
+    non-negative magnitudes (lib.rs:321): within 1e-6, or at most 2 ulps apart."""
+    a = np.asarray(a, np.float32)
+    b = np.asarray(b, np.float32)
+    ulps = np.abs(a.view(np.uint32).astype(np.int64) - b.view(np.uint32).astype(np.int64))
+    return (np.abs(a.astype(np.float64) - b.astype(np.float64)) <= np.float32(1e-6)) | (ulps <= 2)
+
+
+def grid_vs_restatement(gpu, ref, cell_diag, threads):
+    """Cells whose value or sign differ between the GPU grid and the
+    restatement's.  The reference's propagation is order-dependent, so values
+    may differ where triangles compete; a sign difference means the two sides
+    hold different triangles there (the same triangle gives the same signed
+    value), split by how their distances compare: the same bits, inside
+    compare_distances' tie band (lib.rs:315-332), or apart (a different
+    triangle won through the propagation order)."""
+    ga, ra = np.abs(gpu), np.abs(ref)
+    differ = ga.view(np.uint32) != ra.view(np.uint32)
+    flip = np.signbit(gpu) != np.signbit(ref)
+    fa_, fr = ga[flip], ra[flip]
+    same = fa_.view(np.uint32) == fr.view(np.uint32)
+    band = ~same & approx_eq_band(fa_, fr)
+    order = ~same & ~band
+    gap = np.abs(fa_[order].astype(np.float64) - fr[order]) / cell_diag
+    return {"cells": int(len(gpu)), "value_differs": int(differ.sum()), "value_differs_frac": float(differ.mean()),
+            "max_value_diff_cell_diagonals": float(np.abs(ga.astype(np.float64) - ra).max() / cell_diag),
+            "sign_differs": int(flip.sum()), "sign_differs_same_distance": int(same.sum()),
+            "sign_differs_tie_band": int(band.sum()), "sign_differs_order": int(order.sum()),
+            "sign_differs_order_max_gap_cell_diagonals": float(gap.max()) if len(gap) else 0.0,
+            "threads": threads}
+
+
+def grid_accuracy(v, idx, grid, gpu, threads, sign="raycast", strip=False, n_sample=10_000, ref=None):
+    """Accuracy of a GPU grid (reported, not timed): against the restatement's
+    own grid on all host threads, and against an FP64 brute force on seeded
+    sample cells — beside the restatement's own FP64 error on the same cells,
+    which shows what the reference's propagation itself gives up there."""
+    import oracle
+
+    t0 = time.perf_counter()
+    if ref is None:
+        ref = oracle.generate_grid_sdf(v, idx, grid.first_cell, grid.cell_size, grid.cell_count, sign, strip=strip,
+                                       n_threads=threads)
+    ref_s = time.perf_counter() - t0
+    cell_diag = float(np.linalg.norm(grid.cell_size.astype(np.float64)))
+    cells, centres = sample_cells(grid, n_sample, SEED + 3)
+    raycast = sign == "raycast"
+    gpu_err = fp64_report(v, idx, centres, gpu[cells], threads, strip=strip, raycast_sign=raycast)
+    ref_err = fp64_report(v, idx, centres, ref[cells], threads, strip=strip, raycast_sign=raycast)
+    return {"restatement": grid_vs_restatement(gpu, ref, cell_diag, threads),
+            "fp64": {"gpu": gpu_err, "restatement": ref_err}}, ref_s
+
+
+ORACLE_ACCEL = {0: "none", 1: "bvh", 2: "rtree", 3: "rtree_bvh"}
+
+
+def point_accuracy(v, idx, q, outs, points, threads, n_parity=50_000, n_fp64=20_000, strip=False):
+    """Point results against the oracle and FP64 (reported, not timed): every
+    LBVH method on a seeded sample of `n_parity` of its points, the brute
+    force (None) on all of its points — bit for bit; and each method's FP64
+    max / RMS error on a seeded sample of `n_fp64` points (the FP64 distances
+    are computed once per sample and shared)."""
+    import oracle
+
+    rng = np.random.default_rng(SEED + 5)
+    cache = {}
+    for name, (am, gpu) in outs.items():
+        n = len(gpu)
+        if am.kind == 0:
+            pick = np.arange(n)
+        else:
+            pick = np.sort(rng.choice(n, min(n_parity, n), replace=False))
+        ref = oracle.generate_sdf(v, idx, q[pick], ORACLE_ACCEL[am.kind], int(am.sign), strip=strip,
+                                  n_threads=threads)
+        points[name]["parity"] = {"points": int(len(pick)),
+                                  "bits_differ": int(np.sum(gpu[pick].view(np.uint32) != ref.view(np.uint32))),
+                                  "against": "oracle (C++ restatement), bit for bit"}
+        key = min(n, N_BRUTE) if am.kind == 0 else n
+        if key not in cache:
+            sel = np.sort(np.random.default_rng(SEED + 6).choice(key, min(n_fp64, key), replace=False))
+            cache[key] = (sel, oracle.generate_sdf_f64(v, idx, q[sel], strip=strip, n_threads=threads))
+        sel, ref64 = cache[key]
+        raycast = int(am.sign) == 0 and am.kind != 2  # Rtree signs by the normal
+        points[name]["fp64"] = fp64_report(v, idx, q[sel], gpu[sel], threads, strip=strip, raycast_sign=raycast,
+                                           ref64=ref64)
 
 
 def synth_bbox(v):
@@ -314,6 +440,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-points", action="store_true")
+    ap.add_argument("--no-workloads", action="store_true",
+                    help="leave the bounded c1 / c3 / c4 / c5 entries out of the default line")
     ap.add_argument("--small", action="store_true",
                     help="one short pass for profilers: one grid, 100k Rtree / RtreeBvh points, 8k brute-force points")
     ap.add_argument("--grid", type=int, default=128, help="grid edge of the --small pass")
@@ -409,18 +537,28 @@ def main():
     except Exception:
         pass
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
-    # Algorithmic bytes of a relax round: per relaxed state its entry (8 B) and
-    # triangle record (48 B); per neighbour proposal (the on-grid cells of the
-    # 26 around the state) the neighbour's snapshot key read (8 B) and its
-    # working key (8 B).
-    relax_bytes = stats["states_relaxed"] * 56 + stats["neighbour_evals"] * 16
-    prop_s = phases["propagation"] / 1e3
-    achieved = relax_bytes / prop_s / 1e9 if prop_s > 0 else 0.0
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                "frac": achieved / hbm_peak, "traffic": PROPAGATE_DRAM_BYTES,
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one 256^3 launch",
-                "kernel": "k_propagate (propagation rounds)", "peak_source": "measured" if peaks else "fallback",
-                "phase_ms": phases, "stats": stats}
+    roofline = grid_roofline(N, len(v), T, phases, stats, hbm_peak, "measured" if peaks else "fallback",
+                             float(peaks.get("sm_max_mhz", 1965.0)), "raycast")
+    # the filtered propagation variant on the same grid (untimed beside the
+    # step; results are identical), and the FP64 audit of the grid's f32
+    # decisions (counts only)
+    m2s.set_grid_bound_filter(True)
+    m2s.set_profiling(True)
+    flush.fill_(1)
+    step()
+    torch.cuda.synchronize()
+    m2s.set_profiling(False)
+    m2s.set_grid_bound_filter(False)
+    fst = m2s.last_grid_stats()
+    roofline["filter_variant"] = {"propagation_ms": m2s.last_grid_phase_ms()["propagation"],
+                                  "proposals": fst["neighbour_evals"], "dropped_same": fst["dropped_same"],
+                                  "dropped_bound": fst["dropped_bound"]}
+    m2s.set_fp64_audit(True)
+    step()
+    torch.cuda.synchronize()
+    m2s.set_fp64_audit(False)
+    grid_audit = m2s.last_grid_audit()
+    assert int(status.item()) == 0
 
     # ---- e2e: the host-pointer C ABI with pinned buffers, H2D + D2H inside the timed region
     vh = torch.from_numpy(np.ascontiguousarray(v)).pin_memory().numpy()
@@ -455,9 +593,10 @@ def main():
     assert np.array_equal(oh.view(np.uint32), out.cpu().numpy().view(np.uint32)), "e2e result differs from device path"
 
     # ---- point queries of the same configuration
-    points = {}
+    points, point_outs = {}, {}
+    q_host = synth.mixed_points(v, idx, N_POINTS, seed=SEED)
     if not args.no_points:
-        q = torch.from_numpy(synth.mixed_points(v, idx, N_POINTS, seed=SEED)).to(dev)
+        q = torch.from_numpy(q_host).to(dev)
         qo = torch.empty(N_POINTS, dtype=torch.float32, device=dev)
         # the library's query autotuner picks the node budget (one thread per
         # query, then one warp) on the Bvh+Raycast batch
@@ -483,14 +622,18 @@ def main():
             e1.record()
             torch.cuda.synchronize()
             ms = e0.elapsed_time(e1) / reps
+            point_outs[name] = (am, qo[:n].cpu().numpy().copy())
             points[name] = {"points": n, "ms": ms, "pts_per_s": n / (ms / 1e3)}
             if name.startswith("none"):
                 points[name]["pairs_per_s"] = n * T / (ms / 1e3)
-            else:  # traversal counts per query, from one profiled (untimed) run
+            else:  # traversal counts per query and the FP64 audit, from one untimed run
                 m2s.set_profiling(True)
+                m2s.set_fp64_audit(True)
                 acc.query_device(qq, qo, status, stream)
                 torch.cuda.synchronize()
                 qs = m2s.last_query_stats()
+                points[name]["fp64_audit"] = m2s.last_query_audit()
+                m2s.set_fp64_audit(False)
                 m2s.set_profiling(False)
                 points[name]["per_query"] = {k[:-len("_per_query")]: round(v_, 2) for k, v_ in qs.items()
                                              if k.endswith("_per_query")}
@@ -528,7 +671,26 @@ def main():
         sec = run_cpu_grid(v, idx, slab, cores)
         cpu = {"value": slab.get_total_cell_count() / sec, "unit": "cells/s", "cores": cores, "kind": "port",
                "sample": "256x256x32 middle z-slab (2.1M cells) of the 256^3 grid, C++ restatement, all host threads"}
-        accuracy = grid_accuracy(v, idx, grid, out.cpu().numpy(), cores)
+        accuracy, _ = grid_accuracy(v, idx, grid, out.cpu().numpy(), cores)
+        point_accuracy(v, idx, q_host, point_outs, points, cores)
+
+    # ---- the other configurations, bounded (rank 0, one GPU): each with its
+    # own CPU baseline and accuracy figures
+    workloads = {}
+    if rank == 0 and world == 1 and not args.no_workloads:
+        mesh.close()
+        acc_on = not args.no_cpu_baseline
+        jobs = (("c1", lambda: small_or_terrain_entry("c1", 5, 3, acc_on, peaks)),
+                ("c3", lambda: small_or_terrain_entry("c3", 3, 2, acc_on, peaks)),
+                ("c4", lambda: batch_entry(256, 2, True, 0, acc_on, cpu_every=32)),
+                ("c5", lambda: serving_entry((100.0, 400.0), 200, True)))
+        for name, fn in jobs:
+            t0 = time.perf_counter()
+            try:
+                workloads[name] = fn()
+            except Exception as e:  # reported in the line; the headline stands
+                workloads[name] = {"error": f"{type(e).__name__}: {e}"}
+            workloads[name]["wall_s"] = round(time.perf_counter() - t0, 1)
 
     if rank == 0:
         line = {"metric": "SDF cells/s (generate_grid_sdf, Raycast)", "value": value, "unit": "cells/s",
@@ -540,24 +702,30 @@ def main():
                            "l2": "flushed between steps (256 MiB write, untimed)"},
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": int(launches),
                 "clocks": clk.summary(), "points": points, "results": results, "accuracy": accuracy,
-                "wall_s_timed": t_wall}
+                "fp64_audit": grid_audit,
+                "workloads": workloads, "wall_s_timed": t_wall}
         print(json.dumps(line), flush=True)
-    mesh.close()
+    if not workloads:
+        mesh.close()
     if world > 1:
         torch_destroy()
 
 
-def other_workload(args):
-    """c1: icosphere s3, 32^3 Raycast grid over [-1.2, 1.2]^3, 10,000 RtreeBvh points.
-    c3: 512 x 512 fBm terrain as one TriangleStrip, 384 x 384 x 128 Normal grid over
-    the 10 %-padded bbox, 4M uniform Rtree points.  One JSON line per workload."""
+def small_or_terrain_entry(which, steps=5, warmup=3, accuracy=True, peaks=None):
+    """c1: icosphere s3, 32^3 Raycast grid over [-1.2, 1.2]^3, 10,000 RtreeBvh
+    points.  c3: 512 x 512 fBm terrain as one TriangleStrip, 384 x 384 x 128
+    Normal grid over the 10 %-padded bbox, 4M uniform Rtree points.  Returns
+    one dict: GPU rates, the propagation roofline, and (accuracy=True) the
+    restatement's grid and the oracle's points on the host cores — both the
+    accuracy checks and the CPU baseline of this configuration."""
     import torch
 
     import mesh_to_sdf_b200 as m2s
     from mesh_to_sdf_b200 import synth
 
     A, S = m2s.AccelerationMethod, m2s.SignMethod
-    if args.workload == "c1":
+    strip = which == "c3"
+    if which == "c1":
         v, idx = synth.icosphere(3)
         topo = m2s.Topology.TriangleList(idx)
         grid = m2s.Grid.from_bounding_box([-1.2] * 3, [1.2] * 3, [32, 32, 32])
@@ -575,17 +743,33 @@ def other_workload(args):
     out = torch.empty(N, dtype=torch.float32, device="cuda")
     status = torch.zeros(1, dtype=torch.int32, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    for _ in range(args.warmup):
+    for _ in range(max(warmup, 1)):
         mesh.grid_device(grid, sign, out, status)
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    for i in range(args.steps):
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for i in range(steps):
         flush.fill_(i & 0xFF)
         ev[i][0].record()
         mesh.grid_device(grid, sign, out, status)
         ev[i][1].record()
     torch.cuda.synchronize()
     gms = float(np.mean([a.elapsed_time(b_) for a, b_ in ev]))
-    stats = m2s.last_grid_stats()
+    m2s.set_profiling(True)
+    flush.fill_(1)
+    mesh.grid_device(grid, sign, out, status)
+    torch.cuda.synchronize()
+    m2s.set_profiling(False)
+    phases, stats = m2s.last_grid_phase_ms(), m2s.last_grid_stats()
+    m2s.set_fp64_audit(True)
+    mesh.grid_device(grid, sign, out, status)
+    torch.cuda.synchronize()
+    m2s.set_fp64_audit(False)
+    grid_audit = m2s.last_grid_audit()
+    peaks = peaks or {}
+    sname = "raycast" if int(sign) == 0 else "normal"
+    roof = grid_roofline(N, len(v), mesh.triangle_count, phases, stats, float(peaks.get("hbm_gbs", 6650.0)),
+                         "measured" if peaks else "fallback", float(peaks.get("sm_max_mhz", 1965.0)), sname)
+    for k in ("traffic", "traffic_ratio", "traffic_source", "stats", "phase_ms"):
+        roof.pop(k)  # the ncu traffic figure belongs to the bench grid
     qd = torch.from_numpy(q).cuda()
     qo = torch.empty(npts, dtype=torch.float32, device="cuda")
     budget, _ = mesh.autotune_queries(qd)  # the library's query autotuner, on these points
@@ -598,57 +782,74 @@ def other_workload(args):
     e1.record()
     torch.cuda.synchronize()
     qms = e0.elapsed_time(e1)
+    m2s.set_fp64_audit(True)
+    mesh.query_device(qd, qo, status)
+    torch.cuda.synchronize()
+    m2s.set_fp64_audit(False)
+    points_audit = m2s.last_query_audit()
     assert int(status.item()) == 0, int(status.item())
-    accuracy = None
-    if not args.no_cpu_baseline:
-        accuracy = workload_accuracy(v, idx, args.workload == "c3", grid, sign, out.cpu().numpy(), q,
-                                     qo.cpu().numpy(), am)
-    print(json.dumps({"workload": args.workload, "triangles": mesh.triangle_count, "grid": list(grid.cell_count),
-                      "sign": sign.name, "grid_ms": gms, "cells_per_s": N / (gms / 1e3), "grid_stats": stats,
-                      "points": npts, "method": repr(am), "points_ms": qms, "pts_per_s": npts / (qms / 1e3),
-                      "node_budget": budget, "accuracy": accuracy}),
-          flush=True)
+    line = {"workload": which, "triangles": mesh.triangle_count, "grid": [int(c) for c in grid.cell_count],
+            "sign": sign.name, "grid_ms": gms, "cells_per_s": N / (gms / 1e3), "grid_phase_ms": phases,
+            "grid_stats": stats, "roofline": roof, "points": npts, "method": repr(am), "points_ms": qms,
+            "pts_per_s": npts / (qms / 1e3), "node_budget": budget,
+            "fp64_audit": {"grid": grid_audit, "points": points_audit}}
+    mesh.close()
+    if accuracy:
+        import oracle
+
+        threads = os.cpu_count() or 1
+        gpu_grid, gpu_pts = out.cpu().numpy(), qo.cpu().numpy()
+        acc, ref_s = grid_accuracy(v, idx, grid, gpu_grid, threads, sname, strip,
+                                   n_sample=10_000 if which == "c1" else 2_000)
+        pts = {which: {"points": npts}}
+        point_accuracy(v, idx, q, {which: (am, gpu_pts)}, pts, threads,
+                       n_parity=10_000 if which == "c1" else 50_000, n_fp64=10_000 if which == "c1" else 2_000,
+                       strip=strip)
+        acc["points"] = pts[which]
+        line["accuracy"] = acc
+        # the CPU baseline of this configuration: the restatement's grid above,
+        # and its points (RtreeBvh: a serial loop, as in the reference)
+        ncpu = npts if which == "c1" else 200_000
+        t0 = time.perf_counter()
+        oracle.generate_sdf(v, idx, q[:ncpu], ORACLE_ACCEL[am.kind], int(am.sign), strip=strip,
+                            n_threads=1 if am.kind == 3 else threads)
+        pt_s = time.perf_counter() - t0
+        line["cpu_baseline"] = {"cells_per_s": N / ref_s, "points_per_s": ncpu / pt_s, "cores": threads,
+                                "kind": "port",
+                                "sample": f"the whole grid; {ncpu} of the {npts} points"
+                                          + (" (RtreeBvh: one thread, as the reference's serial loop)"
+                                             if am.kind == 3 else "")}
+    return line
 
 
-def workload_accuracy(v, idx, strip, grid, sign, gpu_grid, q, gpu_pts, am, n_sample=50_000):
-    """The c1 / c3 lines' accuracy (reported, not timed).  Grid: the
-    restatement on all host threads; cells whose sign differs are split into
-    tie-ambiguous ones (the same distance bits from a differently oriented
-    triangle, so the sign follows the tie order) and the rest.  Points: the
-    oracle on a seeded sample (the same lowest-index tie rule, so bit-exact)."""
-    import oracle
-
-    threads = os.cpu_count() or 1
-    ref = oracle.generate_grid_sdf(v, idx, grid.first_cell, grid.cell_size, grid.cell_count,
-                                   "raycast" if int(sign) == 0 else "normal", strip=strip, n_threads=threads)
-    ga, ra = np.abs(gpu_grid), np.abs(ref)
-    flip = np.signbit(gpu_grid) != np.signbit(ref)
-    tie = flip & (ga.view(np.uint32) == ra.view(np.uint32))
-    rng = np.random.default_rng(SEED + 11)
-    pick = rng.choice(len(q), min(n_sample, len(q)), replace=False)
-    codes = {0: "none", 1: "bvh", 2: "rtree", 3: "rtree_bvh"}
-    opts = oracle.generate_sdf(v, idx, q[pick], codes[am.kind], int(am.sign), strip=strip, n_threads=threads)
-    return {"grid_vs_restatement": {"cells": int(len(gpu_grid)),
-                                    "value_differs_frac": float(np.mean(ga.view(np.uint32) != ra.view(np.uint32))),
-                                    "sign_differs": int(flip.sum()), "sign_differs_tie_ambiguous": int(tie.sum()),
-                                    "threads": threads},
-            "points_vs_oracle": {"sample": int(len(pick)),
-                                 "bits_differ": int(np.sum(gpu_pts[pick].view(np.uint32) != opts.view(np.uint32)))}}
+def other_workload(args):
+    print(json.dumps(small_or_terrain_entry(args.workload, args.steps, args.warmup, not args.no_cpu_baseline,
+                                            load_peaks())), flush=True)
 
 
-def batch_workload(args):
-    """c4: `--batch` displaced spheres (subdivision 2..6, scale U[0.5, 2], random
-    rotation) with cubic Raycast grids of edge 32..192 over their padded boxes,
-    all resident.  Times one pass of single-grid calls (one per mesh) against the
-    same grids as one batched plan replayed from its CUDA graph, after checking
-    that both give the same bits.  One JSON line."""
+def load_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+def batch_entry(n_meshes=256, steps=3, autotune=True, wave_cells=0, accuracy=True, cpu_every=16):
+    """c4: `n_meshes` displaced spheres (subdivision 2..6, scale U[0.5, 2],
+    random rotation) with cubic Raycast grids of edge 32..192 over their
+    padded boxes, all resident.  Times one pass of single-grid calls (one per
+    mesh: the plain path) against the same grids as one batched plan replayed
+    from its CUDA graph, after checking that both give the same bits.  With
+    accuracy: FP64 errors on sample cells of every 16th grid, and the CPU
+    baseline (the restatement, one generate_grid_sdf call per mesh, on every
+    `cpu_every`-th mesh).  Returns one dict."""
     import torch
 
     import mesh_to_sdf_b200 as m2s
     from mesh_to_sdf_b200 import synth
 
     A, S = m2s.AccelerationMethod, m2s.SignMethod
-    items = synth.batch_meshes(args.batch, seed=SEED)
+    items = synth.batch_meshes(n_meshes, seed=SEED)
     meshes = [m2s.build_sdf_acceleration(v, m2s.Topology.TriangleList(i), A.none(S.Raycast)) for v, i, *_ in items]
     grids = [m2s.Grid.from_bounding_box(lo, hi, [e, e, e]) for _, _, lo, hi, e in items]
     off = m2s.grid_offsets(grids)
@@ -676,9 +877,9 @@ def batch_workload(args):
             per[e] = (n_ + 1, t_ + a.elapsed_time(b))
         return {str(e): {"grids": n_, "ms": round(t_, 2)} for e, (n_, t_) in sorted(per.items())}
 
-    def timed(fn, steps):
+    def timed(fn, k):
         ms = []
-        for _ in range(steps):
+        for _ in range(k):
             torch.cuda.synchronize()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record()
@@ -689,20 +890,20 @@ def batch_workload(args):
         return float(np.median(ms))
 
     plain_pass()
-    plain_ms = timed(plain_pass, max(1, min(args.steps, 3)))
+    plain_ms = timed(plain_pass, max(1, min(steps, 3)))
     per_edge = plain_by_edge()
     batched = torch.empty(N, dtype=torch.float32, device="cuda")
-    if args.wave_cells:
-        m2s.set_grid_tuning(wave_cells=args.wave_cells)
+    if wave_cells:
+        m2s.set_grid_tuning(wave_cells=wave_cells)
     plan = m2s.GridPlan(meshes, grids, S.Raycast, batched, status)
     blocks0 = plan.blocks
     plan.run()
     t0 = time.time()
-    chosen = blocks0 if args.no_autotune else plan.autotune()
+    chosen = plan.autotune() if autotune else blocks0
     tune_s = time.time() - t0
     plan.run()
     stats = m2s.last_grid_stats()
-    batch_ms = timed(plan.run, max(3, args.steps))
+    batch_ms = timed(plan.run, max(3, steps))
     diff = plain.view(torch.int32) != batched.view(torch.int32)
     ndiff = int(diff.sum().item())
     same = ndiff == 0
@@ -716,19 +917,59 @@ def batch_workload(args):
             "blocks_default": blocks0, "blocks_autotuned": chosen, "autotune_s": tune_s,
             "plan_device_gb": plan.device_bytes / 1e9, "grid_stats": stats}
     plan.close()
+    if wave_cells:
+        m2s.set_grid_tuning()
+    if accuracy:
+        import oracle
+
+        threads = os.cpu_count() or 1
+        host = batched.cpu().numpy()
+        errs = []
+        for k in range(0, len(grids), 16):
+            v, i = items[k][:2]
+            cells, centres = sample_cells(grids[k], 500, SEED + 100 + k)
+            vals = host[int(off[k]):int(off[k + 1])][cells]
+            errs.append(fp64_report(v, i, centres, vals, threads))
+        worst = max(errs, key=lambda e: e["max_err_rel_bbox_diag"])
+        line["accuracy"] = {"fp64": {"grids": len(errs), "sample_cells_per_grid": 500,
+                                     "max_err_rel_bbox_diag": worst["max_err_rel_bbox_diag"],
+                                     "max_err": max(e["max_err"] for e in errs),
+                                     "rms_err": float(np.sqrt(np.mean([e["rms_err"] ** 2 for e in errs]))),
+                                     "sign_mismatch": sum(e["sign_mismatch"] for e in errs),
+                                     "sign_mismatch_ambiguous": sum(e["sign_mismatch_ambiguous"] for e in errs)}}
+        sub = items[::cpu_every]
+        cells, t0 = 0, time.perf_counter()
+        for v, i, lo, hi, e in sub:
+            g = m2s.Grid.from_bounding_box(lo, hi, [e, e, e])
+            oracle.generate_grid_sdf(v, i, g.first_cell, g.cell_size, g.cell_count, "raycast", n_threads=threads)
+            cells += g.get_total_cell_count()
+        line["cpu_baseline"] = {"cells_per_s": cells / (time.perf_counter() - t0), "cores": threads, "kind": "port",
+                                "sample": f"every {cpu_every}th of the {n_meshes} meshes ({len(sub)} grids, "
+                                          f"{cells} cells), one generate_grid_sdf call each"}
+    for m in meshes:
+        m.close()
+    return line
+
+
+def batch_workload(args):
+    line = batch_entry(args.batch, args.steps, not args.no_autotune, args.wave_cells, not args.no_cpu_baseline)
     print(json.dumps(line), flush=True)
-    if not same:
+    if not line["bit_identical"]:
         raise SystemExit("batched grids differ from single-grid calls")
 
 
-def serving_workload(args):
+def serving_entry(rates=(50.0, 100.0, 200.0, 400.0), n_req=200, plain=True):
     """c5: a server with a 120 GB device-memory budget and 64 resident meshes
-    of the batched-grid kind (RtreeBvh), fed Poisson arrivals at each rate of
-    `--rates`: 5 % uploads of new meshes (built on the GPU), 60 % point
-    requests (Q log-uniform in [1e3, 1e6], uniform in the mesh's padded box),
-    40 % Raycast grid requests (edge log-uniform in [64, 256] over the padded
-    box).  Host buffers are pinned.  Latency is submission to completion as the
-    server records it; one JSON line with p50/p99 per rate."""
+    of the batched-grid kind (RtreeBvh), fed Poisson arrivals at each rate:
+    5 % uploads of new meshes (built on the GPU), 60 % point requests (Q
+    log-uniform in [1e3, 1e6], uniform in the mesh's padded box), 40 % Raycast
+    grid requests (edge log-uniform in [64, 256] over the padded box).  Host
+    buffers are pinned.  Latency is arrival to completion.  With `plain`, the
+    same arrivals also go through the plain path — one library call per
+    request (query_sdf, a resident-mesh grid call with its copies, or
+    build_sdf_acceleration), served in arrival order by one host thread — and
+    both arms report p50 / p99 and aggregate cells/s and points/s.  Returns
+    one dict."""
     import torch
 
     import mesh_to_sdf_b200 as m2s
@@ -751,19 +992,39 @@ def serving_workload(args):
     # Warm-up, untimed: every kernel loaded once and the memory pool grown to
     # its working size (a pool growth may synchronise the device), as a
     # server does before it takes traffic.
-    warm = []
     wq = unit.numpy()
     wg = torch.empty(256 ** 3, dtype=torch.float32).pin_memory().numpy()
     wp = torch.empty(len(wq), dtype=torch.float32).pin_memory().numpy()
     for j, e in enumerate((64, 96, 128, 192, 256, 256)):
         lo, hi = boxes[j]
-        warm.append(srv.submit_grid(ids[j], m2s.Grid.from_bounding_box(lo, hi, [e, e, e]), S.Raycast, wg[:e ** 3]))
-        warm.append(srv.submit_points(ids[j], wq, wp))
+        warm = [srv.submit_grid(ids[j], m2s.Grid.from_bounding_box(lo, hi, [e, e, e]), S.Raycast, wg[:e ** 3]),
+                srv.submit_points(ids[j], wq, wp)]
         for t in warm:
             assert srv.wait(t)[0] == 0
-        warm = []
-    rates = [float(r) for r in args.rates.split(",") if r]
-    n_req = args.requests
+    plain_meshes = []
+    if plain:
+        plain_meshes = [m2s.build_sdf_acceleration(v, m2s.Topology.TriangleList(i), A.rtree_bvh())
+                        for v, i, *_ in resident]
+        dev_grid = torch.empty(256 ** 3, dtype=torch.float32, device="cuda")
+        for j, e in enumerate((64, 256)):
+            g = m2s.Grid.from_bounding_box(*boxes[j], [e, e, e])
+            plain_meshes[j].grid_device(g, S.Raycast, dev_grid[:e ** 3])
+            m2s.query_sdf(plain_meshes[j], wq[:1000])
+        torch.cuda.synchronize()
+
+    def pct(a, p):
+        return round(float(np.percentile(a, p)) * 1e3, 3) if len(a) else None
+
+    def summary(lat, work, span):
+        allv = np.array(sum(lat.values(), []))
+        return {"span_s": round(span, 3), "achieved_rps": round(n_req / span, 1),
+                "p50_ms": pct(allv, 50), "p99_ms": pct(allv, 99),
+                "cells_per_s": work["grid"] / span, "points_per_s": work["points"] / span,
+                "points": {"n": len(lat["points"]), "p50_ms": pct(lat["points"], 50), "p99_ms": pct(lat["points"], 99)},
+                "grid": {"n": len(lat["grid"]), "p50_ms": pct(lat["grid"], 50), "p99_ms": pct(lat["grid"], 99)},
+                "upload": {"n": len(lat["upload"]), "p50_ms": pct(lat["upload"], 50),
+                           "p99_ms": pct(lat["upload"], 99)}}
+
     lines = []
     fresh_next = 0
     for rate in rates:
@@ -782,7 +1043,8 @@ def serving_workload(args):
                 reqs.append(("grid", j, e, out_elems))
                 out_elems += e ** 3
             else:
-                reqs.append(("upload", j, 0, out_elems))
+                reqs.append(("upload", fresh_next % len(fresh), 0, out_elems))
+                fresh_next += 1
         out = torch.empty(out_elems, dtype=torch.float32).pin_memory()
         outn = out.numpy()
         # per-request query arrays: the pinned unit cube scaled into the mesh's box
@@ -791,6 +1053,7 @@ def serving_workload(args):
             if kind == "points":
                 lo, hi = boxes[j]
                 qbufs[r_] = (unit[:n] * torch.from_numpy(hi - lo) + torch.from_numpy(lo)).pin_memory().numpy()
+        # ---- served: submissions at the arrival times, completions as the server records them
         tickets = []
         t0 = time.perf_counter()
         for r_, (kind, j, n, o) in enumerate(reqs):
@@ -800,12 +1063,10 @@ def serving_workload(args):
             if kind == "points":
                 tickets.append((kind, n, srv.submit_points(ids[j], qbufs[r_], outn[o:o + n])))
             elif kind == "grid":
-                lo, hi = boxes[j]
-                g = m2s.Grid.from_bounding_box(lo, hi, [n, n, n])
+                g = m2s.Grid.from_bounding_box(*boxes[j], [n, n, n])
                 tickets.append((kind, n ** 3, srv.submit_grid(ids[j], g, S.Raycast, outn[o:o + n ** 3])))
             else:
-                v, i = fresh[fresh_next % len(fresh)][:2]
-                fresh_next += 1
+                v, i = fresh[j][:2]
                 mid, t = srv.submit_upload(v, m2s.Topology.TriangleList(i), A.rtree_bvh())
                 tickets.append((kind, len(i) // 3, t))
         lat = {"points": [], "grid": [], "upload": []}
@@ -815,26 +1076,44 @@ def serving_workload(args):
             assert st == 0, (kind, st)
             lat[kind].append(l)
             work[kind] += n
-        span = time.perf_counter() - t0
-        allv = np.array(sum(lat.values(), []))
-
-        def pct(a, p):
-            return round(float(np.percentile(a, p)) * 1e3, 3) if len(a) else None
-
-        lines.append({"rate_rps": rate, "requests": n_req, "span_s": round(span, 3),
-                      "achieved_rps": round(n_req / span, 1),
-                      "p50_ms": pct(allv, 50), "p99_ms": pct(allv, 99),
-                      "points": {"n": len(lat["points"]), "p50_ms": pct(lat["points"], 50),
-                                 "p99_ms": pct(lat["points"], 99), "points_per_s": work["points"] / span},
-                      "grid": {"n": len(lat["grid"]), "p50_ms": pct(lat["grid"], 50),
-                               "p99_ms": pct(lat["grid"], 99), "cells_per_s": work["grid"] / span},
-                      "upload": {"n": len(lat["upload"]), "p50_ms": pct(lat["upload"], 50),
-                                 "p99_ms": pct(lat["upload"], 99)}})
+        entry = {"rate_rps": rate, "requests": n_req, "served": summary(lat, work, time.perf_counter() - t0)}
+        # ---- plain: the same arrivals, one call per request, in arrival order on one thread
+        if plain:
+            lat = {"points": [], "grid": [], "upload": []}
+            work = {"points": 0, "grid": 0, "upload": 0}
+            t0 = time.perf_counter()
+            for r_, (kind, j, n, o) in enumerate(reqs):
+                arrive = t0 + arrivals[r_]
+                wait = arrive - time.perf_counter()
+                if wait > 0:
+                    time.sleep(wait)
+                if kind == "points":
+                    outn[o:o + n] = m2s.query_sdf(plain_meshes[j], qbufs[r_])
+                    work["points"] += n
+                elif kind == "grid":
+                    g = m2s.Grid.from_bounding_box(*boxes[j], [n, n, n])
+                    plain_meshes[j].grid_device(g, S.Raycast, dev_grid[:n ** 3])
+                    out[o:o + n ** 3].copy_(dev_grid[:n ** 3])
+                    work["grid"] += n ** 3
+                else:
+                    v, i = fresh[j][:2]
+                    m2s.build_sdf_acceleration(v, m2s.Topology.TriangleList(i), A.rtree_bvh()).close()
+                lat[kind].append(time.perf_counter() - arrive)
+            entry["plain"] = summary(lat, work, time.perf_counter() - t0)
+            entry["served_over_plain_cells_per_s"] = (entry["served"]["cells_per_s"] /
+                                                      max(entry["plain"]["cells_per_s"], 1e-9))
+        lines.append(entry)
     stats = srv.stats()
     srv.close()
-    print(json.dumps({"workload": "c5_serving", "budget_bytes": 120 * 10**9, "resident_meshes": 64,
-                      "mix": {"upload": 0.05, "points": 0.57, "grid": 0.38}, "sweep": lines,
-                      "server_stats": stats}), flush=True)
+    for m in plain_meshes:
+        m.close()
+    return {"workload": "c5_serving", "budget_bytes": 120 * 10**9, "resident_meshes": 64,
+            "mix": {"upload": 0.05, "points": 0.57, "grid": 0.38}, "sweep": lines, "server_stats": stats}
+
+
+def serving_workload(args):
+    rates = [float(r) for r in args.rates.split(",") if r]
+    print(json.dumps(serving_entry(rates, args.requests, not args.no_cpu_baseline)), flush=True)
 
 
 def small_case(edge=128, points=100_000):

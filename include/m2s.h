@@ -175,12 +175,15 @@ void m2s_clear_grid_autotune(void);
  * many states run on one block with block barriers only (0 = never, negative
  * = the default 64, at most 64). */
 void m2s_set_grid_tuning(int blocks_per_sm, uint32_t cells_per_block, uint64_t wave_cells, int solo_max);
-/* Process-wide (no counterpart in the reference): with enable != 0 (the
- * default) grid propagation drops, before their closest-point evaluation, the
- * proposals that a per-triangle distance bound (the triangle's plane and edge
- * lines, with a slack far above f32 rounding) proves cannot beat the cell's
- * value; 0 keeps only the same-triangle test.  Results are identical either
- * way; the switch exists so that tests can show it. */
+/* Process-wide (no counterpart in the reference): with enable != 0, grid
+ * propagation runs its filtered kernel variant, which drops, before their
+ * closest-point evaluation, the proposals that a per-triangle distance bound
+ * (the triangle's plane and edge lines, with a slack far above f32 rounding)
+ * proves cannot beat the cell's value (on the star s6 256^3 grid: half of
+ * them); 0 (the default) runs the plain variant.  Results are identical
+ * either way.  The propagation is bound by dependent memory trips, not by
+ * the evaluations, so the filter pays only on some inputs (the star s6 Normal
+ * grid 13.9 -> 13.3 ms; the Raycast grid and the terrain slightly slower). */
 void m2s_set_grid_bound_filter(int enable);
 
 /* generate_sdf with AccelerationMethod::None for callers that cannot allocate
@@ -192,7 +195,8 @@ void m2s_set_grid_bound_filter(int enable);
  * risk the device-wide synchronisation an allocation may cause, and
  * applications that have already given their whole device-memory budget to
  * their own pool.  Limits: at most 262,144 triangles (more returns
- * M2S_ERR_INVALID_ARGUMENT); the array is held by every device that loads the
+ * M2S_ERR_INVALID_ARGUMENT); devices 0..63 only (a higher current device
+ * returns M2S_ERR_INVALID_ARGUMENT); the array is held by every device that loads the
  * library until the process exits; all calls share it, so calls that overlap
  * on the GPU race and must be serialised by the caller.  The first call on a
  * device looks up the array's address with that device current — make it
@@ -207,12 +211,14 @@ int m2s_generate_sdf_none_noalloc(const float* d_vertices, uint64_t n_vertices,
 
 /* The crate's resident API (build_sdf_acceleration / query_sdf, lib.rs:410-485)
  * answers one call at a time on the caller's thread.  A server owns resident
- * meshes and three worker threads (uploads, point requests, grid requests)
+ * meshes and worker threads (uploads, point requests, and two grid lanes)
  * and admits requests against a device-memory budget: each reserves an
  * estimate of what it will hold and waits, in arrival order per kind, until
  * that fits.  Point requests on different meshes overlap on a pool of
- * `point_streams` streams (0 = 4); grid requests that wait together are
- * computed as one batch.  Every result equals the one the single-request
+ * `point_streams` streams (0 = 4); a free grid lane takes the grid requests
+ * waiting at that moment (up to 4M cells) as one wave, so a request is
+ * admitted at the next wave boundary, and the two lanes' waves run side by
+ * side.  Every result equals the one the single-request
  * calls give (m2s_query_sdf with the mesh's method; m2s_grid_sdf_device).
  * Submissions return a ticket at once; the caller's host buffers (queries,
  * outputs) must stay valid until m2s_server_wait returns for that ticket.
@@ -242,8 +248,8 @@ int m2s_server_wait(m2s_server* server, uint64_t ticket, double timeout_s, int* 
                     double* latency_s);
 /* Frees a resident mesh that no queued or running request uses. */
 int m2s_server_remove_mesh(m2s_server* server, uint32_t mesh_id);
-/* [uploads, point requests, grid requests completed; failed; grid batches;
- *  grid requests batched; largest batch; reserved bytes; peak reserved bytes;
+/* [uploads, point requests, grid requests completed; failed; grid waves;
+ *  grid requests in waves; most requests in one wave; reserved bytes; peak reserved bytes;
  *  resident meshes; queued requests; evicted meshes]. */
 int m2s_server_stats(m2s_server* server, uint64_t out[12]);
 
@@ -303,6 +309,24 @@ int m2s_last_grid_stats(uint64_t out[10]);
  * distance bound (m2s_set_grid_bound_filter)]; the rest were evaluated. */
 int m2s_last_grid_filter_stats(uint64_t out[2]);
 
+/* FP64 audit (no counterpart in the reference; a report, never a change of
+ * output).  Results are the reference's f32 arithmetic, decision for
+ * decision.  With enable != 0 (process-wide), grid calls and point queries
+ * also check every aligned ray test (geo.rs:165-216) and the Voronoi-region
+ * choice behind each result (geo.rs:97-128) against a forward-error bound of
+ * the f32 arithmetic, and re-decide in FP64, on the device, only those whose
+ * compared quantity lies within the bound.  Point queries run their counting
+ * kernels then (as with m2s_set_profiling) and synchronise their stream.
+ * m2s_last_grid_audit / m2s_last_query_audit read the last call's counts on
+ * this thread: [ray tests, ambiguous ray tests, ray tests FP64 decides the
+ * other way, cells / queries whose 2-of-3 vote the FP64 decisions flip,
+ * cells / queries whose nearest triangle's region was audited (proper
+ * triangles), ambiguous region choices, region choices FP64 makes
+ * otherwise].  Point counts cover the LBVH methods (Bvh, Rtree, RtreeBvh). */
+void m2s_set_fp64_audit(int enable);
+int m2s_last_grid_audit(uint64_t out[7]);
+int m2s_last_query_audit(uint64_t out[7]);
+
 /* When enabled (per thread), grid calls time their phases with CUDA events on
  * their stream — the points the crate logs at generate/grid.rs:303-307,
  * 342-346 and 369-373 — readable with m2s_last_grid_phase_ms as
@@ -351,12 +375,22 @@ uint32_t m2s_query_budget(void);
  * mesh's LBVH query on the caller's device queries d_q[0..nq) with each
  * base budget of {0, 256, 512, 768, 1024, 1536, 2048, 4096} (see
  * m2s_set_query_budget: where a query moves from one thread to one warp,
- * scaled down for batches under 2^20 queries) and sets the fastest.  Results do not depend on the budget.  out_budget (may be
- * NULL) receives the choice, out_ms (may be NULL, 8 entries) each
- * candidate's time.  Synchronous; meshes built with AccelerationMethod::None
- * have no traversal to tune (M2S_ERR_INVALID_ARGUMENT). */
+ * scaled down for batches under 2^20 queries) and sets the fastest.  Results
+ * do not depend on the budget.  Candidates are timed on this call alone:
+ * queries running meanwhile on other threads keep the current budget, and if
+ * another thread sets a budget while the tuner runs, that setting stands and
+ * the tuner's choice is not published.  out_budget (may be NULL) receives the
+ * choice, out_ms (may be NULL, 8 entries) each candidate's time.  Synchronous;
+ * meshes built with AccelerationMethod::None have no traversal to tune
+ * (M2S_ERR_INVALID_ARGUMENT). */
 int m2s_query_autotune(const m2s_mesh* mesh, const float* d_q, uint64_t nq, void* stream, uint32_t* out_budget,
                        float out_ms[8]);
+
+/* Diagnostics (no counterpart in the reference): [bytes in use, bytes
+ * reserved] of this library's device-memory pool on the current device (both
+ * 0 before the library's first allocation there).  Every allocating entry
+ * point draws its workspace from this pool. */
+int m2s_pool_usage(uint64_t out[2]);
 
 const char* m2s_status_string(int status);
 /* Detail of the last failure on the calling thread ("" if none). */

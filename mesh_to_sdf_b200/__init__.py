@@ -26,7 +26,7 @@ __all__ = [
     "SignMethod", "AccelerationMethod", "Topology", "Grid", "SnapResult", "SdfAccelerationMesh", "M2SError",
     "generate_sdf", "generate_grid_sdf", "build_sdf_acceleration", "query_sdf",
     "query_vector_to_closest_point_rtree_bvh", "ALL_SDF_ACCELERATION_METHODS", "device_available",
-    "grid_sdf_batch_device", "GridPlan", "grid_offsets", "set_grid_tuning", "set_grid_bound_filter", "clear_grid_autotune", "Server",
+    "grid_sdf_batch_device", "GridPlan", "grid_offsets", "set_grid_tuning", "set_grid_bound_filter", "set_fp64_audit", "last_grid_audit", "last_query_audit", "clear_grid_autotune", "Server",
     "sort_cells_by_distance", "sort_cells_by_distance_device", "check_mesh_triangle_list",
 ]
 
@@ -296,11 +296,36 @@ def last_grid_stats():
     return d
 
 
+AUDIT_STATS = ("ray_tests", "ray_ambiguous", "ray_fp64_disagrees", "vote_flips", "regions", "region_ambiguous",
+               "region_fp64_disagrees")
+
+
+def set_fp64_audit(enable: bool):
+    """Process-wide: audit every f32 ray test and Voronoi-region choice against
+    a forward-error bound and re-decide the ambiguous ones in FP64 on the
+    device (counts only; results do not change).  See last_grid_audit() and
+    last_query_audit()."""
+    _lib.lib().m2s_set_fp64_audit(1 if enable else 0)
+
+
+def last_grid_audit():
+    """The FP64 audit counts of the last grid call on this thread (names in AUDIT_STATS)."""
+    a = np.zeros(len(AUDIT_STATS), np.uint64)
+    _lib.lib().m2s_last_grid_audit(_vp(a))
+    return dict(zip(AUDIT_STATS, (int(x) for x in a)))
+
+
+def last_query_audit():
+    """The FP64 audit counts of the last point query on this thread (names in AUDIT_STATS)."""
+    a = np.zeros(len(AUDIT_STATS), np.uint64)
+    _lib.lib().m2s_last_query_audit(_vp(a))
+    return dict(zip(AUDIT_STATS, (int(x) for x in a)))
+
+
 def set_grid_bound_filter(enable: bool):
-    """Process-wide: drop grid-propagation proposals that a per-triangle
-    distance bound proves cannot win (the default), or evaluate every proposal
-    but those to a cell already holding the proposing triangle.  Results are
-    identical either way."""
+    """Process-wide: run grid propagation's filtered variant, which drops the
+    proposals a per-triangle distance bound proves cannot win before their
+    evaluation (off by default).  Results are identical either way."""
     _lib.lib().m2s_set_grid_bound_filter(1 if enable else 0)
 
 

@@ -42,6 +42,10 @@ SIGNATURES = {
     "m2s_set_grid_tuning": (None, [I, ctypes.c_uint32, U64, I]),
     "m2s_set_grid_bound_filter": (None, [I]),
     "m2s_last_grid_filter_stats": (I, [P]),
+    "m2s_pool_usage": (I, [P]),
+    "m2s_set_fp64_audit": (None, [I]),
+    "m2s_last_grid_audit": (I, [P]),
+    "m2s_last_query_audit": (I, [P]),
     "m2s_grid_plan_waves": (ctypes.c_uint32, [P]),
     "m2s_radix_sort_pairs_device": (I, [P, P, U64, I, P]),
     "m2s_sort_cells_by_distance_device": (I, [P, U64, P, P, P]),

@@ -22,7 +22,7 @@ thread_local std::string t_last_error;
 thread_local uint64_t t_grid_stats[kGridStats];
 thread_local float t_grid_phase_ms[4];
 thread_local bool t_profile = false;
-thread_local uint64_t t_query_stats[5];
+thread_local uint64_t t_query_stats[12];
 thread_local std::vector<uint32_t> t_round_log;
 
 std::mutex g_pool_mu;
@@ -180,8 +180,8 @@ float* grid_phase_slot() { return t_profile ? t_grid_phase_ms : nullptr; }
 
 bool profiling_enabled() { return t_profile; }
 
-void record_query_stats(const uint64_t stats[5]) {
-  for (int i = 0; i < 5; ++i) t_query_stats[i] = stats[i];
+void record_query_stats(const uint64_t stats[12]) {
+  for (int i = 0; i < 12; ++i) t_query_stats[i] = stats[i];
 }
 
 void record_round_log(const std::vector<uint32_t>& log) { t_round_log = log; }
@@ -252,6 +252,31 @@ uint32_t m2s_query_budget(void) { return g_query_budget; }
 int m2s_last_grid_stats(uint64_t out[10]) {
   if (!out) return M2S_ERR_INVALID_ARGUMENT;
   for (int i = 0; i < 10; ++i) out[i] = t_grid_stats[i];
+  return M2S_OK;
+}
+
+int m2s_pool_usage(uint64_t out[2]) {
+  if (!out) return M2S_ERR_INVALID_ARGUMENT;
+  out[0] = out[1] = 0;
+  int dev = 0;
+  M2S_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return M2S_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (!g_pool_ready[dev]) return M2S_OK;  // nothing allocated on this device yet
+  M2S_CUDA(cudaMemPoolGetAttribute(g_pools[dev], cudaMemPoolAttrUsedMemCurrent, &out[0]));
+  M2S_CUDA(cudaMemPoolGetAttribute(g_pools[dev], cudaMemPoolAttrReservedMemCurrent, &out[1]));
+  return M2S_OK;
+}
+
+int m2s_last_query_audit(uint64_t out[7]) {
+  if (!out) return M2S_ERR_INVALID_ARGUMENT;
+  for (int i = 0; i < 7; ++i) out[i] = t_query_stats[5 + i];
+  return M2S_OK;
+}
+
+int m2s_last_grid_audit(uint64_t out[7]) {
+  if (!out) return M2S_ERR_INVALID_ARGUMENT;
+  for (int i = 0; i < 7; ++i) out[i] = t_grid_stats[12 + i];
   return M2S_OK;
 }
 
@@ -470,17 +495,19 @@ int m2s_query_autotune(const m2s_mesh* mesh, const float* d_q, uint64_t nq, void
   cudaEvent_t e0, e1;
   M2S_CUDA(cudaEventCreate(&e0));
   M2S_CUDA(cudaEventCreate(&e1));
-  const uint32_t saved = g_query_budget;
+  // Candidates are passed to each timed call, never published while timing:
+  // concurrent queries keep the current budget, and a budget set by another
+  // thread meanwhile wins over the result below.
+  uint32_t saved = g_query_budget.load();
   float best_ms = INFINITY;
   uint32_t best = saved;
   for (int c = 0; c < kQueryBudgetCandidates && !st; ++c) {
-    g_query_budget = kQueryBudgets[c];
     float ms = INFINITY;
     // one warm-up, then the faster of two timed runs
     for (int rep = 0; rep < 3 && !st; ++rep) {
       if (rep && cudaEventRecord(e0, s) != cudaSuccess) st = M2S_ERR_CUDA;
       if (!st) st = query_points(mesh->mesh.view(), mesh->accel, mesh->sign, d_q, nq, out.p, nullptr, nullptr,
-                                 status.p, s);
+                                 status.p, s, kQueryBudgets[c]);
       if (!st && rep) {
         float t = 0.0f;
         if (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
@@ -497,8 +524,8 @@ int m2s_query_autotune(const m2s_mesh* mesh, const float* d_q, uint64_t nq, void
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  g_query_budget = st ? saved : best;
-  if (out_budget) *out_budget = g_query_budget;
+  if (!st) g_query_budget.compare_exchange_strong(saved, best);  // unless it was set meanwhile
+  if (out_budget) *out_budget = st ? saved : best;
   return st;
 }
 

@@ -147,6 +147,7 @@ struct m2s_grid_plan {
         sum[9] = std::max<uint64_t>(sum[9], info.max_list);
         sum[10] += info.filter_same;
         sum[11] += info.filter_bound;
+        for (int a = 0; a < 7; ++a) sum[12 + a] += info.audit[a];
         if (!info.overflow) continue;
         if (attempt >= 6 || j->capacity() >= 0x40000000u) {
           set_error("grid propagation lists overflowed at the largest capacity");
@@ -349,6 +350,12 @@ void m2s_set_grid_tuning(int blocks_per_sm, uint32_t cells_per_block, uint64_t w
   t.cells_per_block = cells_per_block ? cells_per_block : 1024;
   t.wave_cells = wave_cells ? wave_cells : (1ull << 26);
   t.solo_max = solo_max < 0 ? 64u : (uint32_t)solo_max;
+  set_grid_tuning(t);
+}
+
+void m2s_set_fp64_audit(int enable) {
+  GridTuning t = grid_tuning();
+  t.fp64_audit = enable != 0;
   set_grid_tuning(t);
 }
 

@@ -45,6 +45,7 @@
 #include <mutex>
 #include <vector>
 
+#include "m2s_audit.cuh"
 #include "m2s_internal.cuh"
 
 namespace m2s {
@@ -58,6 +59,7 @@ constexpr int kFar0 = kRing + 1;    // far lists kFar0 and kFar0 + 1 (ping-pong)
 constexpr int kLists = kRing + 3;
 constexpr uint32_t kNoBucket = 0xFFFFFFFFu;
 constexpr uint32_t kMaxSteps = 1u << 22;  // bound on rounds + redistributions
+constexpr int kAuditStats = 7;
 
 // Unsigned 32-bit division by an invariant divisor with a multiply-high and
 // two shifts (Granlund & Montgomery, "Division by invariant integers using
@@ -182,6 +184,10 @@ struct PropState {
   unsigned long long entries, evals, seeds, ray_hits;
   unsigned long long filter_same;   // proposals dropped: the neighbour holds the proposing triangle
   unsigned long long filter_bound;  // proposals dropped by the distance bound
+  // FP64 audit (GridTuning::fp64_audit): ray tests, ambiguous, FP64 decides
+  // otherwise; cells whose 2-of-3 vote the FP64 decisions flip; cells whose
+  // region was audited (proper triangles), ambiguous, FP64 picks another.
+  unsigned long long audit[kAuditStats];
 };
 
 __device__ __forceinline__ P3 center(const GridK& g, int x, int y, int z) {
@@ -606,6 +612,7 @@ __global__ void k_barrier_probe(GridBarrier* bar, unsigned int expected, unsigne
 constexpr int kTouchStage = 6144;
 constexpr int kUnroll = 2;  // proposals per thread in flight
 
+
 enum { kRelax = 0, kRedistribute = 1, kDone = 2, kLimit = 3 };
 
 // Next step of the schedule, computed by warp 0 of every block from the
@@ -830,96 +837,45 @@ __device__ __forceinline__ void relax_commit_solo(const GridSet& gs, unsigned lo
 
 // Propose phase of a relax round over list[0..n): every state offers its
 // triangle to the 26 cells around it (its own cell holds that triangle's
-// distance or a better one, so it never gains).  Proposals t0, t0 + T, ...
-// advance as (state e, neighbour k) pairs without division: T = 26 * dE + dK;
-// consecutive threads share a state, so its entry and triangle loads are warp
-// broadcasts.
+// distance or a better one, so it never gains).  Results do not depend on
+// how proposals are shared out or ordered, nor on the filter below.
 //
 // With the filter (the default), a proposal is dropped unevaluated when the
 // neighbour already holds the same triangle (the distance of a (cell,
 // triangle) pair is one deterministic value, so it cannot gain) or when the
-// triangle's distance bound proves it cannot beat the snapshot; each warp
-// queues the rest in shared memory and evaluates them 32 at a time with every
-// lane busy.  Without it, Raycast proposals are evaluated where they arise,
-// kUnroll per thread at a time, and Normal ones pass the same-triangle test
-// and the queue only.  Results do not depend on the filter or on the order of
-// proposals.
-template <int SIGN, bool MULTI>
+// triangle's distance bound proves that it cannot beat the snapshot; each
+// warp queues the rest in shared memory and evaluates them 32 at a time with
+// every lane busy.  The work unit is a row: state e and a (dx, dy) offset, the
+// three neighbours at z - 1, z, z + 1 (nine rows per state; the state's own
+// cell is left out of its row).  A row's three snapshot keys are adjacent, so
+// a thread issues their loads together and they share a memory sector; the
+// bound's plane values are formed once at the row's middle cell and moved
+// along z by one addition each (the slack covers that rounding); only a
+// survivor's exact cell centre is computed.  Units t0, t0 + T, ... advance as
+// (state, row) pairs without division: T = 9 * dE + dR.
+//
+// Without the filter, proposals are single (state, neighbour) pairs, T =
+// 26 * dE + dK: Raycast proposals are evaluated where they arise, kUnroll per
+// thread at a time, and Normal ones pass the same-triangle test and the queue.
+template <int SIGN, bool MULTI, bool FILTER>
 __device__ __forceinline__ void relax_propose(const GridSet& gs, const TriRec* __restrict__ tris,
                                               const TriBound* __restrict__ bounds, const float* __restrict__ slack,
-                                              bool filter, const unsigned long long* snap_keys,
+                                              const unsigned long long* snap_keys,
                                               unsigned long long* work_keys, const uint2* list, uint32_t n,
                                               uint32_t T, uint32_t t0, uint32_t* s_touch, uint32_t* s_ntouch,
                                               PropState* st, uint32_t parity, uint32_t* spill, uint32_t cap,
                                               bool& nan, unsigned long long& evals, uint32_t& dropped_same,
                                               uint32_t& dropped_bound, WarpQueue* q) {
-  const uint32_t dE = T / 26u, dK = T % 26u;
-  uint32_t e = t0 / 26u, k = t0 % 26u;
-  // The neighbour of state e for proposal k: false when it lies off the grid.
-  auto neighbour = [&](uint32_t eu, uint32_t kk, uint32_t& tri, uint32_t& j, int& X, int& Y, int& Z) {
-    const uint2 ent = __ldcg(&list[eu]);  // written by other blocks in earlier rounds
-    tri = ent.y;
-    return neighbour_cell<MULTI>(gs, ent, kk, j, X, Y, Z);
-  };
-  auto step = [&]() {
-    k += dK;
-    e += dE;
-    if (k >= 26u) {
-      k -= 26u;
-      ++e;
-    }
-  };
-  if (SIGN == M2S_SIGN_RAYCAST && !filter) {
-    while (e < n) {
-      bool first[kUnroll];
-      uint32_t jj[kUnroll];
-#pragma unroll
-      for (int u = 0; u < kUnroll; ++u) {
-        first[u] = false;
-        jj[u] = 0;
-        const uint32_t eu = e, ku = k;
-        step();
-        uint32_t tri, j;
-        int X, Y, Z;
-        if (eu >= n || !neighbour(eu, ku, tri, j, X, Y, Z)) continue;
-        ++evals;
-        const P3 pos = center(grid_of_tri<MULTI>(gs, tri), X, Y, Z);
-        first[u] = propose_at<SIGN>(tris[tri], tri, j, pos, __ldcg(&snap_keys[j]), work_keys, nan);
-        jj[u] = j;
-      }
-#pragma unroll
-      for (int u = 0; u < kUnroll; ++u)
-        if (first[u]) stage_touch(jj[u], s_touch, s_ntouch, st, parity, spill, cap);
-    }
-    return;
-  }
   const uint32_t lane = threadIdx.x & 31u;
-  uint32_t qn = 0;  // warp-uniform queue length, < 32 between iterations
+  uint32_t qn = 0;  // warp-uniform queue length, < 32 between pushes
   auto run = [&](uint32_t i) {
     const uint32_t tri = q->tri[i], j = q->j[i];
     if (propose_at<SIGN>(tris[tri], tri, j, P3{q->px[i], q->py[i], q->pz[i]}, q->snap[i], work_keys, nan))
       stage_touch(j, s_touch, s_ntouch, st, parity, spill, cap);
   };
-  while (__any_sync(0xFFFFFFFFu, e < n)) {
-    const uint32_t eu = e, ku = k;
-    step();
-    uint32_t tri = 0, j = 0;
-    int X = 0, Y = 0, Z = 0;
-    P3 pos{0.f, 0.f, 0.f};
-    unsigned long long snap = 0;
-    bool keep = false;
-    if (eu < n && neighbour(eu, ku, tri, j, X, Y, Z)) {
-      ++evals;
-      snap = __ldcg(&snap_keys[j]);
-      pos = center(grid_of_tri<MULTI>(gs, tri), X, Y, Z);
-      if (key_tri(snap) == tri) {
-        ++dropped_same;
-      } else if (filter && bound_rejects<SIGN>(bounds[tri], slack[tri], pos, snap)) {
-        ++dropped_bound;
-      } else {
-        keep = true;
-      }
-    }
+  // Called by all 32 lanes: queues this lane's proposal if `keep`, and
+  // evaluates 32 queued proposals once there are that many.
+  auto queue_push = [&](bool keep, uint32_t tri, uint32_t j, P3 pos, unsigned long long snap) {
     const unsigned m = __ballot_sync(0xFFFFFFFFu, keep);
     if (keep) {
       const uint32_t w = qn + __popc(m & ((1u << lane) - 1u));  // qn + 31 at most
@@ -934,8 +890,147 @@ __device__ __forceinline__ void relax_propose(const GridSet& gs, const TriRec* _
     if (qn >= 32u) {
       __syncwarp();
       run(qn - 32u + lane);
-      __syncwarp();  // the slots are written again next iteration
+      __syncwarp();  // the slots are written again by the next push
       qn -= 32u;
+    }
+  };
+  if constexpr (FILTER) {
+    const uint32_t dE = T / 9u, dR = T % 9u;
+    uint32_t e = t0 / 9u, r = t0 % 9u;
+    // The entry of a thread's next unit is loaded while it works on the
+    // current one (entries were written by other blocks in earlier rounds).
+    uint2 ent_next = e < n ? __ldcg(&list[e]) : make_uint2(0u, 0u);
+    while (__any_sync(0xFFFFFFFFu, e < n)) {
+      const uint32_t eu = e, ru = r;
+      const uint2 ent = ent_next;
+      r += dR;
+      e += dE;
+      if (r >= 9u) {
+        r -= 9u;
+        ++e;
+      }
+      if (e < n) ent_next = __ldcg(&list[e]);
+      bool on[3] = {false, false, false};
+      uint32_t tri = 0, j0 = 0;
+      int X = 0, Y = 0, z = 0;
+      unsigned long long snap[3] = {0ull, 0ull, 0ull};
+      const GridK* gp = nullptr;
+      if (eu < n) {
+        tri = ent.y;
+        const GridK& g = grid_of_tri<MULTI>(gs, tri);
+        gp = &g;
+        int x, y;
+        cell_coords(g, ent.x - g.cell_off, &x, &y, &z);
+        X = x + (int)(ru / 3u) - 1;  // iproduct order (grid.rs:512): x outermost
+        Y = y + (int)(ru % 3u) - 1;
+        if ((unsigned)X < (unsigned)g.n[0] && (unsigned)Y < (unsigned)g.n[1]) {
+          j0 = g.cell_off + local_index(g, X, Y, z);
+          on[0] = z > 0;
+          on[1] = ru != 4u;  // the state's own cell
+          on[2] = z + 1 < g.n[2];
+#pragma unroll
+          for (int d = 0; d < 3; ++d)
+            if (on[d]) snap[d] = __ldcg(&snap_keys[j0 + d - 1]);
+        }
+      }
+      bool keep[3] = {false, false, false};
+      if (on[0] || on[1] || on[2]) {
+        const GridK& g = *gp;
+        const TriBound tb = bounds[tri];
+        const float sl = slack[tri];
+        // the bound's plane values at the row's middle cell, and their step along z
+        const P3 pc = center(g, X, Y, z);
+        const float fh = fmaf(tb.n.x, pc.x, fmaf(tb.n.y, pc.y, fmaf(tb.n.z, pc.z, -tb.n.w)));
+        const float f0 = fmaf(tb.e0.x, pc.x, fmaf(tb.e0.y, pc.y, fmaf(tb.e0.z, pc.z, -tb.e0.w)));
+        const float f1 = fmaf(tb.e1.x, pc.x, fmaf(tb.e1.y, pc.y, fmaf(tb.e1.z, pc.z, -tb.e1.w)));
+        const float f2 = fmaf(tb.e2.x, pc.x, fmaf(tb.e2.y, pc.y, fmaf(tb.e2.z, pc.z, -tb.e2.w)));
+        const float sz = g.s[2];
+        const float ph = tb.n.z * sz, p0 = tb.e0.z * sz, p1 = tb.e1.z * sz, p2 = tb.e2.z * sz;
+        const float pm = fmaxf(fmaxf(fabsf(pc.x), fabsf(pc.y)), fabsf(pc.z)) + fabsf(sz);
+        const float base = fmaf((float)kBoundAbs, pm, sl) + (SIGN == M2S_SIGN_NORMAL ? 1e-6f : 0.0f);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          if (!on[d]) continue;
+          ++evals;
+          if (key_tri(snap[d]) == tri) {
+            ++dropped_same;
+            continue;
+          }
+          const float sd = (float)(d - 1);
+          const float h = fmaf(sd, ph, fh);
+          const float o = fmaxf(0.0f, -fminf(fmaf(sd, p0, f0), fminf(fmaf(sd, p1, f1), fmaf(sd, p2, f2))));
+          const float thr = fmaf(fabsf(key_dist(snap[d])), 1.0f + kBoundRel, base);
+          if (fmaf(h, h, o * o) > thr * thr) {  // false when thr is infinite or anything is NaN
+            ++dropped_bound;
+            continue;
+          }
+          keep[d] = true;
+        }
+      }
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        P3 pos{0.f, 0.f, 0.f};
+        if (keep[d]) pos = center(*gp, X, Y, z + d - 1);
+        queue_push(keep[d], tri, j0 + d - 1, pos, snap[d]);
+      }
+    }
+  } else {
+    const uint32_t dE = T / 26u, dK = T % 26u;
+    uint32_t e = t0 / 26u, k = t0 % 26u;
+    // The neighbour of state e for proposal k: false when it lies off the grid.
+    auto neighbour = [&](uint32_t eu, uint32_t kk, uint32_t& tri, uint32_t& j, int& X, int& Y, int& Z) {
+      const uint2 ent = __ldcg(&list[eu]);  // written by other blocks in earlier rounds
+      tri = ent.y;
+      return neighbour_cell<MULTI>(gs, ent, kk, j, X, Y, Z);
+    };
+    auto step = [&]() {
+      k += dK;
+      e += dE;
+      if (k >= 26u) {
+        k -= 26u;
+        ++e;
+      }
+    };
+    if (SIGN == M2S_SIGN_RAYCAST) {
+      while (e < n) {
+        bool first[kUnroll];
+        uint32_t jj[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+          first[u] = false;
+          jj[u] = 0;
+          const uint32_t eu = e, ku = k;
+          step();
+          uint32_t tri, j;
+          int X, Y, Z;
+          if (eu >= n || !neighbour(eu, ku, tri, j, X, Y, Z)) continue;
+          ++evals;
+          const P3 pos = center(grid_of_tri<MULTI>(gs, tri), X, Y, Z);
+          first[u] = propose_at<SIGN>(tris[tri], tri, j, pos, __ldcg(&snap_keys[j]), work_keys, nan);
+          jj[u] = j;
+        }
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u)
+          if (first[u]) stage_touch(jj[u], s_touch, s_ntouch, st, parity, spill, cap);
+      }
+      return;
+    }
+    while (__any_sync(0xFFFFFFFFu, e < n)) {
+      const uint32_t eu = e, ku = k;
+      step();
+      uint32_t tri = 0, j = 0;
+      int X = 0, Y = 0, Z = 0;
+      P3 pos{0.f, 0.f, 0.f};
+      unsigned long long snap = 0;
+      bool keep = false;
+      if (eu < n && neighbour(eu, ku, tri, j, X, Y, Z)) {
+        ++evals;
+        snap = __ldcg(&snap_keys[j]);
+        pos = center(grid_of_tri<MULTI>(gs, tri), X, Y, Z);
+        if (key_tri(snap) == tri) ++dropped_same;
+        else keep = true;
+      }
+      queue_push(keep, tri, j, pos, snap);
     }
   }
   __syncwarp();
@@ -980,18 +1075,22 @@ __device__ __forceinline__ void relax_commit(const GridSet& gs, unsigned long lo
   }
 }
 
-template <int SIGN, bool MULTI>
-__global__ void __launch_bounds__(256, 4) k_propagate(const __grid_constant__ GridSet gs, const TriRec* __restrict__ tris,
+// The kernel exists without and with the proposal filter (FILTER): without,
+// 4 blocks of 256 threads fit per SM (64 registers a thread); the filtered
+// propose loop needs about 80 registers, so that variant runs 3 per SM.
+template <int SIGN, bool MULTI, bool FILTER>
+__global__ void __launch_bounds__(256, FILTER ? 3 : 4) k_propagate(const __grid_constant__ GridSet gs, const TriRec* __restrict__ tris,
                                                    unsigned long long* snap_keys, unsigned long long* work_keys,
                                                    uint2* lists, uint32_t cap, uint32_t* spill_lists,
                                                    PropState* st, GridBarrier* bar, uint32_t max_steps,
                                                    uint32_t* status, uint32_t* round_log, uint32_t log_cap,
                                                    uint32_t solo_max, const TriBound* __restrict__ bounds,
-                                                   const float* __restrict__ slack, uint32_t filter) {
+                                                   const float* __restrict__ slack) {
   __shared__ Sched sh;
   __shared__ __align__(16) uint32_t s_touch[kTouchStage];  // also a solo run's min table
   __shared__ uint16_t s_taken[26 * kSoloCap];              // a solo round's taken table slots
-  __shared__ WarpQueue s_queue[kWarps];
+  constexpr bool kQueued = SIGN == M2S_SIGN_NORMAL || FILTER;  // the plain Raycast loop needs no queue
+  __shared__ WarpQueue s_queue[kQueued ? kWarps : 1];
   __shared__ uint32_t s_ntouch, s_gen, s_pending, s_more, s_runs, s_solo_run;
   __shared__ uint32_t s_count[kLists], s_far_min[2], s_overflow;  // block 0's counters during a solo run
   // (built where used, so no pointer stays live across the propose loop)
@@ -1162,9 +1261,10 @@ __global__ void __launch_bounds__(256, 4) k_propagate(const __grid_constant__ Gr
       relax_propose_solo<SIGN, MULTI>(gs, tris, snap_keys, lists + (unsigned long long)sh.cur * cap, n, HJ, HK,
                                       s_taken, &s_ntouch, nan, evals, dropped_same);
     else
-      relax_propose<SIGN, MULTI>(gs, tris, bounds, slack, filter != 0u, snap_keys, work_keys,
+      relax_propose<SIGN, MULTI, FILTER>(gs, tris, bounds, slack, snap_keys, work_keys,
                                  lists + (unsigned long long)sh.cur * cap, n, T, t0, s_touch, &s_ntouch, st, parity,
-                                 spill, cap, nan, evals, dropped_same, dropped_bound, &s_queue[threadIdx.x >> 5]);
+                                 spill, cap, nan, evals, dropped_same, dropped_bound,
+                                         &s_queue[kQueued ? threadIdx.x >> 5 : 0]);
     if (lead_block && threadIdx.x == 0) atomicAdd(&st->entries, (unsigned long long)n);
     if (solo) {
       __syncthreads();
@@ -1264,9 +1364,11 @@ __device__ __forceinline__ void lattice_range(const GridK& g, int d, float lo, f
   if (fb_ < 0.0f || fa_ > (float)(g.n[d] - 1)) *b = *a - 1;  // no lattice point in range
 }
 
-template <int AXIS, bool MULTI>
+// With AUDIT, each ray test is also audited (m2s_audit.cuh): the f32
+// decision toggles `bits` exactly as without, the FP64 one toggles `bits64`.
+template <int AXIS, bool MULTI, bool AUDIT = false>
 __global__ void k_rays(const __grid_constant__ GridSet gs, const TriRec* __restrict__ tris, uint32_t T, uint32_t* bits,
-                       PropState* st) {
+                       PropState* st, uint32_t* bits64 = nullptr) {
   constexpr int IY = (AXIS + 1) % 3, IZ = (AXIS + 2) % 3;
   const uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
@@ -1284,7 +1386,7 @@ __global__ void k_rays(const __grid_constant__ GridSet gs, const TriRec* __restr
   const long long total = (long long)nj * nk;
   uint32_t* bitsA = bits + g.bits_off[AXIS];
   const uint32_t W = g.words[AXIS];
-  uint32_t hits = 0;
+  uint32_t hits = 0, tests = 0, ambiguous = 0, disagree = 0;
   const bool small = total <= 0x7FFFFFFFll;  // 32-bit division (64-bit costs ~4x the instructions)
   for (long long q = lane; q < total; q += 32) {
     int c3[3];
@@ -1299,17 +1401,97 @@ __global__ void k_rays(const __grid_constant__ GridSet gs, const TriRec* __restr
     }
     P3 o = center(g, c3[0], c3[1], c3[2]);  // ray origin: a low-face cell centre (grid.rs:580)
     float tt;
-    if (!ray_hit_aligned<AXIS>(o, a, b, c, &tt)) continue;
+    const unsigned long long last = (unsigned long long)g.n[AXIS] - 1;
+    const unsigned long long col = column_of(g, AXIS, c3[0], c3[1], c3[2]);
+    if constexpr (AUDIT) {
+      const RayAudit ra = ray_audit<AXIS>(o, a, b, c);
+      ++tests;
+      ambiguous += ra.ambiguous;
+      disagree += ra.hit64 != ra.hit32;
+      if (ra.hit64) {  // the FP64 decision's crossing, in the FP64 parity bits
+        unsigned long long kk;
+        if (ra.hit32) {
+          kk = sat_u64(floorf(fd(ra.t32, g.s[AXIS])));
+        } else {
+          const double u = floor(ra.t64 / (double)g.s[AXIS]);
+          kk = u <= 0.0 ? 0ull : (u >= 1.8e19 ? ULLONG_MAX : (unsigned long long)u);
+        }
+        const uint32_t k = (uint32_t)(kk < last ? kk : last);
+        atomicXor(&bits64[g.bits_off[AXIS] + col * W + (k >> 5)], 1u << (k & 31));
+      }
+      if (!ra.hit32) continue;
+      tt = ra.t32;
+    } else {
+      if (!ray_hit_aligned<AXIS>(o, a, b, c, &tt)) continue;
+    }
     ++hits;
     // grid.rs:604-607
     unsigned long long kk = sat_u64(floorf(fd(tt, g.s[AXIS])));
-    unsigned long long last = (unsigned long long)g.n[AXIS] - 1;
     uint32_t k = (uint32_t)(kk < last ? kk : last);
-    unsigned long long col = column_of(g, AXIS, c3[0], c3[1], c3[2]);
     atomicXor(&bitsA[col * W + (k >> 5)], 1u << (k & 31));
   }
   for (int o = 16; o; o >>= 1) hits += __shfl_xor_sync(0xFFFFFFFFu, hits, o);
   if (lane == 0 && hits) atomicAdd(&st->ray_hits, (unsigned long long)hits);
+  if constexpr (AUDIT) {
+    for (int o = 16; o; o >>= 1) {
+      tests += __shfl_xor_sync(0xFFFFFFFFu, tests, o);
+      ambiguous += __shfl_xor_sync(0xFFFFFFFFu, ambiguous, o);
+      disagree += __shfl_xor_sync(0xFFFFFFFFu, disagree, o);
+    }
+    if (lane == 0) {
+      atomicAdd(&st->audit[0], (unsigned long long)tests);
+      atomicAdd(&st->audit[1], (unsigned long long)ambiguous);
+      atomicAdd(&st->audit[2], (unsigned long long)disagree);
+    }
+  }
+}
+
+// FP64 audit of every cell (reports only): the Voronoi region of its final
+// (cell, triangle) pair, and, for Raycast, whether the 2-of-3 vote of the
+// FP64-decided parities differs from the f32 one.
+template <int SIGN, bool MULTI>
+__global__ void k_audit_cells(const __grid_constant__ GridSet gs, const TriRec* __restrict__ tris,
+                              const unsigned long long* __restrict__ keys, const uint32_t* __restrict__ bits,
+                              const uint32_t* __restrict__ bits64, PropState* st) {
+  SegCursor<uint32_t> sc;
+  uint32_t flips = 0, audited = 0, ambiguous = 0, disagree = 0;
+  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < gs.ncell;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    const GridK& g = MULTI ? gs.table[sc.at(gs.cell_off, gs.ngrids, (uint32_t)i)] : gs.g0;
+    int x, y, z;
+    cell_coords(g, (uint32_t)i - g.cell_off, &x, &y, &z);
+    if (SIGN == M2S_SIGN_RAYCAST) {
+      uint32_t v32 = 0, v64 = 0;
+      const uint32_t c3[3] = {(uint32_t)x, (uint32_t)y, (uint32_t)z};
+      for (int a = 0; a < 3; ++a) {
+        const unsigned long long w = g.bits_off[a] + column_of(g, a, x, y, z) * g.words[a] + (c3[a] >> 5);
+        v32 += (bits[w] >> (c3[a] & 31)) & 1u;
+        v64 += (bits64[w] >> (c3[a] & 31)) & 1u;
+      }
+      flips += (v32 >= 2) != (v64 >= 2);
+    }
+    const uint32_t t = key_tri(keys[i]);
+    if (t == NO_TRI) continue;
+    const TriRec r = tris[t];
+    if (__float_as_int(r.a.w) != TRI_PROPER) continue;
+    const RegionAudit ra = region_audit(center(g, x, y, z), p3(r.a), p3(r.b), p3(r.c));
+    ++audited;
+    ambiguous += ra.ambiguous;
+    disagree += ra.region64 != ra.region32;
+  }
+  const int lane = threadIdx.x & 31;
+  for (int o = 16; o; o >>= 1) {
+    flips += __shfl_xor_sync(0xFFFFFFFFu, flips, o);
+    audited += __shfl_xor_sync(0xFFFFFFFFu, audited, o);
+    ambiguous += __shfl_xor_sync(0xFFFFFFFFu, ambiguous, o);
+    disagree += __shfl_xor_sync(0xFFFFFFFFu, disagree, o);
+  }
+  if (lane == 0) {
+    atomicAdd(&st->audit[3], (unsigned long long)flips);
+    atomicAdd(&st->audit[4], (unsigned long long)audited);
+    atomicAdd(&st->audit[5], (unsigned long long)ambiguous);
+    atomicAdd(&st->audit[6], (unsigned long long)disagree);
+  }
 }
 
 // Toggle bits -> suffix parity: bit i becomes the XOR of toggles i..n-1, i.e.
@@ -1383,8 +1565,9 @@ PropState* host_state() {
 }
 
 template <int SIGN>
-const void* propagate_kernel(bool multi) {
-  return multi ? (const void*)k_propagate<SIGN, true> : (const void*)k_propagate<SIGN, false>;
+const void* propagate_kernel(bool multi, bool filter) {
+  if (filter) return multi ? (const void*)k_propagate<SIGN, true, true> : (const void*)k_propagate<SIGN, false, true>;
+  return multi ? (const void*)k_propagate<SIGN, true, false> : (const void*)k_propagate<SIGN, false, false>;
 }
 
 }  // namespace
@@ -1418,7 +1601,9 @@ struct GridJob::Impl {
   DevBuf<uint32_t> round_log;  // profiling only
   DevBuf<TriBound> bounds;     // the proposal filter's per-triangle records
   DevBuf<float> slack;
-  bool filter = true;
+  bool filter = false;
+  bool audit = false;          // FP64 audit (reports only)
+  DevBuf<uint32_t> bits64;     // the audit's FP64-decided ray parities
 };
 
 GridJob::GridJob() : p(new Impl) {}
@@ -1444,6 +1629,15 @@ uint64_t GridJob::device_bytes() const {
   return J.comb_tris.n * sizeof(TriRec) + J.tri_grid.n * 4 + (J.snap.n + J.work.n) * 8 + J.bits.n * 4 +
          J.bounds.n * sizeof(TriBound) + J.slack.n * 4 +
          (uint64_t)kLists * J.cap * 8 + 2ull * J.cap * 4 + J.table.n * sizeof(GridK);
+}
+
+int propagate_blocks_per_sm(int sign) {
+  const bool filter = grid_tuning().bound_filter;
+  const void* kern = sign == M2S_SIGN_RAYCAST ? propagate_kernel<M2S_SIGN_RAYCAST>(true, filter)
+                                              : propagate_kernel<M2S_SIGN_NORMAL>(true, filter);
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0) != cudaSuccess) return 1;
+  return std::max(per_sm, 1);
 }
 
 uint32_t default_list_capacity(uint64_t cells) {
@@ -1560,14 +1754,16 @@ int GridJob::prepare(const MeshView* meshes, uint32_t n, const GridDesc* gds, in
       (st = J.bar.alloc(1, s)))
     return st;
   J.filter = tune.bound_filter;
+  J.audit = tune.fp64_audit;
   if (tris && ((st = J.bounds.alloc(tris, s)) || (st = J.slack.alloc(tris, s)))) return st;
   if (sign == M2S_SIGN_RAYCAST && (st = J.bits.alloc(woff, s))) return st;
+  if (sign == M2S_SIGN_RAYCAST && J.audit && (st = J.bits64.alloc(woff, s))) return st;
   J.cap = tune.list_capacity ? tune.list_capacity : default_list_capacity(N);
   J.solo_max = std::min<uint32_t>(tune.solo_max, kSoloCap);  // a solo round never spills
   // Cooperative grid: co-resident blocks, fewer for small jobs (a barrier
   // over fewer blocks is faster and a small bucket does not fill many).
-  const void* kern = sign == M2S_SIGN_RAYCAST ? propagate_kernel<M2S_SIGN_RAYCAST>(J.multi)
-                                              : propagate_kernel<M2S_SIGN_NORMAL>(J.multi);
+  const void* kern = sign == M2S_SIGN_RAYCAST ? propagate_kernel<M2S_SIGN_RAYCAST>(J.multi, J.filter)
+                                              : propagate_kernel<M2S_SIGN_NORMAL>(J.multi, J.filter);
   int dev = 0, sms = 0, per_sm = 0;
   M2S_CUDA(cudaGetDevice(&dev));
   M2S_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -1635,15 +1831,15 @@ int GridJob::enqueue(cudaStream_t s, cudaEvent_t* ev) {
     if (multi) k_collect<true><<<blocks_for(N, 256), 256, 0, s>>>(J.gs, J.snap.p, J.state.p, J.lists.p, J.cap);
     else k_collect<false><<<blocks_for(N, 256), 256, 0, s>>>(J.gs, J.snap.p, J.state.p, J.lists.p, J.cap);
     M2S_CUDA(cudaGetLastError());
-    const void* kern = raycast ? propagate_kernel<M2S_SIGN_RAYCAST>(multi) : propagate_kernel<M2S_SIGN_NORMAL>(multi);
+    const void* kern = raycast ? propagate_kernel<M2S_SIGN_RAYCAST>(multi, J.filter)
+                               : propagate_kernel<M2S_SIGN_NORMAL>(multi, J.filter);
     uint32_t max_steps = kMaxSteps;
     const TriRec* tris = J.tris;
     uint32_t* log = J.round_log.p;
     uint32_t log_cap = (uint32_t)(J.round_log.n / 2);
-    uint32_t filter = J.filter ? 1u : 0u;
     void* args[] = {&J.gs,     &tris,   &J.snap.p,  &J.work.p,    &J.lists.p, &J.cap,     &J.touched.p,
                     &J.state.p, &J.bar.p, &max_steps, &J.d_status, &log,       &log_cap, &J.solo_max,
-                    &J.bounds.p, &J.slack.p, &filter};
+                    &J.bounds.p, &J.slack.p};
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(J.coop_blocks);
     cfg.blockDim = dim3(256);
@@ -1661,9 +1857,21 @@ int GridJob::enqueue(cudaStream_t s, cudaEvent_t* ev) {
   const unsigned fb = blocks_for(N, 256, 148u * 32u);
   if (raycast) {
     M2S_CUDA(cudaMemsetAsync(J.bits.p, 0, J.ray_words * 4, s));
+    if (J.audit) M2S_CUDA(cudaMemsetAsync(J.bits64.p, 0, J.ray_words * 4, s));
     if (J.T > 0) {
       const unsigned rb = (unsigned)((J.T * 32ull + 255) / 256);
-      if (multi) {
+      uint32_t* b64 = J.bits64.p;
+      if (J.audit) {
+        if (multi) {
+          k_rays<0, true, true><<<rb, 256, 0, s>>>(J.gs, J.tris, J.T, J.bits.p, J.state.p, b64);
+          k_rays<1, true, true><<<rb, 256, 0, s>>>(J.gs, J.tris, J.T, J.bits.p, J.state.p, b64);
+          k_rays<2, true, true><<<rb, 256, 0, s>>>(J.gs, J.tris, J.T, J.bits.p, J.state.p, b64);
+        } else {
+          k_rays<0, false, true><<<rb, 256, 0, s>>>(J.gs, J.tris, J.T, J.bits.p, J.state.p, b64);
+          k_rays<1, false, true><<<rb, 256, 0, s>>>(J.gs, J.tris, J.T, J.bits.p, J.state.p, b64);
+          k_rays<2, false, true><<<rb, 256, 0, s>>>(J.gs, J.tris, J.T, J.bits.p, J.state.p, b64);
+        }
+      } else if (multi) {
         k_rays<0, true><<<rb, 256, 0, s>>>(J.gs, J.tris, J.T, J.bits.p, J.state.p);
         k_rays<1, true><<<rb, 256, 0, s>>>(J.gs, J.tris, J.T, J.bits.p, J.state.p);
         k_rays<2, true><<<rb, 256, 0, s>>>(J.gs, J.tris, J.T, J.bits.p, J.state.p);
@@ -1677,8 +1885,12 @@ int GridJob::enqueue(cudaStream_t s, cudaEvent_t* ev) {
     for (int a = 0; a < 3; ++a) {
       if (multi) k_suffix<true><<<blocks_for(J.gs.ncols[a], 256), 256, 0, s>>>(J.gs, a, J.bits.p);
       else k_suffix<false><<<blocks_for(J.gs.ncols[a], 256), 256, 0, s>>>(J.gs, a, J.bits.p);
+      if (J.audit) {
+        if (multi) k_suffix<true><<<blocks_for(J.gs.ncols[a], 256), 256, 0, s>>>(J.gs, a, J.bits64.p);
+        else k_suffix<false><<<blocks_for(J.gs.ncols[a], 256), 256, 0, s>>>(J.gs, a, J.bits64.p);
+      }
     }
-    J.launches += 3;
+    J.launches += J.audit ? 6 : 3;
     M2S_CUDA(cudaGetLastError());
     if ((st = mark(3))) return st;
     if (multi) k_finalize<M2S_SIGN_RAYCAST, true><<<fb, 256, 0, s>>>(J.gs, J.snap.p, J.bits.p, J.d_out);
@@ -1690,6 +1902,17 @@ int GridJob::enqueue(cudaStream_t s, cudaEvent_t* ev) {
   }
   M2S_CUDA(cudaGetLastError());
   ++J.launches;
+  if (J.audit) {  // reports only: the output is written already
+    if (raycast) {
+      if (multi) k_audit_cells<M2S_SIGN_RAYCAST, true><<<fb, 256, 0, s>>>(J.gs, J.tris, J.snap.p, J.bits.p, J.bits64.p, J.state.p);
+      else k_audit_cells<M2S_SIGN_RAYCAST, false><<<fb, 256, 0, s>>>(J.gs, J.tris, J.snap.p, J.bits.p, J.bits64.p, J.state.p);
+    } else {
+      if (multi) k_audit_cells<M2S_SIGN_NORMAL, true><<<fb, 256, 0, s>>>(J.gs, J.tris, J.snap.p, nullptr, nullptr, J.state.p);
+      else k_audit_cells<M2S_SIGN_NORMAL, false><<<fb, 256, 0, s>>>(J.gs, J.tris, J.snap.p, nullptr, nullptr, J.state.p);
+    }
+    M2S_CUDA(cudaGetLastError());
+    ++J.launches;
+  }
   return mark(4);
 }
 
@@ -1711,6 +1934,7 @@ int GridJob::read_state(cudaStream_t s, GridRunInfo* info) {
   info->log_n = h->log_n;
   info->filter_same = h->filter_same;
   info->filter_bound = h->filter_bound;
+  for (int k = 0; k < kAuditStats; ++k) info->audit[k] = h->audit[k];
   info->launches = J.launches;
   return M2S_OK;
 }
@@ -1754,6 +1978,7 @@ int run_grid_job(GridJob& job, cudaStream_t s, uint64_t stats[kGridStats], float
     stats[9] = info.max_list;
     stats[10] = info.filter_same;
     stats[11] = info.filter_bound;
+    for (int k = 0; k < kAuditStats; ++k) stats[12 + k] = info.audit[k];
   }
   if (phase_ms) {
     for (int i = 0; i < 4; ++i) M2S_CUDA(cudaEventElapsedTime(&phase_ms[i], ev[i], ev[i + 1]));

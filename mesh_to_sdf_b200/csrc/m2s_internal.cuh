@@ -122,8 +122,10 @@ int exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint64_t n, uint32_t* 
 
 // ---- point queries (m2s_query.cu) -------------------------------------------
 
+// budget >= 0 overrides the process-wide node budget (g_query_budget) for
+// this call only: the autotuner times candidates without publishing them.
 int query_points(const MeshView& m, int accel, int sign, const float* d_q, uint64_t nq, float* d_out,
-                 float* d_vec, uint8_t* d_inside, uint32_t* d_status, cudaStream_t s);
+                 float* d_vec, uint8_t* d_inside, uint32_t* d_status, cudaStream_t s, int64_t budget = -1);
 
 // Node visits a query may spend in the one-thread-per-query pass before it is
 // continued one warp per query (0 disables the second pass).
@@ -145,7 +147,8 @@ constexpr uint32_t kQueryBudgets[kQueryBudgetCandidates] = {0, 256, 512, 768, 10
 // [queries, search node fetches, search triangle tests, sign node fetches,
 // sign triangle tests].
 bool profiling_enabled();
-void record_query_stats(const uint64_t stats[5]);
+// [queries, the four traversal counts, the seven FP64-audit counts]
+void record_query_stats(const uint64_t stats[12]);
 
 // allow_alloc = false keeps the brute force in one pass with no scratch buffer.
 int brute_force_sdf(const MeshView& m, int sign, const float* d_q, uint64_t nq, float* d_out,
@@ -170,9 +173,13 @@ struct GridDesc {
 // ray hits, overflow restarts, kernel launches, far-list redistributions,
 // rounds relaxed by one block alone, largest list relaxed in one round,
 // proposals dropped because the neighbour holds the proposing triangle,
-// proposals dropped by the distance bound].  phase_ms (may be NULL) receives
-// device time of [seeding, propagation, rays, finalize].
-constexpr int kGridStats = 12;
+// proposals dropped by the distance bound, then the FP64 audit's seven
+// counters (zero unless GridTuning::fp64_audit): ray tests, ambiguous ray
+// tests, ray tests FP64 decides otherwise, cells whose Raycast vote the FP64
+// decisions flip, cells whose Voronoi region was audited, ambiguous region
+// choices, region choices FP64 makes otherwise].  phase_ms (may be NULL)
+// receives device time of [seeding, propagation, rays, finalize].
+constexpr int kGridStats = 19;
 int grid_sdf(const MeshView& m, const GridDesc& g, int sign, float* d_out, uint32_t* d_status, cudaStream_t s,
              uint64_t stats[kGridStats], float phase_ms[4]);
 
@@ -188,14 +195,20 @@ struct GridTuning {
   // barriers only (0: every round on every block).
   uint32_t solo_max = 64;
   // Drop proposals that a per-triangle distance bound proves cannot win
-  // before their closest-point evaluation (false: only the same-triangle test).
-  bool bound_filter = true;
+  // before their closest-point evaluation, in the filtered kernel variant
+  // (off: the plain variant; results are identical either way).
+  bool bound_filter = false;
+  // Audit every ray test and every cell's Voronoi region against an f32
+  // error bound and re-decide the ambiguous ones in FP64 (counts only; the
+  // output does not change).
+  bool fp64_audit = false;
 };
 
 struct GridRunInfo {
   bool overflow = false;
   uint64_t seeds = 0, rounds = 0, entries = 0, evals = 0, ray_hits = 0, far_phases = 0, launches = 0, solo_rounds = 0,
            max_list = 0, log_n = 0, filter_same = 0, filter_bound = 0;
+  uint64_t audit[7] = {0, 0, 0, 0, 0, 0, 0};
 };
 
 // A set of (mesh, grid) pairs computed together: one cell index space (grid k
@@ -257,6 +270,9 @@ int grid_sdf_batch(const MeshView* meshes, uint32_t n, const GridDesc* grids, in
 
 // Validates a grid description for the device path (32-bit cell indices).
 int check_grid(const GridDesc& g);
+
+// Blocks of the propagation kernel that fit on one SM (its occupancy limit).
+int propagate_blocks_per_sm(int sign);
 
 // Entries per bucket list of a job of `cells` cells (before any overflow
 // restart), and the device bytes of such a job's workspace.

@@ -28,6 +28,7 @@
 #include <algorithm>
 #include <cmath>
 #include <mutex>
+#include <string>
 
 #include "m2s_internal.cuh"
 
@@ -41,14 +42,18 @@ constexpr size_t kScratchBytes = kRecordBytes + 256;  // records, then the statu
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
 std::mutex g_mu;
-void* g_scratch_ptr[64];
+constexpr int kMaxDevices = 64;  // devices whose scratch address is remembered
+void* g_scratch_ptr[kMaxDevices];
 
 // Device address of g_scratch on the current device (looked up once per device).
 int scratch_address(void** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
-  if (dev < 0 || dev >= 64) return M2S_ERR_INVALID_ARGUMENT;
+  if (dev < 0 || dev >= kMaxDevices) {
+    set_error("m2s_generate_sdf_none_noalloc serves devices 0..63; the current device is " + std::to_string(dev));
+    return M2S_ERR_INVALID_ARGUMENT;
+  }
   std::lock_guard<std::mutex> lk(g_mu);
   if (!g_scratch_ptr[dev]) {
     void* p = nullptr;

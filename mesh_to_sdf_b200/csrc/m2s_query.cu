@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <cfloat>
 
+#include "m2s_audit.cuh"
 #include "m2s_internal.cuh"
 #include "m2s_tma.cuh"
 
@@ -250,7 +251,13 @@ struct Nearest {
 // the same for the sign step (the three axis rays, or the Normal tie band).
 struct QCount {
   uint32_t visits = 0, tests = 0, sign_visits = 0, sign_tests = 0;
+  // FP64 audit (m2s_audit.cuh): ray tests, ambiguous, FP64 decides
+  // otherwise; whether the FP64 decisions flip the query's vote; whether its
+  // nearest triangle's region was audited, ambiguous, FP64 picks another.
+  uint32_t ray_tests = 0, ray_ambiguous = 0, ray_disagree = 0, vote_flip = 0, region = 0, region_ambiguous = 0,
+           region_disagree = 0;
 };
+constexpr int kQueryCounters = 11;
 
 // Exact nearest triangle under the f32 point_triangle_distance2 (geo.rs:33-37),
 // ties to the lowest triangle index.  Boxes are padded by 1e-4 (geo.rs:4-22),
@@ -541,16 +548,28 @@ __device__ bool nearest_triangle_warp(const MeshView& m, P3 p, Nearest* io, uint
 
 // Number of triangles the +AXIS ray from o crosses (geo.rs:165-216).  A box is
 // entered when the ray's (y, z) lies inside it and its far side is ahead of o.
+// The counting (STATS) instantiation also audits every ray test and counts
+// the crossings the FP64 decisions give in *count64.
 template <int AXIS, bool STATS = false>
-__device__ uint32_t ray_crossings(const MeshView& m, P3 o, bool* overflow, QCount* qc = nullptr) {
+__device__ uint32_t ray_crossings(const MeshView& m, P3 o, bool* overflow, QCount* qc = nullptr,
+                                  uint32_t* count64 = nullptr) {
   constexpr int IY = (AXIS + 1) % 3, IZ = (AXIS + 2) % 3;
   const float oy = vget(o, IY), oz = vget(o, IZ), ox = vget(o, AXIS);
   uint32_t count = 0;
   auto test = [&](uint32_t leaf) {
-    if constexpr (STATS) ++qc->sign_tests;
     TriRec r = load_tri(m.stris, leaf);
-    float t;
-    count += ray_hit_aligned<AXIS>(o, p3(r.a), p3(r.b), p3(r.c), &t) ? 1u : 0u;
+    if constexpr (STATS) {
+      ++qc->sign_tests;
+      const RayAudit ra = ray_audit<AXIS>(o, p3(r.a), p3(r.b), p3(r.c));
+      ++qc->ray_tests;
+      qc->ray_ambiguous += ra.ambiguous;
+      qc->ray_disagree += ra.hit64 != ra.hit32;
+      count += ra.hit32 ? 1u : 0u;
+      *count64 += ra.hit64 ? 1u : 0u;
+    } else {
+      float t;
+      count += ray_hit_aligned<AXIS>(o, p3(r.a), p3(r.b), p3(r.c), &t) ? 1u : 0u;
+    }
   };
   auto inside = [&](float4 lo, float4 hi) {
     float loy = IY == 0 ? lo.x : (IY == 1 ? lo.y : lo.z), hiy = IY == 0 ? hi.x : (IY == 1 ? hi.y : hi.z);
@@ -601,9 +620,30 @@ __device__ uint32_t ray_crossings(const MeshView& m, P3 o, bool* overflow, QCoun
 // bvh.rs:293-328 / rtree_bvh.rs:163-199: inside when >= 2 of 3 axis rays are odd.
 template <bool STATS = false>
 __device__ __forceinline__ bool vote_inside(const MeshView& m, P3 p, bool* overflow, QCount* qc = nullptr) {
-  int insides = (ray_crossings<0, STATS>(m, p, overflow, qc) & 1u) + (ray_crossings<1, STATS>(m, p, overflow, qc) & 1u) +
-                (ray_crossings<2, STATS>(m, p, overflow, qc) & 1u);
+  uint32_t c64[3] = {0u, 0u, 0u};
+  int insides = (ray_crossings<0, STATS>(m, p, overflow, qc, &c64[0]) & 1u) +
+                (ray_crossings<1, STATS>(m, p, overflow, qc, &c64[1]) & 1u) +
+                (ray_crossings<2, STATS>(m, p, overflow, qc, &c64[2]) & 1u);
+  if constexpr (STATS) {
+    const int insides64 = (c64[0] & 1u) + (c64[1] & 1u) + (c64[2] & 1u);
+    qc->vote_flip += (insides > 1) != (insides64 > 1);
+  }
   return insides > 1;
+}
+
+// The counting instantiation's audit of the Voronoi region of the query's
+// nearest triangle (the closest point every method's result comes from).
+template <bool STATS>
+__device__ __forceinline__ void audit_region(const MeshView& m, P3 p, uint32_t tri, QCount* qc) {
+  if constexpr (STATS) {
+    if (tri == 0xFFFFFFFFu) return;
+    const TriRec r = load_tri(m.tris, tri);
+    if (__float_as_int(r.a.w) != TRI_PROPER) return;
+    const RegionAudit ra = region_audit(p, p3(r.a), p3(r.b), p3(r.c));
+    ++qc->region;
+    qc->region_ambiguous += ra.ambiguous;
+    qc->region_disagree += ra.region64 != ra.region32;
+  }
 }
 
 // Bvh(Normal): compare_distances over every triangle whose |signed distance|
@@ -714,6 +754,7 @@ __device__ __forceinline__ void finish_query(const MeshView& m, uint64_t i, P3 p
                                              float* out, float* vec, uint8_t* inside_out, bool* nan, bool* overflow,
                                              QCount* qc = nullptr) {
   if (nn.tri == 0xFFFFFFFFu) nn = {INFINITY, 0u, 0u};  // every distance NaN
+  audit_region<STATS>(m, p, nn.tri, qc);
   if (MODE == Q_BVH_RAYCAST) {
     // bvh.rs:283-328 / rtree_bvh.rs:156-199: unsigned distance, 3-ray vote.
     float d = fminf(F32_MAX, fsqrt(nn.d2));
@@ -740,10 +781,16 @@ __device__ __forceinline__ void finish_query(const MeshView& m, uint64_t i, P3 p
 // Adds a thread's traversal counts to qstats[0..3] (one atomic per warp).
 __device__ __forceinline__ void add_counts(const QCount& c, unsigned long long* qstats) {
   const unsigned mask = __activemask();  // lanes past the last query have left
-  const unsigned v[4] = {__reduce_add_sync(mask, c.visits), __reduce_add_sync(mask, c.tests),
-                         __reduce_add_sync(mask, c.sign_visits), __reduce_add_sync(mask, c.sign_tests)};
+  const unsigned v[kQueryCounters] = {
+      __reduce_add_sync(mask, c.visits),          __reduce_add_sync(mask, c.tests),
+      __reduce_add_sync(mask, c.sign_visits),     __reduce_add_sync(mask, c.sign_tests),
+      __reduce_add_sync(mask, c.ray_tests),       __reduce_add_sync(mask, c.ray_ambiguous),
+      __reduce_add_sync(mask, c.ray_disagree),    __reduce_add_sync(mask, c.vote_flip),
+      __reduce_add_sync(mask, c.region),          __reduce_add_sync(mask, c.region_ambiguous),
+      __reduce_add_sync(mask, c.region_disagree)};
   if ((threadIdx.x & 31) == (unsigned)(__ffs(mask) - 1))
-    for (int f = 0; f < 4; ++f) atomicAdd(&qstats[f], (unsigned long long)v[f]);
+    for (int f = 0; f < kQueryCounters; ++f)
+      if (v[f]) atomicAdd(&qstats[f], (unsigned long long)v[f]);
 }
 
 template <int MODE, bool STATS = false>
@@ -992,7 +1039,7 @@ void launch_queries(int mode, const MeshView& m, const float* d_q, const uint32_
 }  // namespace
 
 int query_points(const MeshView& m, int accel, int sign, const float* d_q, uint64_t nq, float* d_out, float* d_vec,
-                 uint8_t* d_inside, uint32_t* d_status, cudaStream_t s) {
+                 uint8_t* d_inside, uint32_t* d_status, cudaStream_t s, int64_t budget_override) {
   if (nq == 0) return M2S_OK;
   if (accel == M2S_ACCEL_NONE && !d_vec) return brute_force_sdf(m, sign, d_q, nq, d_out, d_status, s);
   if (m.n_tris == 0) return M2S_ERR_EMPTY_MESH;
@@ -1020,7 +1067,8 @@ int query_points(const MeshView& m, int accel, int sign, const float* d_q, uint6
   // Queries over the node budget continue one warp per query.
   DevBuf<HardQuery> hard;
   DevBuf<uint32_t> hard_count;
-  const uint32_t base_budget = g_query_budget.load(std::memory_order_relaxed);
+  const uint32_t base_budget =
+      budget_override >= 0 ? (uint32_t)budget_override : g_query_budget.load(std::memory_order_relaxed);
   const bool two_pass = mode != Q_BVH_NORMAL && base_budget > 0;
   if (two_pass) {
     if ((st = hard.alloc(nq, s)) || (st = hard_count.alloc(1, s))) return st;
@@ -1033,11 +1081,11 @@ int query_points(const MeshView& m, int accel, int sign, const float* d_q, uint6
   uint32_t* hc = two_pass ? hard_count.p : nullptr;
   // With profiling on, the counting instantiations run and their totals are
   // read back (a synchronisation, as profiling's phase timings are).
-  const bool counting = profiling_enabled();
+  const bool counting = profiling_enabled() || grid_tuning().fp64_audit;
   DevBuf<unsigned long long> qs;
   if (counting) {
-    if ((st = qs.alloc(4, s))) return st;
-    M2S_CUDA(cudaMemsetAsync(qs.p, 0, 32, s));
+    if ((st = qs.alloc(kQueryCounters, s))) return st;
+    M2S_CUDA(cudaMemsetAsync(qs.p, 0, 8 * kQueryCounters, s));
   }
   // Morton-ordered warps search together (nearest_triangle_packet): always
   // for Bvh(Normal), whose searches have no budget, and for the others from
@@ -1052,10 +1100,10 @@ int query_points(const MeshView& m, int accel, int sign, const float* d_q, uint6
                           blocks, nullptr, s);
   M2S_CUDA(cudaGetLastError());
   if (counting) {
-    unsigned long long h[4];
-    M2S_CUDA(cudaMemcpyAsync(h, qs.p, 32, cudaMemcpyDeviceToHost, s));
+    unsigned long long h[kQueryCounters];
+    M2S_CUDA(cudaMemcpyAsync(h, qs.p, 8 * kQueryCounters, cudaMemcpyDeviceToHost, s));
     M2S_CUDA(cudaStreamSynchronize(s));
-    const uint64_t rec[5] = {nq, h[0], h[1], h[2], h[3]};
+    const uint64_t rec[1 + kQueryCounters] = {nq, h[0], h[1], h[2], h[3], h[4], h[5], h[6], h[7], h[8], h[9], h[10]};
     record_query_stats(rec);
   }
   return M2S_OK;

@@ -11,12 +11,15 @@
 //  * points: each request is copied in, queried and copied out on one of a
 //    pool of streams, so requests on different meshes overlap on the device;
 //    completions are picked up from CUDA events;
-//  * grids: the grid requests waiting when the previous batch finishes join
-//    the next batch (up to four waves' worth of cells), computed as the
-//    batched grid job's waves, smallest wave first; a wave's requests complete
-//    when it is done.  A grid's values in a batch are bit-identical to
-//    computing it alone, and a point request runs exactly the kernels of
-//    m2s_query_sdf, so every result is the same alone and in the mix.
+//  * grids: kGridLanes lanes (a thread and a stream each) form waves from
+//    the head of the grid queue: whenever a lane is free it takes the
+//    waiting requests in arrival order, up to a wave's worth of cells (a
+//    larger grid alone), and computes them as one batched job.  A request is
+//    therefore admitted at the next wave boundary of any lane, and two waves
+//    run on the device at once, each a persistent launch sized so that both
+//    fit.  A grid's values in a wave are bit-identical to computing it alone,
+//    and a point request runs exactly the kernels of m2s_query_sdf, so every
+//    result is the same alone and in the mix.
 //
 // Admission: every request reserves an estimate of the device memory it will
 // hold (workspace and outputs; a mesh's resident structure for an upload)
@@ -93,16 +96,16 @@ uint64_t upload_bytes(uint64_t tris, uint64_t nv, uint64_t ni, int bits, int acc
 // with their sort buffers, and the continuation list of the two-pass query.
 uint64_t point_bytes(uint64_t nq) { return 64 * nq + (1u << 20); }
 
-// Largest grid batch, in waves of the batched job, and the serving wave size.
-constexpr uint64_t kBatchWaves = 4;
+// The serving wave size, and the lanes that run waves side by side.
 constexpr uint64_t kServeWaveCells = 4ull << 20;
-// Grid waves run 3 propagation blocks per SM (of the 4 that fit) unless the
-// tuning names a count: the persistent launch then leaves room on every SM
-// for point queries, which otherwise wait for the wave to end (64 resident
-// meshes, 200 requests per rate: point p99 11.6-12.3 -> 7.3-7.8 ms at 100
-// requests/s, 13.6-22 -> 9.1 ms at 200, 18-21 -> 12.7-15.8 ms at 400; grid
-// p50 unchanged; 2 per SM slows the grids).
-constexpr int kServeBlocksPerSm = 3;
+constexpr int kGridLanes = 2;
+// Unless the tuning names a count, each lane's waves run (fit - 1) / lanes
+// propagation blocks per SM, where `fit` is how many fit on one SM: the lanes'
+// persistent launches then fit on the device together and one block's room
+// per SM stays free for point queries.  A cooperative launch starts only once
+// all of its blocks can be resident, so a wave that does not fit yet waits
+// for room; it never runs partly resident.
+int serve_blocks_per_sm(int sign) { return std::max(1, (propagate_blocks_per_sm(sign) - 1) / kGridLanes); }
 
 }  // namespace
 
@@ -124,9 +127,9 @@ struct m2s_server {
   // counters
   uint64_t completed[3] = {0, 0, 0}, failed = 0, grid_batches = 0, grid_batched = 0, max_batch = 0, evictions = 0;
 
-  cudaStream_t s_upload = nullptr, s_grid = nullptr;
+  cudaStream_t s_upload = nullptr, s_grid[kGridLanes] = {};
   std::vector<cudaStream_t> s_points;
-  std::thread th[3];
+  std::thread th[2 + kGridLanes];  // uploads, points, grid lanes
 
   // ---- helpers (mu held) ----
   bool fits(uint64_t need) const { return reserved + need <= budget; }
@@ -177,7 +180,7 @@ struct m2s_server {
 
   void upload_loop();
   void points_loop();
-  void grid_loop();
+  void grid_loop(int lane);
 };
 
 void m2s_server::upload_loop() {
@@ -337,27 +340,24 @@ void m2s_server::points_loop() {
   cudaFree(d_status);
 }
 
-void m2s_server::grid_loop() {
+void m2s_server::grid_loop(int lane) {
   cudaSetDevice(device);
+  cudaStream_t s = s_grid[lane];
   uint32_t* h_status = nullptr;
   cudaHostAlloc((void**)&h_status, 4, cudaHostAllocPortable);
   for (;;) {
-    std::vector<RequestP> batch;
+    std::vector<RequestP> wave;
     std::vector<MeshView> views;
-    // Serving keeps waves small: a wave's requests complete together.
     GridTuning tune = grid_tuning();
     tune.wave_cells = std::min<uint64_t>(tune.wave_cells ? tune.wave_cells : kServeWaveCells, kServeWaveCells);
-    if (tune.blocks_per_sm <= 0) tune.blocks_per_sm = kServeBlocksPerSm;
-    const uint64_t wave_cells = tune.wave_cells;
+    uint64_t cells = 0;
     {
       std::unique_lock<std::mutex> lk(mu);
       cv_work.wait(lk, [&] { return stop || head_ready(kGrid); });
       if (stop) break;
-      // What waits joins the batch, in arrival order, up to kBatchWaves
-      // waves' worth of cells (a larger grid alone): a batch's requests
-      // complete wave by wave, and a bounded batch keeps the wait of a
-      // request that arrives during one bounded too.
-      uint64_t cells = 0;
+      // The waiting requests join this wave in arrival order, up to a
+      // wave's worth of cells (a larger grid alone); later ones wait for
+      // the next free lane.
       while (!q[kGrid].empty()) {
         RequestP r = q[kGrid].front();
         auto it = meshes.find(r->mesh_id);
@@ -367,68 +367,50 @@ void m2s_server::grid_loop() {
           continue;
         }
         if (!it->second.mesh || !fits(r->need)) break;
-        if (!batch.empty() && r->grid_sign != batch.front()->grid_sign) break;  // one sign per batch
-        if (!batch.empty() && cells + r->cells > kBatchWaves * wave_cells) break;
+        if (!wave.empty() && r->grid_sign != wave.front()->grid_sign) break;  // one sign per wave
+        if (!wave.empty() && cells + r->cells > tune.wave_cells) break;
         q[kGrid].pop_front();
         reserve(r->need);
         it->second.last_use = ++clock;
-        batch.push_back(r);
+        wave.push_back(r);
         views.push_back(it->second.mesh->mesh.view());
         cells += r->cells;
       }
+      if (!wave.empty()) {
+        ++grid_batches;
+        grid_batched += wave.size();
+        max_batch = std::max<uint64_t>(max_batch, wave.size());
+      }
     }
-    if (batch.empty()) continue;
+    if (wave.empty()) continue;
+    if (tune.blocks_per_sm <= 0) tune.blocks_per_sm = serve_blocks_per_sm(wave.front()->grid_sign);
     std::vector<GridDesc> grids;
-    for (auto& r : batch) grids.push_back(r->grid);
-    // Waves as the batched job forms them, run smallest first: the requests
-    // of a wave complete as soon as it is done.
-    auto waves = plan_waves(grids.data(), (uint32_t)batch.size(), wave_cells);
-    auto wave_size = [&](const std::vector<uint32_t>& w) {
-      uint64_t c = 0;
-      for (uint32_t k : w) c += batch[k]->cells;
-      return c;
-    };
-    std::stable_sort(waves.begin(), waves.end(),
-                     [&](const auto& a, const auto& b) { return wave_size(a) < wave_size(b); });
-    for (const auto& w : waves) {
-      std::vector<MeshView> wv;
-      std::vector<GridDesc> wg;
-      for (uint32_t k : w) {
-        wv.push_back(views[k]);
-        wg.push_back(grids[k]);
-      }
-      int st = M2S_OK;
-      {
-        DevBuf<float> dout;
-        DevBuf<uint32_t> dst;
-        if (!(st = dout.alloc(wave_size(w), s_grid)) && !(st = dst.alloc(1, s_grid))) {
-          if (cudaMemsetAsync(dst.p, 0, 4, s_grid) != cudaSuccess) st = M2S_ERR_CUDA;
-          if (!st)
-            st = grid_sdf_batch(wv.data(), (uint32_t)w.size(), wg.data(), batch.front()->grid_sign, dout.p, dst.p,
-                                s_grid, nullptr, nullptr, tune);
-          uint64_t off = 0;
-          for (uint32_t k : w) {
-            const RequestP& r = batch[k];
-            if (!st && cudaMemcpyAsync(r->out, dout.p + off, 4 * r->cells, cudaMemcpyDeviceToHost, s_grid) !=
-                           cudaSuccess)
-              st = M2S_ERR_CUDA;
-            off += r->cells;
-          }
-          if (!st && cudaMemcpyAsync(h_status, dst.p, 4, cudaMemcpyDeviceToHost, s_grid) != cudaSuccess)
+    for (auto& r : wave) grids.push_back(r->grid);
+    tune.wave_cells = std::max<uint64_t>(cells, 1);  // the whole wave is one job
+    int st = M2S_OK;
+    {
+      DevBuf<float> dout;
+      DevBuf<uint32_t> dst;
+      if (!(st = dout.alloc(cells, s)) && !(st = dst.alloc(1, s))) {
+        if (cudaMemsetAsync(dst.p, 0, 4, s) != cudaSuccess) st = M2S_ERR_CUDA;
+        if (!st)
+          st = grid_sdf_batch(views.data(), (uint32_t)wave.size(), grids.data(), wave.front()->grid_sign, dout.p,
+                              dst.p, s, nullptr, nullptr, tune);
+        uint64_t off = 0;
+        for (const RequestP& r : wave) {
+          if (!st && cudaMemcpyAsync(r->out, dout.p + off, 4 * r->cells, cudaMemcpyDeviceToHost, s) != cudaSuccess)
             st = M2S_ERR_CUDA;
-          if (cudaStreamSynchronize(s_grid) != cudaSuccess && !st) st = M2S_ERR_CUDA;
-          if (!st) st = status_from_bits(*h_status);
+          off += r->cells;
         }
+        if (!st && cudaMemcpyAsync(h_status, dst.p, 4, cudaMemcpyDeviceToHost, s) != cudaSuccess) st = M2S_ERR_CUDA;
+        if (cudaStreamSynchronize(s) != cudaSuccess && !st) st = M2S_ERR_CUDA;
+        if (!st) st = status_from_bits(*h_status);
       }
-      std::lock_guard<std::mutex> lk(mu);
-      for (uint32_t k : w) finish(batch[k], st);
     }
     std::lock_guard<std::mutex> lk(mu);
-    ++grid_batches;
-    grid_batched += batch.size();
-    max_batch = std::max<uint64_t>(max_batch, batch.size());
+    for (const RequestP& r : wave) finish(r, st);
   }
-  cudaStreamSynchronize(s_grid);
+  cudaStreamSynchronize(s);
   cudaFreeHost(h_status);
 }
 
@@ -475,8 +457,9 @@ int m2s_server_create(uint64_t hbm_budget_bytes, uint32_t point_streams, m2s_ser
   cudaGetDevice(&S->device);
   S->budget = hbm_budget_bytes;
   S->n_streams = std::max<uint32_t>(1, std::min<uint32_t>(point_streams ? point_streams : 4, 32));
-  bool ok = cudaStreamCreateWithFlags(&S->s_upload, cudaStreamNonBlocking) == cudaSuccess &&
-            cudaStreamCreateWithFlags(&S->s_grid, cudaStreamNonBlocking) == cudaSuccess;
+  bool ok = cudaStreamCreateWithFlags(&S->s_upload, cudaStreamNonBlocking) == cudaSuccess;
+  for (int l = 0; ok && l < kGridLanes; ++l)
+    ok = cudaStreamCreateWithFlags(&S->s_grid[l], cudaStreamNonBlocking) == cudaSuccess;
   for (uint32_t i = 0; ok && i < S->n_streams; ++i) {
     cudaStream_t s;
     ok = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess;
@@ -486,7 +469,8 @@ int m2s_server_create(uint64_t hbm_budget_bytes, uint32_t point_streams, m2s_ser
     st = cuda_fail(cudaGetLastError(), "cudaStreamCreateWithFlags");
     for (auto s : S->s_points) cudaStreamDestroy(s);
     if (S->s_upload) cudaStreamDestroy(S->s_upload);
-    if (S->s_grid) cudaStreamDestroy(S->s_grid);
+    for (auto g : S->s_grid)
+      if (g) cudaStreamDestroy(g);
     delete S;
     return st;
   }
@@ -504,7 +488,7 @@ int m2s_server_create(uint64_t hbm_budget_bytes, uint32_t point_streams, m2s_ser
   }
   S->th[kUpload] = std::thread([S] { S->upload_loop(); });
   S->th[kPoints] = std::thread([S] { S->points_loop(); });
-  S->th[kGrid] = std::thread([S] { S->grid_loop(); });
+  for (int l = 0; l < kGridLanes; ++l) S->th[2 + l] = std::thread([S, l] { S->grid_loop(l); });
   *out = S;
   return M2S_OK;
 }
@@ -527,7 +511,7 @@ void m2s_server_free(m2s_server* S) {
   cudaStreamSynchronize(S->s_upload);
   for (auto s : S->s_points) cudaStreamDestroy(s);
   cudaStreamDestroy(S->s_upload);
-  cudaStreamDestroy(S->s_grid);
+  for (auto g : S->s_grid) cudaStreamDestroy(g);
   cudaSetDevice(prev);
   delete S;
 }

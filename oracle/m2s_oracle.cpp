@@ -791,8 +791,24 @@ D3 d_seg(D3 p, D3 a, D3 b) {
   s = std::min(1.0, std::max(0.0, s));
   return d_add(a, d_mul(ab, s));
 }
+// Nearest of the three edges: the closest point of a zero-area triangle.
+D3 d_closest_edges(D3 p, D3 a, D3 b, D3 c) {
+  D3 e[3] = {d_seg(p, a, b), d_seg(p, b, c), d_seg(p, a, c)};
+  D3 best = e[0];
+  double bd = d_dot(d_sub(p, e[0]), d_sub(p, e[0]));
+  for (int k = 1; k < 3; ++k) {
+    double dd = d_dot(d_sub(p, e[k]), d_sub(p, e[k]));
+    if (dd < bd) bd = dd, best = e[k];
+  }
+  return best;
+}
 D3 d_closest(D3 p, D3 a, D3 b, D3 c) {
   D3 ab = d_sub(b, a), ac = d_sub(c, a), ap = d_sub(p, a);
+  // A zero-area triangle (repeated or collinear vertices, like a strip's
+  // connector windows) is its edges; the region formulas below would divide
+  // by zero on it.
+  D3 n = {ab.y * ac.z - ab.z * ac.y, ab.z * ac.x - ab.x * ac.z, ab.x * ac.y - ab.y * ac.x};
+  if (d_dot(n, n) == 0) return d_closest_edges(p, a, b, c);
   double d1 = d_dot(ab, ap), d2 = d_dot(ac, ap);
   if (d1 <= 0 && d2 <= 0) return a;
   D3 bp = d_sub(p, b);
@@ -809,17 +825,7 @@ D3 d_closest(D3 p, D3 a, D3 b, D3 c) {
   if (va <= 0 && d4 - d3 >= 0 && d5 - d6 >= 0)
     return d_add(b, d_mul(d_sub(c, b), (d4 - d3) / ((d4 - d3) + (d5 - d6))));
   double den = va + vb + vc;
-  if (!(den != 0)) {
-    // Degenerate: the nearest of the three edges.
-    D3 e[3] = {d_seg(p, a, b), d_seg(p, b, c), d_seg(p, a, c)};
-    D3 best = e[0];
-    double bd = d_dot(d_sub(p, e[0]), d_sub(p, e[0]));
-    for (int k = 1; k < 3; ++k) {
-      double dd = d_dot(d_sub(p, e[k]), d_sub(p, e[k]));
-      if (dd < bd) bd = dd, best = e[k];
-    }
-    return best;
-  }
+  if (!(den != 0)) return d_closest_edges(p, a, b, c);
   return d_add(d_add(a, d_mul(ab, vb / den)), d_mul(ac, vc / den));
 }
 bool d_ray(D3 o, D3 t0, D3 t1, D3 t2, int axis) {

@@ -1,7 +1,7 @@
 """The grid propagation's proposal filter changes no bit.
 
-Propagation drops a neighbour proposal unevaluated when the triangle's
-distance bound (its plane and edge lines, with a slack far above f32 rounding)
+The filtered kernel variant (m2s_set_grid_bound_filter; off by default)
+drops a neighbour proposal unevaluated when the triangle's distance bound (its plane and edge lines, with a slack far above f32 rounding)
 proves that it cannot beat the cell's value.  These tests run every grid with
 the filter on and off and require identical bits, on shapes chosen to stress
 the bound: smooth closed meshes, an open terrain strip with zero-area
@@ -25,7 +25,7 @@ def _device():
     if not m2s.device_available():
         pytest.fail("no sm_100 device: the GPU suite must run on a B200")
     yield
-    m2s.set_grid_bound_filter(True)
+    m2s.set_grid_bound_filter(False)
 
 
 def bits(a):
@@ -58,7 +58,7 @@ def run_both(v, topo, grid, sign):
         m2s.set_grid_bound_filter(on)
         out.append(m2s.generate_grid_sdf(v, topo, grid, sign))
         stats.append(m2s.last_grid_stats())
-    m2s.set_grid_bound_filter(True)
+    m2s.set_grid_bound_filter(False)
     return out, stats
 
 
@@ -118,6 +118,6 @@ def test_filter_batched_kernel():
                 outs.append(out.cpu().numpy())
             assert np.array_equal(bits(outs[0]), bits(outs[1])), sign
     finally:
-        m2s.set_grid_bound_filter(True)
+        m2s.set_grid_bound_filter(False)
         for m in meshes:
             m.close()

@@ -1,12 +1,20 @@
 """serde.rs format V1, on the CPU (the codec is host code in the library).
 
-Pinned by the crate's own fixtures, read in place from the reference checkout
-when it is present (serde.rs:298-369: the same data must give the same bytes,
-and the bytes must read back to the same data), and by an independent
-msgpack encoder (the `msgpack` package) for the cases the fixtures do not
-reach: long arrays (16- and 32-bit lengths), cell counts in every integer
-width, non-finite floats, structs written as maps and 64-bit floats.
+Pinned by the crate's own fixtures (serde.rs:298-369: the same data must give
+the same bytes, and the bytes must read back to the same data):
+  * always, by their length and SHA-256 (tests/golden/serde_fixture_digests.json,
+    written by tests/golden/make_serde_digests.py from the crate's files), so
+    the library's bytes are checked against the crate's on any machine;
+  * when M2S_REFERENCE_DIR names a checkout of the reference, also against the
+    fixture files themselves (read in place; the test fails if the variable is
+    set and the files are missing).
+And by an independent msgpack encoder (the `msgpack` package) for the cases
+the fixtures do not reach: long arrays (16- and 32-bit lengths), cell counts
+in every integer width, non-finite floats, structs written as maps and 64-bit
+floats.
 """
+import hashlib
+import json
 import os
 
 import msgpack
@@ -16,15 +24,28 @@ import pytest
 import mesh_to_sdf_b200 as m2s
 from mesh_to_sdf_b200 import serde
 
-REF_TESTS = "/root/reference/mesh_to_sdf/tests"
+DIGESTS = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                                      "serde_fixture_digests.json")))
+
+
+def _check_digest(name, data):
+    want = DIGESTS[name]
+    assert len(data) == want["bytes"], (name, len(data))
+    assert hashlib.sha256(data).hexdigest() == want["sha256"], name
 
 
 def _fixture(name):
-    path = os.path.join(REF_TESTS, name)
-    if not os.path.exists(path):
-        pytest.skip("reference checkout not present")
+    """The crate's fixture bytes from M2S_REFERENCE_DIR, or None when the
+    variable is unset (the digest check stands alone then)."""
+    root = os.environ.get("M2S_REFERENCE_DIR")
+    if not root:
+        return None
+    path = os.path.join(root, "mesh_to_sdf", "tests", name)
+    assert os.path.exists(path), f"M2S_REFERENCE_DIR is set but {path} is missing"
     with open(path, "rb") as f:
-        return f.read()
+        data = f.read()
+    _check_digest(name, data)
+    return data
 
 
 def _bits(a):
@@ -35,8 +56,10 @@ def test_generic_fixture_bytes():
     # serde.rs:298-330: queries (1,2,3), (6,5,4); distances 1, 3
     q = np.array([[1, 2, 3], [6, 5, 4]], np.float32)
     d = np.array([1, 3], np.float32)
-    data = _fixture("sdf_generic_v1.bin")
-    assert serde.serialize(serde.SerializeGeneric(q, d)) == data
+    data = serde.serialize(serde.SerializeGeneric(q, d))
+    _check_digest("sdf_generic_v1.bin", data)
+    fixture = _fixture("sdf_generic_v1.bin")
+    assert fixture is None or fixture == data
     back = serde.deserialize(data)
     assert isinstance(back, serde.DeserializeGeneric)
     assert np.array_equal(back.query_points, q) and np.array_equal(back.distances, d)
@@ -46,8 +69,10 @@ def test_grid_fixture_bytes():
     # serde.rs:333-366: Grid::new([1,2,3],[4,5,6],[7,8,9]), distances 0..504
     grid = m2s.Grid.new([1, 2, 3], [4, 5, 6], [7, 8, 9])
     d = np.arange(grid.get_total_cell_count(), dtype=np.float32)
-    data = _fixture("sdf_grid_v1.bin")
-    assert serde.serialize(serde.SerializeGrid(grid, d)) == data
+    data = serde.serialize(serde.SerializeGrid(grid, d))
+    _check_digest("sdf_grid_v1.bin", data)
+    fixture = _fixture("sdf_grid_v1.bin")
+    assert fixture is None or fixture == data
     back = serde.deserialize(data)
     assert isinstance(back, serde.DeserializeGrid)
     assert back.grid.cell_count == (7, 8, 9)

@@ -9,9 +9,12 @@ Bars:
     submission; requests that fit one at a time but not together all complete,
     and the reserved bytes never exceed the budget;
   * an upload that does not fit evicts an idle mesh, least recently used first;
-  * grid requests that queue up beyond one batch (more than four waves' worth
-    of cells) are split over several batches, and every grid still equals its
-    single-grid call bit for bit.
+  * grid requests that queue up beyond one wave (more than 4M cells) are
+    split over several waves, and every grid still equals its single-grid
+    call bit for bit;
+  * continuous batching: a grid request submitted while a large grid's wave
+    runs is taken by the other lane at once and completes first, its wave
+    overlapping the large one on the device, bit-identical to its single call.
 """
 import numpy as np
 import pytest
@@ -170,6 +173,45 @@ def test_grid_backlog_spans_batches():
             assert np.array_equal(bits(out), bits(d.cpu().numpy()))
         st = srv.stats()
         assert st["grid_requests"] == len(edges) and st["failed"] == 0
-        assert st["grid_batches"] >= 3  # at most four waves of cells per batch
+        assert st["grid_batches"] >= 8  # waves of at most 4M cells
+    finally:
+        srv.close()
+
+
+def test_grid_request_admitted_while_a_wave_runs():
+    import time
+
+    import torch
+
+    v, idx = synth.star(4, seed=22)
+    lo, hi = synth.padded_bbox(v)
+    srv = m2s.Server(64 << 30, point_streams=2)
+    try:
+        mid, t = srv.submit_upload(v, T.TriangleList(idx), A.rtree_bvh())
+        assert srv.wait(t)[0] == 0
+        # a 256^3 grid (a wave of its own on one lane), then a small grid while it runs:
+        # the free lane takes the small one at once and both run on the device together
+        big = m2s.Grid.from_bounding_box(lo, hi, [256, 256, 256])
+        bout = np.full(big.get_total_cell_count(), np.nan, np.float32)
+        t_big = time.perf_counter()
+        tb = srv.submit_grid(mid, big, S.Raycast, bout)
+        time.sleep(0.002)
+        small = m2s.Grid.from_bounding_box(lo, hi, [48, 48, 48])
+        sout = np.full(small.get_total_cell_count(), np.nan, np.float32)
+        t_small = time.perf_counter()
+        ts = srv.submit_grid(mid, small, S.Raycast, sout)
+        st, lat_small = srv.wait(ts)
+        assert st == 0
+        st, lat_big = srv.wait(tb)
+        assert st == 0
+        # completion = submission + the latency the server measured
+        assert t_small + lat_small < t_big + lat_big, (t_small - t_big, lat_small, lat_big)
+        single = m2s.build_sdf_acceleration(v, T.TriangleList(idx), A.none())
+        for grid, out in ((small, sout), (big, bout)):
+            d = torch.empty(grid.get_total_cell_count(), dtype=torch.float32, device="cuda")
+            single.grid_device(grid, S.Raycast, d)
+            assert np.array_equal(bits(out), bits(d.cpu().numpy()))
+        st = srv.stats()
+        assert st["grid_requests"] == 2 and st["failed"] == 0 and st["grid_batches"] == 2
     finally:
         srv.close()
