@@ -446,6 +446,8 @@ def main():
                     help="one short pass for profilers: one grid, 100k Rtree / RtreeBvh points, 8k brute-force points")
     ap.add_argument("--grid", type=int, default=128, help="grid edge of the --small pass")
     ap.add_argument("--points", type=int, default=100_000, help="query points of the --small pass")
+    ap.add_argument("--bound-filter", action="store_true",
+                    help="--small: run the grid with the filtered propagation variant (same results)")
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
                     help="c2 (default): the headline line; c1 / c3: the small and the terrain configurations; "
                          "c4: 256 grids batched in one plan against 256 single-grid calls; "
@@ -457,7 +459,7 @@ def main():
     ap.add_argument("--wave-cells", type=int, default=0, help="c4: cells per batched job (0 = the library default)")
     args = ap.parse_args()
     if args.small:
-        return small_case(args.grid, args.points)
+        return small_case(args.grid, args.points, args.bound_filter)
     if args.impl == "reference" and args.workload in ("c1", "c3", "c4"):
         return reference_workloads(args)
     if args.workload == "c4":
@@ -1116,9 +1118,10 @@ def serving_workload(args):
     print(json.dumps(serving_entry(rates, args.requests, not args.no_cpu_baseline)), flush=True)
 
 
-def small_case(edge=128, points=100_000):
+def small_case(edge=128, points=100_000, bound_filter=False):
     """A short, fixed workload for ncu captures (at most ~1.5 GB on the device);
-    from 2^19 points the queries take the warp-packet search."""
+    from 2^19 points the queries take the warp-packet search.  The grid comes
+    first, so `-k regex:k_propagate -c 1` captures it."""
     import torch
 
     import mesh_to_sdf_b200 as m2s
@@ -1130,7 +1133,9 @@ def small_case(edge=128, points=100_000):
     mesh = m2s.build_sdf_acceleration(v, m2s.Topology.TriangleList(idx), A.rtree_bvh())
     out = torch.empty(grid.get_total_cell_count(), dtype=torch.float32, device="cuda")
     status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    m2s.set_grid_bound_filter(bound_filter)
     mesh.grid_device(grid, S.Raycast, out, status)
+    m2s.set_grid_bound_filter(False)
     q = torch.from_numpy(synth.mixed_points(v, idx, points, seed=SEED)).cuda()
     qo = torch.empty(points, dtype=torch.float32, device="cuda")
     mesh.query_device(q, qo, status)
