@@ -15,6 +15,8 @@
 //  * query_vector_to_closest_point_rtree_bvh (rtree_bvh.rs:217-276).
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include <algorithm>
 #include <cfloat>
 
@@ -455,7 +457,7 @@ __device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v)
 // search on one lane).
 constexpr int kWarpStack = 2048;
 
-template <bool STATS = false>
+template <bool STATS = false, int CAP = kWarpStack>
 __device__ bool nearest_triangle_warp(const MeshView& m, P3 p, Nearest* io, uint32_t* s_node, float* s_dist,
                                       QCount* qc = nullptr) {
   const int lane = threadIdx.x & 31;
@@ -529,7 +531,7 @@ __device__ bool nearest_triangle_warp(const MeshView& m, P3 p, Nearest* io, uint
       if (lane >= o) incl += y;
     }
     const int total = __shfl_sync(0xFFFFFFFFu, incl, 31);
-    if (sp + total > kWarpStack) return false;
+    if (sp + total > CAP) return false;
     int pos = sp + incl - keep;
     for (int c = 0; c < npush; ++c)
       if (push_d[c] <= nb) {
@@ -627,6 +629,112 @@ __device__ __forceinline__ bool vote_inside(const MeshView& m, P3 p, bool* overf
   if constexpr (STATS) {
     const int insides64 = (c64[0] & 1u) + (c64[1] & 1u) + (c64[2] & 1u);
     qc->vote_flip += (insides > 1) != (insides64 > 1);
+  }
+  return insides > 1;
+}
+
+// The +AXIS ray's crossings from o counted by a whole warp (one query): the
+// lanes pop up to 32 nodes of a shared stack, test both children's boxes as
+// ray_crossings does, test child leaves with the aligned ray test and push
+// child nodes.  Every leaf the box test admits is tested exactly once, so the
+// count (and *count64, the FP64 audit's count, in the counting instantiation)
+// is the single-thread one.  Returns false if the stack would overflow.
+template <int AXIS, int CAP, bool STATS = false>
+__device__ bool ray_crossings_warp(const MeshView& m, P3 o, uint32_t* s_stack, uint32_t* count_out, QCount* qc,
+                                   uint32_t* count64_out) {
+  constexpr int IY = (AXIS + 1) % 3, IZ = (AXIS + 2) % 3;
+  const int lane = threadIdx.x & 31;
+  const float oy = vget(o, IY), oz = vget(o, IZ), ox = vget(o, AXIS);
+  auto inside = [&](float4 lo, float4 hi) {
+    float loy = IY == 0 ? lo.x : (IY == 1 ? lo.y : lo.z), hiy = IY == 0 ? hi.x : (IY == 1 ? hi.y : hi.z);
+    float loz = IZ == 0 ? lo.x : (IZ == 1 ? lo.y : lo.z), hiz = IZ == 0 ? hi.x : (IZ == 1 ? hi.y : hi.z);
+    float hix = AXIS == 0 ? hi.x : (AXIS == 1 ? hi.y : hi.z);
+    return oy >= loy && oy <= hiy && oz >= loz && oz <= hiz && hix >= ox;
+  };
+  uint32_t count = 0, count64 = 0;
+  auto test = [&](uint32_t leaf) {
+    TriRec r = load_tri(m.stris, leaf);
+    if constexpr (STATS) {
+      ++qc->sign_tests;
+      const RayAudit ra = ray_audit<AXIS>(o, p3(r.a), p3(r.b), p3(r.c));
+      ++qc->ray_tests;
+      qc->ray_ambiguous += ra.ambiguous;
+      qc->ray_disagree += ra.hit64 != ra.hit32;
+      count += ra.hit32 ? 1u : 0u;
+      count64 += ra.hit64 ? 1u : 0u;
+    } else {
+      float t;
+      count += ray_hit_aligned<AXIS>(o, p3(r.a), p3(r.b), p3(r.c), &t) ? 1u : 0u;
+    }
+  };
+  if (lane == 0) s_stack[0] = 0;
+  int sp = 1;
+  __syncwarp();
+  while (sp > 0) {
+    const int take = min(sp, 32);
+    const int base = sp - take;
+    const uint32_t node = lane < take ? s_stack[base + lane] : 0xFFFFFFFFu;
+    __syncwarp();
+    sp = base;
+    uint32_t push[2] = {0u, 0u};
+    int npush = 0;
+    if (node != 0xFFFFFFFFu) {
+      if constexpr (STATS) ++qc->sign_visits;
+      const BvhNode nd = load_node(m.nodes, node);
+      const uint32_t ch[2] = {__float_as_uint(nd.l_lo.w), __float_as_uint(nd.l_hi.w)};
+      const bool go[2] = {inside(nd.l_lo, nd.l_hi), inside(nd.r_lo, nd.r_hi)};
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        if (!go[c]) continue;
+        if (ch[c] & LEAF_BIT) test(ch[c] & ~LEAF_BIT);
+        else push[npush++] = ch[c];
+      }
+    }
+    int incl = npush;
+    for (int o2 = 1; o2 < 32; o2 <<= 1) {
+      const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o2);
+      if (lane >= o2) incl += y;
+    }
+    const int total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    if (sp + total > CAP) return false;
+    int pos = sp + incl - npush;
+    for (int c = 0; c < npush; ++c) s_stack[pos++] = push[c];
+    sp += total;
+    __syncwarp();
+  }
+  for (int o2 = 16; o2; o2 >>= 1) {
+    count += __shfl_xor_sync(0xFFFFFFFFu, count, o2);
+    if constexpr (STATS) count64 += __shfl_xor_sync(0xFFFFFFFFu, count64, o2);
+  }
+  *count_out = count;
+  if constexpr (STATS) *count64_out = count64;
+  return true;
+}
+
+// The 3-ray vote by a whole warp (every lane returns it).  A ray whose stack
+// would overflow is counted by lane 0 alone.
+template <int CAP, bool STATS = false>
+__device__ bool vote_inside_warp(const MeshView& m, P3 p, uint32_t* s_stack, bool* overflow, QCount* qc) {
+  uint32_t c[3] = {0u, 0u, 0u}, c64[3] = {0u, 0u, 0u};
+  bool ok[3];
+  ok[0] = ray_crossings_warp<0, CAP, STATS>(m, p, s_stack, &c[0], qc, &c64[0]);
+  ok[1] = ray_crossings_warp<1, CAP, STATS>(m, p, s_stack, &c[1], qc, &c64[1]);
+  ok[2] = ray_crossings_warp<2, CAP, STATS>(m, p, s_stack, &c[2], qc, &c64[2]);
+  if (!(ok[0] && ok[1] && ok[2])) {  // warp-uniform
+    if ((threadIdx.x & 31) == 0) {
+      if (!ok[0]) c[0] = ray_crossings<0, STATS>(m, p, overflow, qc, &c64[0]);
+      if (!ok[1]) c[1] = ray_crossings<1, STATS>(m, p, overflow, qc, &c64[1]);
+      if (!ok[2]) c[2] = ray_crossings<2, STATS>(m, p, overflow, qc, &c64[2]);
+    }
+    for (int a = 0; a < 3; ++a) {
+      c[a] = __shfl_sync(0xFFFFFFFFu, c[a], 0);
+      c64[a] = __shfl_sync(0xFFFFFFFFu, c64[a], 0);
+    }
+  }
+  const int insides = (c[0] & 1u) + (c[1] & 1u) + (c[2] & 1u);
+  if constexpr (STATS) {
+    const int insides64 = (c64[0] & 1u) + (c64[1] & 1u) + (c64[2] & 1u);
+    if ((threadIdx.x & 31) == 0) qc->vote_flip += (insides > 1) != (insides64 > 1);
   }
   return insides > 1;
 }
@@ -861,6 +969,46 @@ __global__ void __launch_bounds__(32 * kHardWarps) k_query_hard(MeshView m, cons
   if constexpr (STATS) add_counts(qc, qstats);
 }
 
+// Small batches: one warp per query from the start.  A batch of a few
+// thousand queries leaves most of the GPU idle under one thread per query,
+// and its time is its longest chain of dependent node fetches (the search,
+// then three ray traversals, then the warp pass for long searches).  Here the
+// warp searches (nearest_triangle_warp) and casts the three rays
+// (vote_inside_warp) together, 32 nodes a step.  Results are the other
+// passes' bit for bit: the exact minimum of (distance, triangle) and exact
+// crossing counts.  kSmallStack entries of stack per warp; on overflow lane 0
+// finishes alone.
+constexpr int kSmallWarps = 4;
+constexpr int kSmallStack = 1024;
+
+template <int MODE, bool STATS = false>
+__global__ void __launch_bounds__(32 * kSmallWarps) k_query_warpwise(MeshView m, const float* __restrict__ q,
+                                                                    uint64_t nq, float* __restrict__ out,
+                                                                    float* __restrict__ vec,
+                                                                    uint8_t* __restrict__ inside_out, uint32_t* status,
+                                                                    unsigned long long* qstats = nullptr) {
+  QCount qc;
+  __shared__ uint32_t s_node[kSmallWarps][kSmallStack];
+  __shared__ float s_dist[kSmallWarps][kSmallStack];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  bool overflow = false, nan = false;
+  for (uint64_t i = (uint64_t)blockIdx.x * kSmallWarps + w; i < nq; i += (uint64_t)gridDim.x * kSmallWarps) {
+    const P3 p = load_query(q, i);
+    Nearest nn{INFINITY, 0xFFFFFFFFu, 0};
+    const bool ok = nearest_triangle_warp<STATS, kSmallStack>(m, p, &nn, s_node[w], s_dist[w], &qc);
+    bool inside = false;
+    if (MODE == Q_BVH_RAYCAST || MODE == Q_VECTOR) inside = vote_inside_warp<kSmallStack, STATS>(m, p, s_node[w], &overflow, &qc);
+    if (lane == 0) {
+      if (!ok) nn = nearest_triangle<STATS>(m, p, &overflow, nn, 0xFFFFFFFFu, nullptr, &qc);  // stack full: finish alone
+      finish_query<MODE, STATS>(m, i, p, nn, inside, out, vec, inside_out, &nan, &overflow, &qc);
+    }
+    __syncwarp();
+  }
+  if (overflow) atomicOr(status, bit(M2S_ERR_LIMIT));
+  if (nan) atomicOr(status, bit(M2S_ERR_NAN_DISTANCE));
+  if constexpr (STATS) add_counts(qc, qstats);
+}
+
 // Morton order of the queries (spatially coherent warps).
 __global__ void k_query_keys(const float* __restrict__ q, uint64_t nq, MeshView m, uint32_t* keys, uint32_t* vals) {
   uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -900,6 +1048,12 @@ std::atomic<uint32_t> g_query_budget{768};
 // 600k queries; 1M star points 8.0 -> 7.1 ms, 4M terrain points 15.2 -> 10.7 ms;
 // 100k star points 2.4 -> 2.9 ms).
 constexpr uint64_t kPacketMinQueries = 1u << 19;
+// Batches up to this many queries run one warp per query (k_query_warpwise).
+// Measured on B200, star s6, RtreeBvh / Rtree, against the two-pass path:
+// 1,000 queries 0.39 / 0.37 ms against 0.57 / 0.45 ms, 4,000 0.43 / 0.39
+// against 0.60 / 0.46 ms, but 16,000 1.24 / 1.13 against 0.98 / 0.74 ms
+// (bit-identical results throughout).
+constexpr uint64_t kWarpwiseMaxQueries = 8192;
 constexpr uint64_t kMortonMinQueries = 1u << 17;  // batch size from which queries run in Morton order
 
 namespace {
@@ -1048,6 +1202,42 @@ int query_points(const MeshView& m, int accel, int sign, const float* d_q, uint6
                          : (accel == M2S_ACCEL_RTREE
                                 ? Q_RTREE
                                 : ((accel == M2S_ACCEL_BVH && sign == M2S_SIGN_NORMAL) ? Q_BVH_NORMAL : Q_BVH_RAYCAST));
+  // Small batches (not Bvh(Normal), whose tie-band fold runs per thread;
+  // a mesh of more than one triangle): one warp per query.
+  if (mode != Q_BVH_NORMAL && nq <= kWarpwiseMaxQueries && !(m.root & LEAF_BIT)) {
+    const bool counting = profiling_enabled() || grid_tuning().fp64_audit;
+    DevBuf<unsigned long long> qs;
+    int st;
+    if (counting) {
+      if ((st = qs.alloc(kQueryCounters, s))) return st;
+      M2S_CUDA(cudaMemsetAsync(qs.p, 0, 8 * kQueryCounters, s));
+    }
+    const unsigned wb = (unsigned)std::min<uint64_t>((nq + kSmallWarps - 1) / kSmallWarps, 148ull * 64ull);
+    auto go = [&](auto st_tag) {
+      constexpr bool ST = decltype(st_tag)::value;
+      unsigned long long* qp = ST ? qs.p : nullptr;
+      if (mode == Q_BVH_RAYCAST)
+        k_query_warpwise<Q_BVH_RAYCAST, ST><<<wb, 32 * kSmallWarps, 0, s>>>(m, d_q, nq, d_out, nullptr, nullptr,
+                                                                            d_status, qp);
+      else if (mode == Q_RTREE)
+        k_query_warpwise<Q_RTREE, ST><<<wb, 32 * kSmallWarps, 0, s>>>(m, d_q, nq, d_out, nullptr, nullptr, d_status,
+                                                                      qp);
+      else
+        k_query_warpwise<Q_VECTOR, ST><<<wb, 32 * kSmallWarps, 0, s>>>(m, d_q, nq, nullptr, d_vec, d_inside, d_status,
+                                                                       qp);
+    };
+    if (counting) go(std::true_type{});
+    else go(std::false_type{});
+    M2S_CUDA(cudaGetLastError());
+    if (counting) {
+      unsigned long long h[kQueryCounters];
+      M2S_CUDA(cudaMemcpyAsync(h, qs.p, 8 * kQueryCounters, cudaMemcpyDeviceToHost, s));
+      M2S_CUDA(cudaStreamSynchronize(s));
+      const uint64_t rec[1 + kQueryCounters] = {nq, h[0], h[1], h[2], h[3], h[4], h[5], h[6], h[7], h[8], h[9], h[10]};
+      record_query_stats(rec);
+    }
+    return M2S_OK;
+  }
   // Morton-ordered launch for large batches: from 2^17 queries (below, the
   // sort's launches cost more than coherent warps save: 10k RtreeBvh points
   // on icosphere s3 0.33 -> 0.21 ms unsorted, star s6 50k 1.84 -> 1.65 ms; at

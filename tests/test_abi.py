@@ -30,6 +30,16 @@ def test_library_exports_every_declared_symbol():
     assert set(names) == set(_lib.SIGNATURES)
 
 
+def test_rust_crate_binds_every_declared_symbol():
+    # rust/mesh_to_sdf_cuda/src/ffi.rs (the drop-in crate's raw bindings; no
+    # Rust toolchain on this image) declares exactly the header's functions
+    import re
+
+    ffi = open(os.path.join(ROOT, "rust", "mesh_to_sdf_cuda", "src", "ffi.rs")).read()
+    bound = set(re.findall(r"pub fn (m2s_\w+)\(", ffi))
+    assert bound == set(declared_symbols()), (set(declared_symbols()) - bound, bound - set(declared_symbols()))
+
+
 def test_status_strings():
     L = _lib.lib()
     assert L.m2s_status_string(0) == b"ok"
