@@ -53,7 +53,7 @@ def grid_roofline(cells, n_vertices, n_tris, phases, stats, hbm_peak, peak_sourc
     u32 indices per triangle) — the HBM bytes the result itself needs.
     `implementation_bytes` counts what the kernel's own data structures move
     (per relaxed state its 8 B entry and 48 B triangle record, per proposal
-    the neighbour's 8 B snapshot and 8 B working key), mostly L2 hits.
+    the neighbour's 8 B key read and its 8 B atomic), mostly L2 hits.
     `traffic` is the ncu DRAM count of one launch of the bench grid and
     `traffic_ratio` its multiple of the algorithmic bytes.  `fp32` sets the
     evaluated proposals' FP32 operations against the FP32 peak (148 SMs x

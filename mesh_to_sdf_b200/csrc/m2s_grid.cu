@@ -3,8 +3,9 @@
 //
 // 1. Seeding (generate_preheap, grid.rs:383-457): one warp per triangle walks
 //    the cells of its padded, snapped and widened box and keeps, per cell, the
-//    best (distance, triangle) under compare_distances.  Cells hold a packed
-//    64-bit key: high word = f32 bits of the distance, low word = triangle.
+//    best (distance, triangle) under compare_distances.  Cells hold one packed
+//    64-bit key: high word = f32 bits of the distance, low word = triangle
+//    shifted left by one over a dirty bit (8 bytes of state per cell).
 // 2. Propagation (generate_heap + propagate_heap, grid.rs:464-558): the
 //    reference pops (cell, triangle) states from heaps in distance order and
 //    evaluates the popped triangle on the 27 cells of the 3x3x3 block, keeping
@@ -12,9 +13,11 @@
 //    cooperative launch.  States are binned by distance: a quarter of the
 //    smallest cell size per bucket for the first 8 cells, logarithmically
 //    wider beyond.  Each round relaxes the lowest non-empty bucket, one thread
-//    per (state, neighbour) proposal.  A proposal competes with the cell's
-//    value at the start of the round; the round's best proposal per cell wins
-//    and is queued for further propagation.  Sixteen consecutive buckets (the
+//    per (state, neighbour) proposal.  Proposals lower the cell's key in
+//    place with atomics; the first to lower a clean key sets its dirty bit
+//    and stages the cell, and the commit clears it and queues the round's
+//    best proposal per cell for further propagation — the same winner as if
+//    every proposal had competed with the value at the start of the round.  Sixteen consecutive buckets (the
 //    window) have their own lists; states beyond the window wait in a far list
 //    and are moved into the window, each to its exact bucket, when the window
 //    runs empty.  So every state is relaxed in the round of its own bucket,
@@ -51,8 +54,13 @@
 namespace m2s {
 namespace {
 
-constexpr uint32_t NO_TRI = 0xFFFFFFFFu;
-constexpr unsigned long long KEY_EMPTY = (0x7F7FFFFFull << 32) | 0xFFFFFFFFull;  // (f32::MAX, none)
+// A cell's 64-bit key: the f32 distance bits (high word), the triangle
+// (bits 1..31; a job holds fewer than 2^31 - 1 triangles) and bit 0, kDirty:
+// set while the cell has been lowered in the current relax round and not yet
+// committed.  Between rounds every key is clean.
+constexpr uint32_t NO_TRI = 0x7FFFFFFFu;
+constexpr unsigned long long kDirty = 1ull;
+constexpr unsigned long long KEY_EMPTY = (0x7F7FFFFFull << 32) | ((unsigned long long)NO_TRI << 1);  // (f32::MAX, none)
 constexpr int kRing = 16;           // buckets of the window
 constexpr int kCur0 = kRing;        // list relaxed first (empty)
 constexpr int kFar0 = kRing + 1;    // far lists kFar0 and kFar0 + 1 (ping-pong)
@@ -230,14 +238,15 @@ __device__ __forceinline__ float cell_distance(P3 pos, P3 a, P3 b, P3 c, int kin
 }
 
 __device__ __forceinline__ unsigned long long pack(float d, uint32_t tri) {
-  return ((unsigned long long)__float_as_uint(d) << 32) | tri;
+  return ((unsigned long long)__float_as_uint(d) << 32) | ((unsigned long long)tri << 1);
 }
 __device__ __forceinline__ float key_dist(unsigned long long k) { return __uint_as_float((uint32_t)(k >> 32)); }
-__device__ __forceinline__ uint32_t key_tri(unsigned long long k) { return (uint32_t)k; }
+__device__ __forceinline__ uint32_t key_tri(unsigned long long k) { return (uint32_t)k >> 1; }
 
 // Does `cand` beat `cur`?  Raycast: plain order of non-negative distances,
-// ties to the lower triangle.  Normal: compare_distances (lib.rs:315-332),
-// exact ties to the lower triangle.
+// ties to the lower triangle (a proposal's dirty bit never beats the same
+// distance and triangle).  Normal: compare_distances (lib.rs:315-332), exact
+// ties to the lower triangle; the dirty bit is ignored.
 template <int SIGN>
 __device__ __forceinline__ bool beats(unsigned long long cand, unsigned long long cur, bool* nan) {
   if (SIGN == M2S_SIGN_RAYCAST) return cand < cur;
@@ -246,19 +255,21 @@ __device__ __forceinline__ bool beats(unsigned long long cand, unsigned long lon
   return c == -1 || (c == 0 && (uint32_t)(cand >> 32) == (uint32_t)(cur >> 32) && key_tri(cand) < key_tri(cur));
 }
 
-// Lowers *slot to cand if cand beats it; returns true when this call moved the
-// cell off `snap`, its value at the start of the round — exactly one proposal
-// per touched cell and round sees that.
+// Lowers *slot to cand (a proposal, dirty bit set) if cand beats it; returns
+// true when this call lowered a clean key — the cell's first lowering of the
+// round, which exactly one proposal per touched cell makes.  `seen` is the
+// key as the proposal read it, the first guess of the exchange.
 template <int SIGN>
-__device__ __forceinline__ bool improve_first(unsigned long long* slot, unsigned long long cand, unsigned long long snap,
+__device__ __forceinline__ bool improve_first(unsigned long long* slot, unsigned long long cand, unsigned long long seen,
                                               bool* nan) {
-  if (SIGN == M2S_SIGN_RAYCAST) return atomicMin(slot, cand) == snap;
-  // The slot still holds the snapshot unless another proposal of this round
-  // won it already, so the snapshot is the first guess of the exchange.
-  unsigned long long old = snap;
+  if (SIGN == M2S_SIGN_RAYCAST) {
+    const unsigned long long old = atomicMin(slot, cand);
+    return cand < old && !(old & kDirty);
+  }
+  unsigned long long old = seen;
   while (beats<SIGN>(cand, old, nan)) {
     unsigned long long prev = atomicCAS(slot, old, cand);
-    if (prev == old) return old == snap;
+    if (prev == old) return !(old & kDirty);
     old = prev;
   }
   return false;
@@ -278,13 +289,13 @@ __device__ __forceinline__ bool update_min(unsigned long long* slot, unsigned lo
 
 // ---- the propagation's proposal filter -------------------------------------
 // Most proposals cannot win (on the star s6 256^3 grid under 5 % beat the
-// snapshot), and a proposal's closest-point evaluation is most of its cost.
+// cell's key), and a proposal's closest-point evaluation is most of its cost.
 // A triangle lies in its plane and, inside that plane, on the inner side of
 // each of its three edge lines, so the distance from p to the triangle is at
 // least sqrt(h^2 + o^2), where h is p's distance to the plane and o the
 // largest distance of p's projection outside an edge line.  A proposal whose
-// bound already exceeds the snapshot's distance by a slack far above the
-// rounding of both computations cannot beat the snapshot (for Normal: not
+// bound already exceeds the key's distance by a slack far above the
+// rounding of both computations cannot beat the key (for Normal: not
 // even enter compare_distances' tie band), so it is dropped unevaluated.
 // Results are unchanged; the filter only skips work whose outcome is known.
 //
@@ -294,7 +305,7 @@ __device__ __forceinline__ bool update_min(unsigned long long* slot, unsigned lo
 struct __align__(16) TriBound {
   float4 n, e0, e1, e2;
 };
-// Slack of the test, relative to the snapshot distance and per unit of the
+// Slack of the test, relative to the key's distance and per unit of the
 // largest coordinate magnitude involved (the point's and the triangle's: the
 // f32 closest-point arithmetic errs by a few ulps of these; the slack is
 // about a thousand times that).
@@ -346,8 +357,8 @@ __global__ void k_bounds(const TriRec* __restrict__ tris, uint32_t T, TriBound* 
   }
 }
 
-// True when triangle `tb` (slack `sl`) provably cannot beat the snapshot key
-// at the cell centre p.
+// True when triangle `tb` (slack `sl`) provably cannot beat the cell key
+// `snap` at the cell centre p.
 template <int SIGN>
 __device__ __forceinline__ bool bound_rejects(const TriBound& tb, float sl, P3 p, unsigned long long snap) {
   const float h = fmaf(tb.n.x, p.x, fmaf(tb.n.y, p.y, fmaf(tb.n.z, p.z, -tb.n.w)));
@@ -692,7 +703,7 @@ struct WarpQueue {
 };
 constexpr int kWarps = 8;  // k_propagate runs 256 threads per block
 
-// Stages cell j, which this proposal moved off its snapshot value, for the
+// Stages cell j, whose first lowering of the round this proposal made, for the
 // block's commit (spilling to the round's global list when the stage is full).
 __device__ __forceinline__ void stage_touch(uint32_t j, uint32_t* s_touch, uint32_t* s_ntouch, PropState* st,
                                             uint32_t parity, uint32_t* spill, uint32_t cap) {
@@ -726,25 +737,25 @@ __device__ __forceinline__ bool neighbour_cell(const GridSet& gs, uint2 ent, uin
 }
 
 // Distance of triangle tri (record r) at cell j, centre pos, against the
-// cell's snapshot key; true when this proposal moved the cell off the
-// snapshot (it is then the cell's one staging proposal of the round).
+// cell's key as read (`seen`); true when this proposal made the cell's first
+// lowering of the round (it is then the cell's one staging proposal).
 template <int SIGN>
-__device__ __forceinline__ bool propose_at(const TriRec& r, uint32_t tri, uint32_t j, P3 pos, unsigned long long snap,
-                                           unsigned long long* work_keys, bool& nan) {
+__device__ __forceinline__ bool propose_at(const TriRec& r, uint32_t tri, uint32_t j, P3 pos, unsigned long long seen,
+                                           unsigned long long* keys, bool& nan) {
   const float d = cell_distance<SIGN>(pos, p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
   if (isnan(d)) nan = true;
-  const unsigned long long cand = pack(d, tri);
-  return beats<SIGN>(cand, snap, &nan) && improve_first<SIGN>(&work_keys[j], cand, snap, &nan);
+  const unsigned long long cand = pack(d, tri) | kDirty;
+  return beats<SIGN>(cand, seen, &nan) && improve_first<SIGN>(&keys[j], cand, seen, &nan);
 }
 
 // A solo round (block 0 alone, n <= kSoloCap states) forms the round's minima
-// in a table in shared memory instead of in the working keys: a proposal
-// that beats its cell's snapshot meets the cell's other proposals in the
-// cell's slot (open addressing, linear probing; at most 26 * kSoloCap cells
-// ever take a slot, fewer than kHash), and the commit writes each slot's
-// winner to both key arrays.  The round saves the working-key atomic and the
-// commit's read of it: two dependent trips to L2 of the few a solo round
-// waits for.  The table occupies the block's touch stage, free in a solo run.
+// in a table in shared memory instead of in the keys: a proposal that beats
+// its cell's key meets the cell's other proposals in the cell's slot (open
+// addressing, linear probing; at most 26 * kSoloCap cells ever take a slot,
+// fewer than kHash), and the commit writes each slot's winner to the key.
+// The round saves the key atomic and the commit's read of it: two dependent
+// trips to L2 of the few a solo round waits for.  The table occupies the
+// block's touch stage, free in a solo run.
 constexpr uint32_t kHash = 2048;
 constexpr uint32_t kNoCell = 0xFFFFFFFFu;
 static_assert(26 * kSoloCap < kHash, "a solo round could fill the table");
@@ -752,10 +763,10 @@ static_assert(kHash * 3 <= (uint32_t)kTouchStage, "the table exceeds the touch s
 
 __device__ __forceinline__ uint32_t hash_slot(uint32_t j) { return (j * 2654435761u) >> 21; }  // 11 bits
 
-// Lowers cell j's slot to cand (which beats the cell's snapshot) if it beats
-// the slot's value; a slot taken here is listed for the commit.  Slots start
-// as (kNoCell, KEY_EMPTY); every candidate that beats a snapshot beats
-// KEY_EMPTY too, the order being a total one.
+// Lowers cell j's slot to cand (which beats the cell's key) if it beats the
+// slot's value; a slot taken here is listed for the commit.  Slots start as
+// (kNoCell, KEY_EMPTY); every candidate that beats a key beats KEY_EMPTY too,
+// the order being a total one.  Solo candidates are clean keys.
 template <int SIGN>
 __device__ __forceinline__ void table_improve(uint32_t* HJ, unsigned long long* HK, uint16_t* taken,
                                               uint32_t* ntaken, uint32_t j, unsigned long long cand, bool& nan) {
@@ -784,7 +795,7 @@ __device__ __forceinline__ void table_improve(uint32_t* HJ, unsigned long long* 
 // A neighbour that holds the state's triangle already cannot gain.
 template <int SIGN, bool MULTI>
 __device__ __forceinline__ void relax_propose_solo(const GridSet& gs, const TriRec* __restrict__ tris,
-                                                   const unsigned long long* snap_keys, const uint2* list, uint32_t n,
+                                                   const unsigned long long* keys, const uint2* list, uint32_t n,
                                                    uint32_t* HJ, unsigned long long* HK, uint16_t* taken,
                                                    uint32_t* ntaken, bool& nan, unsigned long long& evals,
                                                    uint32_t& dropped_same) {
@@ -795,7 +806,7 @@ __device__ __forceinline__ void relax_propose_solo(const GridSet& gs, const TriR
     int X, Y, Z;
     if (!neighbour_cell<MULTI>(gs, ent, p % 26u, j, X, Y, Z)) continue;
     ++evals;
-    const unsigned long long snap = __ldcg(&snap_keys[j]);
+    const unsigned long long snap = __ldcg(&keys[j]);
     const TriRec r = tris[ent.y];
     if (key_tri(snap) == ent.y) {
       ++dropped_same;
@@ -810,10 +821,9 @@ __device__ __forceinline__ void relax_propose_solo(const GridSet& gs, const TriR
 }
 
 // Commit phase of a solo round: every taken slot's winner becomes the cell's
-// snapshot and working key and is queued under its bucket; the slot is freed.
+// key and is queued under its bucket; the slot is freed.
 template <bool MULTI>
-__device__ __forceinline__ void relax_commit_solo(const GridSet& gs, unsigned long long* snap_keys,
-                                                  unsigned long long* work_keys, uint32_t* HJ,
+__device__ __forceinline__ void relax_commit_solo(const GridSet& gs, unsigned long long* keys, uint32_t* HJ,
                                                   unsigned long long* HK, const uint16_t* taken, uint32_t ntaken,
                                                   const Counters& ct, const Sched& sh, uint2* lists, uint32_t cap) {
   for (uint32_t base = 0; base < ntaken; base += blockDim.x) {  // warp-uniform trip count
@@ -825,8 +835,7 @@ __device__ __forceinline__ void relax_commit_solo(const GridSet& gs, unsigned lo
       const uint32_t h = taken[i];
       j = HJ[h];
       w = HK[h];
-      snap_keys[j] = w;
-      work_keys[j] = w;
+      keys[j] = w;
       nb = bucket_of(grid_of_tri<MULTI>(gs, key_tri(w)).inv_delta, key_dist(w));
       HJ[h] = kNoCell;
       HK[h] = KEY_EMPTY;
@@ -843,11 +852,11 @@ __device__ __forceinline__ void relax_commit_solo(const GridSet& gs, unsigned lo
 // With the filter (the default), a proposal is dropped unevaluated when the
 // neighbour already holds the same triangle (the distance of a (cell,
 // triangle) pair is one deterministic value, so it cannot gain) or when the
-// triangle's distance bound proves that it cannot beat the snapshot; each
+// triangle's distance bound proves that it cannot beat the cell's key; each
 // warp queues the rest in shared memory and evaluates them 32 at a time with
 // every lane busy.  The work unit is a row: state e and a (dx, dy) offset, the
 // three neighbours at z - 1, z, z + 1 (nine rows per state; the state's own
-// cell is left out of its row).  A row's three snapshot keys are adjacent, so
+// cell is left out of its row).  A row's three keys are adjacent, so
 // a thread issues their loads together and they share a memory sector; the
 // bound's plane values are formed once at the row's middle cell and moved
 // along z by one addition each (the slack covers that rounding); only a
@@ -860,8 +869,7 @@ __device__ __forceinline__ void relax_commit_solo(const GridSet& gs, unsigned lo
 template <int SIGN, bool MULTI, bool FILTER>
 __device__ __forceinline__ void relax_propose(const GridSet& gs, const TriRec* __restrict__ tris,
                                               const TriBound* __restrict__ bounds, const float* __restrict__ slack,
-                                              const unsigned long long* snap_keys,
-                                              unsigned long long* work_keys, const uint2* list, uint32_t n,
+                                              unsigned long long* keys, const uint2* list, uint32_t n,
                                               uint32_t T, uint32_t t0, uint32_t* s_touch, uint32_t* s_ntouch,
                                               PropState* st, uint32_t parity, uint32_t* spill, uint32_t cap,
                                               bool& nan, unsigned long long& evals, uint32_t& dropped_same,
@@ -870,7 +878,7 @@ __device__ __forceinline__ void relax_propose(const GridSet& gs, const TriRec* _
   uint32_t qn = 0;  // warp-uniform queue length, < 32 between pushes
   auto run = [&](uint32_t i) {
     const uint32_t tri = q->tri[i], j = q->j[i];
-    if (propose_at<SIGN>(tris[tri], tri, j, P3{q->px[i], q->py[i], q->pz[i]}, q->snap[i], work_keys, nan))
+    if (propose_at<SIGN>(tris[tri], tri, j, P3{q->px[i], q->py[i], q->pz[i]}, q->snap[i], keys, nan))
       stage_touch(j, s_touch, s_ntouch, st, parity, spill, cap);
   };
   // Called by all 32 lanes: queues this lane's proposal if `keep`, and
@@ -930,7 +938,7 @@ __device__ __forceinline__ void relax_propose(const GridSet& gs, const TriRec* _
           on[2] = z + 1 < g.n[2];
 #pragma unroll
           for (int d = 0; d < 3; ++d)
-            if (on[d]) snap[d] = __ldcg(&snap_keys[j0 + d - 1]);
+            if (on[d]) snap[d] = __ldcg(&keys[j0 + d - 1]);
         }
       }
       bool keep[3] = {false, false, false};
@@ -1006,7 +1014,7 @@ __device__ __forceinline__ void relax_propose(const GridSet& gs, const TriRec* _
           if (eu >= n || !neighbour(eu, ku, tri, j, X, Y, Z)) continue;
           ++evals;
           const P3 pos = center(grid_of_tri<MULTI>(gs, tri), X, Y, Z);
-          first[u] = propose_at<SIGN>(tris[tri], tri, j, pos, __ldcg(&snap_keys[j]), work_keys, nan);
+          first[u] = propose_at<SIGN>(tris[tri], tri, j, pos, __ldcg(&keys[j]), keys, nan);
           jj[u] = j;
         }
 #pragma unroll
@@ -1025,7 +1033,7 @@ __device__ __forceinline__ void relax_propose(const GridSet& gs, const TriRec* _
       bool keep = false;
       if (eu < n && neighbour(eu, ku, tri, j, X, Y, Z)) {
         ++evals;
-        snap = __ldcg(&snap_keys[j]);
+        snap = __ldcg(&keys[j]);
         pos = center(grid_of_tri<MULTI>(gs, tri), X, Y, Z);
         if (key_tri(snap) == tri) ++dropped_same;
         else keep = true;
@@ -1038,12 +1046,12 @@ __device__ __forceinline__ void relax_propose(const GridSet& gs, const TriRec* _
   __syncwarp();
 }
 
-// Commit phase: publish each touched cell's round winner to the snapshot and
-// queue (cell, winner) under the winner's bucket.  A block commits the cells
-// it staged; the spill list is shared out as spill_t0 + k * spill_T.
+// Commit phase: clear each touched cell's dirty bit (its key holds the
+// round's winner) and queue (cell, winner) under the winner's bucket.  A block
+// commits the cells it staged; the spill list is shared out as
+// spill_t0 + k * spill_T.
 template <bool MULTI>
-__device__ __forceinline__ void relax_commit(const GridSet& gs, unsigned long long* snap_keys,
-                                             const unsigned long long* work_keys, const uint32_t* s_touch,
+__device__ __forceinline__ void relax_commit(const GridSet& gs, unsigned long long* keys, const uint32_t* s_touch,
                                              uint32_t nloc, const uint32_t* spill, uint32_t nspill, uint32_t spill_t0,
                                              uint32_t spill_T, const Counters& ct, const Sched& sh, uint2* lists,
                                              uint32_t cap) {
@@ -1054,8 +1062,8 @@ __device__ __forceinline__ void relax_commit(const GridSet& gs, unsigned long lo
     unsigned long long w = KEY_EMPTY;
     if (act) {
       j = s_touch[i];
-      w = __ldcg(&work_keys[j]);
-      snap_keys[j] = w;
+      w = __ldcg(&keys[j]) & ~kDirty;
+      keys[j] = w;
       nb = bucket_of(grid_of_tri<MULTI>(gs, key_tri(w)).inv_delta, key_dist(w));
     }
     push_entry_warp(ct, sh.b, sh.B, sh.slot, sh.fp, lists, cap, act, j, key_tri(w), nb);
@@ -1067,8 +1075,8 @@ __device__ __forceinline__ void relax_commit(const GridSet& gs, unsigned long lo
     unsigned long long w = KEY_EMPTY;
     if (act) {
       j = __ldcg(&spill[i]);
-      w = __ldcg(&work_keys[j]);
-      snap_keys[j] = w;
+      w = __ldcg(&keys[j]) & ~kDirty;
+      keys[j] = w;
       nb = bucket_of(grid_of_tri<MULTI>(gs, key_tri(w)).inv_delta, key_dist(w));
     }
     push_entry_warp(ct, sh.b, sh.B, sh.slot, sh.fp, lists, cap, act, j, key_tri(w), nb);
@@ -1080,7 +1088,7 @@ __device__ __forceinline__ void relax_commit(const GridSet& gs, unsigned long lo
 // propose loop needs about 80 registers, so that variant runs 3 per SM.
 template <int SIGN, bool MULTI, bool FILTER>
 __global__ void __launch_bounds__(256, FILTER ? 3 : 4) k_propagate(const __grid_constant__ GridSet gs, const TriRec* __restrict__ tris,
-                                                   unsigned long long* snap_keys, unsigned long long* work_keys,
+                                                   unsigned long long* keys,
                                                    uint2* lists, uint32_t cap, uint32_t* spill_lists,
                                                    PropState* st, GridBarrier* bar, uint32_t max_steps,
                                                    uint32_t* status, uint32_t* round_log, uint32_t log_cap,
@@ -1258,10 +1266,10 @@ __global__ void __launch_bounds__(256, FILTER ? 3 : 4) k_propagate(const __grid_
     uint32_t* HJ = s_touch;
     unsigned long long* HK = reinterpret_cast<unsigned long long*>(s_touch + kHash);
     if (solo)
-      relax_propose_solo<SIGN, MULTI>(gs, tris, snap_keys, lists + (unsigned long long)sh.cur * cap, n, HJ, HK,
+      relax_propose_solo<SIGN, MULTI>(gs, tris, keys, lists + (unsigned long long)sh.cur * cap, n, HJ, HK,
                                       s_taken, &s_ntouch, nan, evals, dropped_same);
     else
-      relax_propose<SIGN, MULTI, FILTER>(gs, tris, bounds, slack, snap_keys, work_keys,
+      relax_propose<SIGN, MULTI, FILTER>(gs, tris, bounds, slack, keys,
                                  lists + (unsigned long long)sh.cur * cap, n, T, t0, s_touch, &s_ntouch, st, parity,
                                  spill, cap, nan, evals, dropped_same, dropped_bound,
                                          &s_queue[kQueued ? threadIdx.x >> 5 : 0]);
@@ -1273,12 +1281,12 @@ __global__ void __launch_bounds__(256, FILTER ? 3 : 4) k_propagate(const __grid_
       break;
     }
     if (solo) {
-      relax_commit_solo<MULTI>(gs, snap_keys, work_keys, HJ, HK, s_taken, min(s_ntouch, 26u * kSoloCap),
+      relax_commit_solo<MULTI>(gs, keys, HJ, HK, s_taken, min(s_ntouch, 26u * kSoloCap),
                                counters(true), sh, lists, cap);
     } else {
       if (lead_block && threadIdx.x == 0) st->touched2[parity ^ 1u] = 0;
       const uint32_t nspill = min(*(volatile uint32_t*)&st->touched2[parity], cap);
-      relax_commit<MULTI>(gs, snap_keys, work_keys, s_touch, min(s_ntouch, (uint32_t)kTouchStage), spill, nspill, t0,
+      relax_commit<MULTI>(gs, keys, s_touch, min(s_ntouch, (uint32_t)kTouchStage), spill, nspill, t0,
                           T, global_counters(st), sh, lists, cap);
     }
     if (!solo) {
@@ -1592,7 +1600,7 @@ struct GridJob::Impl {
   DevBuf<uint32_t> tri_grid, tri_off, cell_off;
   DevBuf<unsigned long long> col_off[3];
   DevBuf<GridK> table;
-  DevBuf<unsigned long long> snap, work;
+  DevBuf<unsigned long long> keys;  // one per cell
   DevBuf<PropState> state;
   DevBuf<GridBarrier> bar;
   DevBuf<uint32_t> bits;
@@ -1626,7 +1634,7 @@ int GridJob::sign() const { return p->sign; }
 uint32_t GridJob::grids() const { return p->gs.ngrids; }
 uint64_t GridJob::device_bytes() const {
   const Impl& J = *p;
-  return J.comb_tris.n * sizeof(TriRec) + J.tri_grid.n * 4 + (J.snap.n + J.work.n) * 8 + J.bits.n * 4 +
+  return J.comb_tris.n * sizeof(TriRec) + J.tri_grid.n * 4 + J.keys.n * 8 + J.bits.n * 4 +
          J.bounds.n * sizeof(TriBound) + J.slack.n * 4 +
          (uint64_t)kLists * J.cap * 8 + 2ull * J.cap * 4 + J.table.n * sizeof(GridK);
 }
@@ -1648,7 +1656,7 @@ uint32_t default_list_capacity(uint64_t cells) {
 uint64_t grid_job_bytes(uint64_t cells) {
   const uint64_t cap = default_list_capacity(cells);
   const uint64_t ray_words = 3 * (cells / 32 + 3 * std::cbrt((double)cells) * std::cbrt((double)cells));
-  return 16 * cells + (uint64_t)kLists * 8 * cap + 8 * cap + 4 * ray_words + (1u << 20);  // + 68 B per triangle
+  return 8 * cells + (uint64_t)kLists * 8 * cap + 8 * cap + 4 * ray_words + (1u << 20);  // + 68 B per triangle
 }
 
 int check_grid(const GridDesc& g) {
@@ -1750,7 +1758,7 @@ int GridJob::prepare(const MeshView* meshes, uint32_t n, const GridDesc* gds, in
     J.tris = meshes[0].tris;
   }
   const unsigned long long N = cells;
-  if ((st = J.snap.alloc(N, s)) || (st = J.work.alloc(N, s)) || (st = J.state.alloc(1, s)) ||
+  if ((st = J.keys.alloc(N, s)) || (st = J.state.alloc(1, s)) ||
       (st = J.bar.alloc(1, s)))
     return st;
   J.filter = tune.bound_filter;
@@ -1806,16 +1814,16 @@ int GridJob::enqueue(cudaStream_t s, cudaEvent_t* ev) {
   if ((st = mark(0))) return st;
   M2S_CUDA(cudaMemsetAsync(J.state.p, 0, sizeof(PropState), s));
   k_state_init<<<1, 1, 0, s>>>(J.state.p);
-  k_fill_u64<<<blocks_for(N, 256), 256, 0, s>>>(J.snap.p, N, KEY_EMPTY);
+  k_fill_u64<<<blocks_for(N, 256), 256, 0, s>>>(J.keys.p, N, KEY_EMPTY);
   J.launches += 2;
   if (J.T > 0) {
     const unsigned sb = (unsigned)((J.T * 32ull + 255) / 256);
     if (raycast) {
-      if (multi) k_seed<M2S_SIGN_RAYCAST, true><<<sb, 256, 0, s>>>(J.gs, J.tris, J.T, J.snap.p, J.d_status, J.state.p);
-      else k_seed<M2S_SIGN_RAYCAST, false><<<sb, 256, 0, s>>>(J.gs, J.tris, J.T, J.snap.p, J.d_status, J.state.p);
+      if (multi) k_seed<M2S_SIGN_RAYCAST, true><<<sb, 256, 0, s>>>(J.gs, J.tris, J.T, J.keys.p, J.d_status, J.state.p);
+      else k_seed<M2S_SIGN_RAYCAST, false><<<sb, 256, 0, s>>>(J.gs, J.tris, J.T, J.keys.p, J.d_status, J.state.p);
     } else {
-      if (multi) k_seed<M2S_SIGN_NORMAL, true><<<sb, 256, 0, s>>>(J.gs, J.tris, J.T, J.snap.p, J.d_status, J.state.p);
-      else k_seed<M2S_SIGN_NORMAL, false><<<sb, 256, 0, s>>>(J.gs, J.tris, J.T, J.snap.p, J.d_status, J.state.p);
+      if (multi) k_seed<M2S_SIGN_NORMAL, true><<<sb, 256, 0, s>>>(J.gs, J.tris, J.T, J.keys.p, J.d_status, J.state.p);
+      else k_seed<M2S_SIGN_NORMAL, false><<<sb, 256, 0, s>>>(J.gs, J.tris, J.T, J.keys.p, J.d_status, J.state.p);
     }
     ++J.launches;
   }
@@ -1823,13 +1831,12 @@ int GridJob::enqueue(cudaStream_t s, cudaEvent_t* ev) {
   if ((st = mark(1))) return st;
   if (J.T > 0) {
     M2S_CUDA(cudaMemsetAsync(J.bar.p, 0, sizeof(GridBarrier), s));
-    M2S_CUDA(cudaMemcpyAsync(J.work.p, J.snap.p, N * 8, cudaMemcpyDeviceToDevice, s));
     if (J.filter) {
       k_bounds<<<blocks_for(J.T, 256), 256, 0, s>>>(J.tris, J.T, J.bounds.p, J.slack.p);
       ++J.launches;
     }
-    if (multi) k_collect<true><<<blocks_for(N, 256), 256, 0, s>>>(J.gs, J.snap.p, J.state.p, J.lists.p, J.cap);
-    else k_collect<false><<<blocks_for(N, 256), 256, 0, s>>>(J.gs, J.snap.p, J.state.p, J.lists.p, J.cap);
+    if (multi) k_collect<true><<<blocks_for(N, 256), 256, 0, s>>>(J.gs, J.keys.p, J.state.p, J.lists.p, J.cap);
+    else k_collect<false><<<blocks_for(N, 256), 256, 0, s>>>(J.gs, J.keys.p, J.state.p, J.lists.p, J.cap);
     M2S_CUDA(cudaGetLastError());
     const void* kern = raycast ? propagate_kernel<M2S_SIGN_RAYCAST>(multi, J.filter)
                                : propagate_kernel<M2S_SIGN_NORMAL>(multi, J.filter);
@@ -1837,7 +1844,7 @@ int GridJob::enqueue(cudaStream_t s, cudaEvent_t* ev) {
     const TriRec* tris = J.tris;
     uint32_t* log = J.round_log.p;
     uint32_t log_cap = (uint32_t)(J.round_log.n / 2);
-    void* args[] = {&J.gs,     &tris,   &J.snap.p,  &J.work.p,    &J.lists.p, &J.cap,     &J.touched.p,
+    void* args[] = {&J.gs,     &tris,   &J.keys.p,  &J.lists.p, &J.cap,     &J.touched.p,
                     &J.state.p, &J.bar.p, &max_steps, &J.d_status, &log,       &log_cap, &J.solo_max,
                     &J.bounds.p, &J.slack.p};
     cudaLaunchConfig_t cfg{};
@@ -1893,22 +1900,22 @@ int GridJob::enqueue(cudaStream_t s, cudaEvent_t* ev) {
     J.launches += J.audit ? 6 : 3;
     M2S_CUDA(cudaGetLastError());
     if ((st = mark(3))) return st;
-    if (multi) k_finalize<M2S_SIGN_RAYCAST, true><<<fb, 256, 0, s>>>(J.gs, J.snap.p, J.bits.p, J.d_out);
-    else k_finalize<M2S_SIGN_RAYCAST, false><<<fb, 256, 0, s>>>(J.gs, J.snap.p, J.bits.p, J.d_out);
+    if (multi) k_finalize<M2S_SIGN_RAYCAST, true><<<fb, 256, 0, s>>>(J.gs, J.keys.p, J.bits.p, J.d_out);
+    else k_finalize<M2S_SIGN_RAYCAST, false><<<fb, 256, 0, s>>>(J.gs, J.keys.p, J.bits.p, J.d_out);
   } else {
     if ((st = mark(3))) return st;
-    if (multi) k_finalize<M2S_SIGN_NORMAL, true><<<fb, 256, 0, s>>>(J.gs, J.snap.p, nullptr, J.d_out);
-    else k_finalize<M2S_SIGN_NORMAL, false><<<fb, 256, 0, s>>>(J.gs, J.snap.p, nullptr, J.d_out);
+    if (multi) k_finalize<M2S_SIGN_NORMAL, true><<<fb, 256, 0, s>>>(J.gs, J.keys.p, nullptr, J.d_out);
+    else k_finalize<M2S_SIGN_NORMAL, false><<<fb, 256, 0, s>>>(J.gs, J.keys.p, nullptr, J.d_out);
   }
   M2S_CUDA(cudaGetLastError());
   ++J.launches;
   if (J.audit) {  // reports only: the output is written already
     if (raycast) {
-      if (multi) k_audit_cells<M2S_SIGN_RAYCAST, true><<<fb, 256, 0, s>>>(J.gs, J.tris, J.snap.p, J.bits.p, J.bits64.p, J.state.p);
-      else k_audit_cells<M2S_SIGN_RAYCAST, false><<<fb, 256, 0, s>>>(J.gs, J.tris, J.snap.p, J.bits.p, J.bits64.p, J.state.p);
+      if (multi) k_audit_cells<M2S_SIGN_RAYCAST, true><<<fb, 256, 0, s>>>(J.gs, J.tris, J.keys.p, J.bits.p, J.bits64.p, J.state.p);
+      else k_audit_cells<M2S_SIGN_RAYCAST, false><<<fb, 256, 0, s>>>(J.gs, J.tris, J.keys.p, J.bits.p, J.bits64.p, J.state.p);
     } else {
-      if (multi) k_audit_cells<M2S_SIGN_NORMAL, true><<<fb, 256, 0, s>>>(J.gs, J.tris, J.snap.p, nullptr, nullptr, J.state.p);
-      else k_audit_cells<M2S_SIGN_NORMAL, false><<<fb, 256, 0, s>>>(J.gs, J.tris, J.snap.p, nullptr, nullptr, J.state.p);
+      if (multi) k_audit_cells<M2S_SIGN_NORMAL, true><<<fb, 256, 0, s>>>(J.gs, J.tris, J.keys.p, nullptr, nullptr, J.state.p);
+      else k_audit_cells<M2S_SIGN_NORMAL, false><<<fb, 256, 0, s>>>(J.gs, J.tris, J.keys.p, nullptr, nullptr, J.state.p);
     }
     M2S_CUDA(cudaGetLastError());
     ++J.launches;

@@ -189,7 +189,7 @@ struct GridTuning {
   uint32_t cells_per_block = 1024;   // cooperative grid = ceil(cells / this) blocks, at least one per SM
   uint32_t list_capacity = 0;        // entries per bucket list (0: derived from the cell count)
   // A batch runs as jobs ("waves") of at most this many cells each (a larger
-  // grid alone), so a job's 16 bytes of keys per cell stay near L2 size.
+  // grid alone), which bounds a job's keys (8 bytes per cell) and lists.
   uint64_t wave_cells = 1ull << 26;
   // Relax rounds of at most this many states run on one block, with block
   // barriers only (0: every round on every block).
