@@ -244,6 +244,16 @@ __device__ __forceinline__ int compare_distances(float a, float b, bool* nan) {
   return 0;
 }
 
+// A fold under compare_distances (`best` replaced by each d it puts before
+// it) only takes a d with |d| <= B + one tie band, B = |best|: a larger
+// magnitude can win only by the sign rule inside the band.  A replacement
+// that raises the magnitude leaves a positive best, which the next such
+// raise needs to be negative, so no fold from |best| = B ever holds a value
+// above B + one band (at most max(1e-6, 2 ulps of B)).  fold_reach(B) is B
+// plus two bands with room for rounding: a d with |d| > fold_reach(B) is
+// before no value of such a fold.  `!(|d| > reach)` keeps NaN distances.
+__device__ __forceinline__ float fold_reach(float B) { return fmaf(B, 1.0f + 0x1p-19f, 4.0e-6f); }
+
 // geo.rs:4-22: AABB grown by 1e-4 on every side (f32 min/max then -/+ 1e-4).
 __device__ __forceinline__ void padded_box(P3 a, P3 b, P3 c, P3* lo, P3* hi) {
   const float e = 0.0001f;

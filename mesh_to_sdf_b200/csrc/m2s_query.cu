@@ -78,6 +78,7 @@ __global__ void __launch_bounds__(kBfThreads) k_brute(const TriRec* __restrict__
   }
 
   float best = SIGN == 0 ? INFINITY : F32_MAX;  // Raycast keeps the squared distance
+  float reach = INFINITY;                         // Normal: fold_reach(|best|)
   uint32_t hits = 0;
   bool nan = false, lost = false;
   for (uint32_t i = 0; i < ntile; ++i) {
@@ -98,9 +99,13 @@ __global__ void __launch_bounds__(kBfThreads) k_brute(const TriRec* __restrict__
           float t;
           hits += ray_hit_aligned<0>(p, a, b, c, &t) ? 1u : 0u;
         } else {
-          // default.rs:51-53 then :63-70 — compare_distances fold.
+          // default.rs:51-53 then :63-70 — compare_distances fold; a d
+          // beyond the fold's reach cannot be before best.
           float d = point_triangle_signed_distance(p, a, b, c, kind);
-          if (compare_distances(d, best, &nan) == -1) best = d;
+          if (!(fabsf(d) > reach) && compare_distances(d, best, &nan) == -1) {
+            best = d;
+            reach = fold_reach(fabsf(best));
+          }
         }
       }
     }
@@ -148,7 +153,10 @@ __global__ void k_brute_finish(const uint2* __restrict__ part, uint64_t nq, floa
 // before `best` replaces it, and only the lanes after it are tested again,
 // against the new value, until none is before it.  That is the reference's
 // sequential fold (default.rs:63-70) step for step, with 32 triangles
-// evaluated at a time, so a batch of few queries still fills the GPU.
+// evaluated at a time, so a batch of few queries still fills the GPU.  Lanes
+// whose |d| lies beyond fold_reach of the group's first best cannot be
+// before any value the group's fold takes and are left out at once; most
+// groups then need no compare_distances at all.
 constexpr int kBwThreads = 256;                 // 8 queries per block
 constexpr uint64_t kBruteWarpMaxQueries = 1u << 17;  // below: one warp per query
 constexpr uint64_t kBruteSortMinPairs = 1ull << 28;  // from here the thread kernels visit queries in Morton order
@@ -194,7 +202,8 @@ __global__ void __launch_bounds__(kBwThreads) k_brute_normal_warp(const TriRec* 
           const float4 ra = tl[j].a, rb = tl[j].b, rc = tl[j].c;
           d = point_triangle_signed_distance(p, p3(ra), p3(rb), p3(rc), __float_as_int(ra.w));
         }
-        uint32_t todo = __ballot_sync(0xFFFFFFFFu, have);  // lanes not folded yet
+        // lanes not folded yet; none beyond the reach of the group's first best
+        uint32_t todo = __ballot_sync(0xFFFFFFFFu, have && !(fabsf(d) > fold_reach(fabsf(best))));
         while (todo) {
           const bool before = ((todo >> lane) & 1u) && compare_distances(d, best, &nan) == -1;
           const uint32_t m = __ballot_sync(0xFFFFFFFFu, before);
