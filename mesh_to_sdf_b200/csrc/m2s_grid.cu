@@ -863,9 +863,13 @@ __device__ __forceinline__ void relax_commit_solo(const GridSet& gs, unsigned lo
 // survivor's exact cell centre is computed.  Units t0, t0 + T, ... advance as
 // (state, row) pairs without division: T = 9 * dE + dR.
 //
-// Without the filter, proposals are single (state, neighbour) pairs, T =
-// 26 * dE + dK: Raycast proposals are evaluated where they arise, kUnroll per
-// thread at a time, and Normal ones pass the same-triangle test and the queue.
+// Without the filter, Raycast proposals are evaluated where they arise.  In a
+// round of at least two row units per thread (9 n >= 2 T) the unit is a row as
+// above: one entry load, one coordinate decode and one triangle record serve
+// its three proposals, and the three keys are loaded together.  Smaller rounds
+// keep single (state, neighbour) pairs, T = 26 * dE + dK, kUnroll per thread at
+// a time, so that more threads share the round's few states.  Normal
+// proposals are single pairs that pass the same-triangle test and the queue.
 template <int SIGN, bool MULTI, bool FILTER>
 __device__ __forceinline__ void relax_propose(const GridSet& gs, const TriRec* __restrict__ tris,
                                               const TriBound* __restrict__ bounds, const float* __restrict__ slack,
@@ -999,6 +1003,48 @@ __device__ __forceinline__ void relax_propose(const GridSet& gs, const TriRec* _
         ++e;
       }
     };
+    if (SIGN == M2S_SIGN_RAYCAST && 9u * n >= 2u * T) {
+      const uint32_t dR = T / 9u, dRr = T % 9u;
+      uint32_t er = t0 / 9u, rr = t0 % 9u;
+      while (er < n) {
+        const uint32_t eu = er, row = rr;
+        rr += dRr;
+        er += dR;
+        if (rr >= 9u) {
+          rr -= 9u;
+          ++er;
+        }
+        const uint2 ent = __ldcg(&list[eu]);
+        const uint32_t tri = ent.y;
+        const GridK& g = grid_of_tri<MULTI>(gs, tri);
+        int x, y, z;
+        cell_coords(g, ent.x - g.cell_off, &x, &y, &z);
+        const int X = x + (int)(row / 3u) - 1, Y = y + (int)(row % 3u) - 1;  // iproduct order, x outermost
+        if ((unsigned)X >= (unsigned)g.n[0] || (unsigned)Y >= (unsigned)g.n[1]) continue;
+        const TriRec r = tris[tri];
+        const bool lo = z > 0, hi = z + 1 < g.n[2], mid = row != 4u;  // row 4's middle: the state's own cell
+        const uint32_t j0 = g.cell_off + local_index(g, X, Y, z) - 1u;   // the cell at z - 1
+        const unsigned long long k0 = lo ? __ldcg(&keys[j0]) : 0ull;
+        const unsigned long long k1 = mid ? __ldcg(&keys[j0 + 1]) : 0ull;
+        const unsigned long long k2 = hi ? __ldcg(&keys[j0 + 2]) : 0ull;
+        if (lo) {
+          ++evals;
+          if (propose_at<SIGN>(r, tri, j0, center(g, X, Y, z - 1), k0, keys, nan))
+            stage_touch(j0, s_touch, s_ntouch, st, parity, spill, cap);
+        }
+        if (mid) {
+          ++evals;
+          if (propose_at<SIGN>(r, tri, j0 + 1, center(g, X, Y, z), k1, keys, nan))
+            stage_touch(j0 + 1, s_touch, s_ntouch, st, parity, spill, cap);
+        }
+        if (hi) {
+          ++evals;
+          if (propose_at<SIGN>(r, tri, j0 + 2, center(g, X, Y, z + 1), k2, keys, nan))
+            stage_touch(j0 + 2, s_touch, s_ntouch, st, parity, spill, cap);
+        }
+      }
+      return;
+    }
     if (SIGN == M2S_SIGN_RAYCAST) {
       while (e < n) {
         bool first[kUnroll];
