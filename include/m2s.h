@@ -171,7 +171,7 @@ void m2s_clear_grid_autotune(void);
  * cells_per_block: the propagation launch uses ceil(cells / this) blocks, at
  * least one per SM (0 = 1024); wave_cells: a batch runs as jobs of at most this many
  * cells, largest grids first (a larger grid alone); grids in one job share its
- * rounds (0 = 64M; the server keeps its waves at 4M for latency); solo_max: propagation rounds of at most this
+ * rounds (0 = 128M; the server keeps its waves at 4M for latency); solo_max: propagation rounds of at most this
  * many states run on one block with block barriers only (0 = never, negative
  * = the default 64, at most 64). */
 void m2s_set_grid_tuning(int blocks_per_sm, uint32_t cells_per_block, uint64_t wave_cells, int solo_max);

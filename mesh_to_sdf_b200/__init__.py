@@ -556,7 +556,7 @@ class GridPlan:
             pass
 
 
-def set_grid_tuning(blocks_per_sm: int = 0, cells_per_block: int = 1024, wave_cells: int = 1 << 26,
+def set_grid_tuning(blocks_per_sm: int = 0, cells_per_block: int = 1024, wave_cells: int = 1 << 27,
                     solo_max: int = 64):
     """Process-wide grid propagation knobs (speed only): cooperative blocks per
     SM, cells per cooperative block, the most cells a batch job holds, and the

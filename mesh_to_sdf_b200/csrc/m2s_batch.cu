@@ -9,12 +9,14 @@
 // whatever else is in the job, so each grid's output is bit-identical to
 // computing it alone; a job takes as many rounds as its slowest grid.
 //
-// A batch runs as waves: jobs of at most wave_cells cells (64M by default; a
+// A batch runs as waves: jobs of at most wave_cells cells (128M by default; a
 // larger grid alone), packed largest grid first.  Grids that share a job
 // share its rounds and barriers, so the more a job holds the fewer rounds the
-// batch pays for; past a few tens of millions of cells the gain levels off
-// (256 grids, 547M cells: 4M-cell waves 568 ms, 16M 432 ms, 64M 383 ms, 128M
-// 382 ms) while a plan's autotuning, which times one wave per class, grows.
+// batch pays for, until a job's keys and lists outgrow the L2 cache so far
+// that each round's accesses slow down (256 grids, 547M cells: 64M-cell waves
+// 306 ms, 128M 297 ms, 256M 321 ms, one job 438 ms), while a plan's
+// autotuning, which times one wave per class, grows (6.5 s at 64M, 11.6 s at
+// 128M).
 //
 // A plan captures every wave's whole pipeline (memsets, seeding, collection,
 // the cooperative propagation kernel, rays, finalisation) into one CUDA graph
@@ -348,7 +350,7 @@ void m2s_set_grid_tuning(int blocks_per_sm, uint32_t cells_per_block, uint64_t w
   GridTuning t = grid_tuning();
   t.blocks_per_sm = blocks_per_sm > 0 ? blocks_per_sm : 0;
   t.cells_per_block = cells_per_block ? cells_per_block : 1024;
-  t.wave_cells = wave_cells ? wave_cells : (1ull << 26);
+  t.wave_cells = wave_cells ? wave_cells : (1ull << 27);
   t.solo_max = solo_max < 0 ? 64u : (uint32_t)solo_max;
   set_grid_tuning(t);
 }

@@ -190,7 +190,7 @@ struct GridTuning {
   uint32_t list_capacity = 0;        // entries per bucket list (0: derived from the cell count)
   // A batch runs as jobs ("waves") of at most this many cells each (a larger
   // grid alone), which bounds a job's keys (8 bytes per cell) and lists.
-  uint64_t wave_cells = 1ull << 26;
+  uint64_t wave_cells = 1ull << 27;
   // Relax rounds of at most this many states run on one block, with block
   // barriers only (0: every round on every block).
   uint32_t solo_max = 64;
