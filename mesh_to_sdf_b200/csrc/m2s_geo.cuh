@@ -134,12 +134,10 @@ __device__ __forceinline__ float point_triangle_distance2(P3 p, P3 a, P3 b, P3 c
 // region's value comes from the same operations as above, so the result is
 // bit-identical; lanes of a warp in different regions no longer run every
 // region's path and division one after another.
-__device__ __forceinline__ P3 closest_point_proper_sel(P3 p, P3 a, P3 b, P3 c) {
-  const P3 ab = dvsub(b, a), ac = dvsub(c, a);
-  const P3 ap = dvsub(p, a), bp = dvsub(p, b), cp = dvsub(p, c);
-  const float d1 = dvdot(ab, ap), d2 = dvdot(ac, ap);
-  const float d3 = dvdot(ab, bp), d4 = dvdot(ac, bp);
-  const float d5 = dvdot(ab, cp), d6 = dvdot(ac, cp);
+// The region choice and result of closest_point_proper_sel from the six dot
+// products d1..d6 (ab.ap, ac.ap, ab.bp, ac.bp, ab.cp, ac.cp).
+__device__ __forceinline__ P3 closest_from_dots(P3 a, P3 b, P3 c, P3 ab, P3 ac, float d1, float d2, float d3,
+                                                float d4, float d5, float d6) {
   const float vc = ds(dm(d1, d4), dm(d3, d2));
   const float vb = ds(dm(d5, d2), dm(d1, d6));
   const float va = ds(dm(d3, d6), dm(d5, d4));
@@ -163,6 +161,38 @@ __device__ __forceinline__ P3 closest_point_proper_sel(P3 p, P3 a, P3 b, P3 c) {
   if (face) x = x2;
   if (rA || rB || rC) x = rA ? a : (rB ? b : c);
   return x;
+}
+
+__device__ __forceinline__ P3 closest_point_proper_sel(P3 p, P3 a, P3 b, P3 c) {
+  const P3 ab = dvsub(b, a), ac = dvsub(c, a);
+  const P3 ap = dvsub(p, a), bp = dvsub(p, b), cp = dvsub(p, c);
+  return closest_from_dots(a, b, c, ab, ac, dvdot(ab, ap), dvdot(ac, ap), dvdot(ab, bp), dvdot(ac, bp),
+                           dvdot(ab, cp), dvdot(ac, cp));
+}
+
+// Points that share x and y (the cells of one grid row along z) share the x
+// and y parts of the six dot products, (e.x q.x + e.y q.y) in the reference's
+// order (x*x' + y*y') + z*z': RowXY holds them, formed once per row, and
+// row_distance2 adds each point's z terms.  Same operations, same rounding:
+// bit-identical to point_triangle_distance2_sel of a proper triangle.
+struct RowXY {
+  float d1, d2, d3, d4, d5, d6;
+};
+__device__ __forceinline__ RowXY row_xy(float px, float py, P3 a, P3 b, P3 c) {
+  const P3 ab = dvsub(b, a), ac = dvsub(c, a);
+  const float apx = ds(px, a.x), apy = ds(py, a.y), bpx = ds(px, b.x), bpy = ds(py, b.y);
+  const float cpx = ds(px, c.x), cpy = ds(py, c.y);
+  return {da(dm(ab.x, apx), dm(ab.y, apy)), da(dm(ac.x, apx), dm(ac.y, apy)), da(dm(ab.x, bpx), dm(ab.y, bpy)),
+          da(dm(ac.x, bpx), dm(ac.y, bpy)), da(dm(ab.x, cpx), dm(ab.y, cpy)), da(dm(ac.x, cpx), dm(ac.y, cpy))};
+}
+__device__ __forceinline__ float row_distance2(const RowXY& r, P3 p, P3 a, P3 b, P3 c) {
+  const P3 ab = dvsub(b, a), ac = dvsub(c, a);
+  const float apz = ds(p.z, a.z), bpz = ds(p.z, b.z), cpz = ds(p.z, c.z);
+  const P3 x = closest_from_dots(a, b, c, ab, ac, da(r.d1, dm(ab.z, apz)), da(r.d2, dm(ac.z, apz)),
+                                 da(r.d3, dm(ab.z, bpz)), da(r.d4, dm(ac.z, bpz)), da(r.d5, dm(ab.z, cpz)),
+                                 da(r.d6, dm(ac.z, cpz)));
+  const P3 d = dvsub(p, x);
+  return dvdot(d, d);
 }
 
 // point_triangle_distance2 with the branch-free proper case.

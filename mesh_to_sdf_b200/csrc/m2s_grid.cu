@@ -740,12 +740,17 @@ __device__ __forceinline__ bool neighbour_cell(const GridSet& gs, uint2 ent, uin
 // cell's key as read (`seen`); true when this proposal made the cell's first
 // lowering of the round (it is then the cell's one staging proposal).
 template <int SIGN>
-__device__ __forceinline__ bool propose_at(const TriRec& r, uint32_t tri, uint32_t j, P3 pos, unsigned long long seen,
-                                           unsigned long long* keys, bool& nan) {
-  const float d = cell_distance<SIGN>(pos, p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
+__device__ __forceinline__ bool propose_dist(float d, uint32_t tri, uint32_t j, unsigned long long seen,
+                                             unsigned long long* keys, bool& nan) {
   if (isnan(d)) nan = true;
   const unsigned long long cand = pack(d, tri) | kDirty;
   return beats<SIGN>(cand, seen, &nan) && improve_first<SIGN>(&keys[j], cand, seen, &nan);
+}
+template <int SIGN>
+__device__ __forceinline__ bool propose_at(const TriRec& r, uint32_t tri, uint32_t j, P3 pos, unsigned long long seen,
+                                           unsigned long long* keys, bool& nan) {
+  return propose_dist<SIGN>(cell_distance<SIGN>(pos, p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w)), tri, j, seen,
+                            keys, nan);
 }
 
 // A solo round (block 0 alone, n <= kSoloCap states) forms the round's minima
@@ -1027,19 +1032,30 @@ __device__ __forceinline__ void relax_propose(const GridSet& gs, const TriRec* _
         const unsigned long long k0 = lo ? __ldcg(&keys[j0]) : 0ull;
         const unsigned long long k1 = mid ? __ldcg(&keys[j0 + 1]) : 0ull;
         const unsigned long long k2 = hi ? __ldcg(&keys[j0 + 2]) : 0ull;
+        // the row's cells share x and y, and so the x and y parts of the
+        // closest-point dot products of a proper triangle
+        const P3 a = p3(r.a), b = p3(r.b), c = p3(r.c);
+        const int kind = __float_as_int(r.a.w);
+        const bool proper = kind == TRI_PROPER;
+        const P3 pm = center(g, X, Y, z);
+        const RowXY rxy = row_xy(pm.x, pm.y, a, b, c);
+        auto dist = [&](int dz) {
+          const P3 pos{pm.x, pm.y, fa(g.f[2], fm(__int2float_rn(z + dz), g.s[2]))};  // center(g, X, Y, z + dz)
+          return fsqrt(proper ? row_distance2(rxy, pos, a, b, c) : point_triangle_distance2_sel(pos, a, b, c, kind));
+        };
         if (lo) {
           ++evals;
-          if (propose_at<SIGN>(r, tri, j0, center(g, X, Y, z - 1), k0, keys, nan))
+          if (propose_dist<SIGN>(dist(-1), tri, j0, k0, keys, nan))
             stage_touch(j0, s_touch, s_ntouch, st, parity, spill, cap);
         }
         if (mid) {
           ++evals;
-          if (propose_at<SIGN>(r, tri, j0 + 1, center(g, X, Y, z), k1, keys, nan))
+          if (propose_dist<SIGN>(dist(0), tri, j0 + 1, k1, keys, nan))
             stage_touch(j0 + 1, s_touch, s_ntouch, st, parity, spill, cap);
         }
         if (hi) {
           ++evals;
-          if (propose_at<SIGN>(r, tri, j0 + 2, center(g, X, Y, z + 1), k2, keys, nan))
+          if (propose_dist<SIGN>(dist(1), tri, j0 + 2, k2, keys, nan))
             stage_touch(j0 + 2, s_touch, s_ntouch, st, parity, spill, cap);
         }
       }
