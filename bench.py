@@ -36,7 +36,7 @@ SEED = 0
 
 # DRAM bytes (read + write) of one propagation launch of the bench grid, from
 # an ncu capture of dram__bytes_read.sum and dram__bytes_write.sum (one launch).
-PROPAGATE_DRAM_BYTES = 145_430_016 + 241_688_064
+PROPAGATE_DRAM_BYTES = 145_844_224 + 243_579_392
 PROPAGATE_DRAM_SOURCE = "profiles/k_propagate_star_s6_grid256.md (ncu, one 256^3 launch)"
 
 
