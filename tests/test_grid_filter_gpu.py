@@ -6,7 +6,9 @@ proves that it cannot beat the cell's value.  These tests run every grid with
 the filter on and off and require identical bits, on shapes chosen to stress
 the bound: smooth closed meshes, an open terrain strip with zero-area
 connector windows, slivers and needles, a coarse mesh whose states reach far
-from the surface, a grid far from the origin, and the batched kernel.
+from the surface, grids one or two cells thick (the plain kernel's row units
+of three z-neighbours all meet a boundary there), a grid far from the
+origin, and the batched kernel.
 """
 import numpy as np
 import pytest
@@ -70,6 +72,11 @@ CASES = {
     "terrain_strip_raycast": (lambda: synth.terrain(96, seed=3), True, [64, 64, 40], S.Raycast),
     "slivers_raycast": (lambda: slivers(3000, 7), False, [60, 60, 60], S.Raycast),
     "slivers_normal": (lambda: slivers(3000, 7), False, [60, 60, 60], S.Normal),
+    # one and two cells along z: every row unit of the plain kernel's big
+    # rounds meets the grid's z boundary
+    "star_s4_flat_z1": (lambda: synth.star(4, seed=4), False, [420, 400, 1], S.Raycast),
+    "star_s4_flat_z2": (lambda: synth.star(4, seed=4), False, [300, 320, 2], S.Raycast),
+    "star_s4_thin_x": (lambda: synth.star(4, seed=4), False, [2, 300, 320], S.Raycast),
 }
 
 
@@ -85,7 +92,8 @@ def test_filter_changes_no_bit(case):
     assert len(bad) == 0, f"{case}: {len(bad)} cells differ, e.g. {bad[:5]} on {on[bad[:5]]} off {off[bad[:5]]}"
     # the same proposals are made either way; the filter only drops some unevaluated
     assert s_on["neighbour_evals"] == s_off["neighbour_evals"] and s_off["dropped_bound"] == 0
-    assert s_on["dropped_bound"] > 0, s_on
+    if min(count) > 2:
+        assert s_on["dropped_bound"] > 0, s_on
 
 
 def test_filter_far_from_origin():
