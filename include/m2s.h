@@ -218,7 +218,8 @@ int m2s_generate_sdf_none_noalloc(const float* d_vertices, uint64_t n_vertices,
  * `point_streams` streams (0 = 4); a free grid lane takes the grid requests
  * waiting at that moment (up to 4M cells) as one wave, so a request is
  * admitted at the next wave boundary, and the two lanes' waves run side by
- * side.  Every result equals the one the single-request
+ * side (each on half the propagation blocks per SM; a wave that starts while
+ * the other lane is idle and nothing else waits takes all but one).  Every result equals the one the single-request
  * calls give (m2s_query_sdf with the mesh's method; m2s_grid_sdf_device).
  * Submissions return a ticket at once; the caller's host buffers (queries,
  * outputs) must stay valid until m2s_server_wait returns for that ticket.
