@@ -95,6 +95,8 @@ def test_reference_distance_never_below_plane_bound(scale, offset, least):
     dists = [scale * f for f in (1e-6, 1e-3, 0.1, 1.0, 10.0, 1e3, 1e5)]
     checked = positive = 0
     for a, b, c in triangles(rng, 40, scale, offset):
+        if not np.any(np.cross(b.astype(np.float64) - a, c.astype(np.float64) - a)):
+            continue  # rounded to a degenerate triangle: never admitted
         pts = points_around(rng, a, b, c, dists)
         pts = pts[np.all(np.abs(pts) < 2.0 ** 29, axis=1)].astype(F)
         ref = reference_distances(a, b, c, pts)
