@@ -284,6 +284,55 @@ __device__ __forceinline__ int compare_distances(float a, float b, bool* nan) {
 // before no value of such a fold.  `!(|d| > reach)` keeps NaN distances.
 __device__ __forceinline__ float fold_reach(float B) { return fmaf(B, 1.0f + 0x1p-19f, 4.0e-6f); }
 
+// Plane bound.  Whatever Voronoi region the reference's f32 closest point x
+// takes (closest_point_proper), x lies within rounding of the triangle's
+// plane: a vertex; a point a + s e of an edge with s in [0, 1] (the region
+// tests make the computed s so); or, in the face region, a + ab v + ac w,
+// whose rounding is at most ~2^-22 (|a| + |ab||v| + |ac||w|).  If the weights
+// are so inaccurate that |ab||v| + |ac||w| is large, then so is |x - a| (at
+// least that sum over sqrt(2 / (1 - |cos A|)), A the angle at a: 32 when
+// sin A >= 1/16), and x is far from p anyway.  Either way the reference's
+// distance from p is at least
+//     |h| (1 - 2^-13) - 2^-11 (|p|max + |triangle|max),
+// h the distance from p to the plane, for a proper triangle with
+// sin^2 A >= 1/200 and coordinates below 2^30 (a margin of some 64x over the
+// error terms).  So a triangle whose bound exceeds a search's best distance
+// cannot be strictly nearer.  TriPlane holds the unit normal (n.w = n . a)
+// and the triangle's share of the slack, +inf where the bound does not apply
+// (the normal is then zero).  Float arithmetic suffices: for the triangles
+// kept the normal's rounding is a few ulps, far inside the slack, and the
+// shape test asks sin^2 A >= 1/200 so that its own rounding cannot admit
+// sin A < 1/16.
+struct TriPlane {
+  float4 n;
+  float slack;
+};
+__device__ __forceinline__ TriPlane tri_plane(P3 a, P3 b, P3 c, int kind) {
+  const float abx = b.x - a.x, aby = b.y - a.y, abz = b.z - a.z;
+  const float acx = c.x - a.x, acy = c.y - a.y, acz = c.z - a.z;
+  const float nx = aby * acz - abz * acy, ny = abz * acx - abx * acz, nz = abx * acy - aby * acx;
+  const float nn2 = nx * nx + ny * ny + nz * nz;
+  const float lab2 = abx * abx + aby * aby + abz * abz, lac2 = acx * acx + acy * acy + acz * acz;
+  const float vmax = fmaxf(fmaxf(fmaxf(fabsf(a.x), fabsf(a.y)), fmaxf(fabsf(a.z), fabsf(b.x))),
+                           fmaxf(fmaxf(fabsf(b.y), fabsf(b.z)), fmaxf(fmaxf(fabsf(c.x), fabsf(c.y)), fabsf(c.z))));
+  const bool ok = kind == TRI_PROPER && vmax < 0x1p30f && nn2 > 0.0f && 200.0f * nn2 >= lab2 * lac2;
+  if (!ok) return {make_float4(0.f, 0.f, 0.f, 0.f), INFINITY};
+  const float inv = rsqrtf(nn2);
+  const float ux = nx * inv, uy = ny * inv, uz = nz * inv;
+  return {make_float4(ux, uy, uz, ux * a.x + uy * a.y + uz * a.z), 0x1p-11f * vmax};
+}
+// The query's share of the slack.
+__device__ __forceinline__ float plane_query_slack(P3 p) {
+  return 0x1p-11f * fmaxf(fabsf(p.x), fmaxf(fabsf(p.y), fabsf(p.z)));
+}
+// The lower bound of the reference's distance from p (-inf where it does not apply).
+__device__ __forceinline__ float plane_bound(float4 n, float slack, P3 p, float pslack) {
+  const float h = fabsf(fmaf(n.x, p.x, fmaf(n.y, p.y, fmaf(n.z, p.z, -n.w))));
+  return fmaf(h, 1.0f - 0x1p-13f, -(slack + pslack));
+}
+// A bound above this proves the triangle's squared distance exceeds d2.
+__device__ __forceinline__ float plane_above(float d2) { return sqrtf(d2) * (1.0f + 0x1p-18f); }
+
 // geo.rs:4-22: AABB grown by 1e-4 on every side (f32 min/max then -/+ 1e-4).
 __device__ __forceinline__ void padded_box(P3 a, P3 b, P3 c, P3* lo, P3* hi) {
   const float e = 0.0001f;

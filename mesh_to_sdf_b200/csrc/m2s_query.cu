@@ -41,52 +41,20 @@ constexpr int kBfTile = 256;  // triangles per stage: 256 * 48 B = 12 KiB
 // squared distance bits, atomicXor on the parity).  Normal folds all
 // triangles in order in one chunk (compare_distances ties depend on order).
 //
-// Raycast plane bound.  Whatever Voronoi region the reference's f32 closest
-// point x takes, x lies within rounding of the triangle's plane: a vertex; a
-// point a + s e of an edge with s in [0, 1] (the region tests make the
-// computed s so); or, in the face region, a + ab v + ac w, whose rounding is
-// at most ~2^-22 (|a| + |ab||v| + |ac||w|).  If the weights are so inaccurate
-// that |ab||v| + |ac||w| is large, then so is |x - a| (by at least that sum
-// over sqrt(2 / (1 - |cos A|)), A the angle at a: 32 when sin A >= 1/16), and
-// x is far from p anyway.  Either way the reference's distance from p is at
-// least |h| (1 - 2^-13) - 2^-11 (|p|max + |triangle|max), h the distance from
-// p to the plane, for a proper triangle with sin A >= 1/16 and coordinates
-// below 2^30 (a margin of some 64x over the error terms).  A triangle whose
-// bound exceeds the query's best distance so far cannot lower the minimum, so
-// its closest point is not evaluated; its +X ray test always is (the
-// parity counts every triangle).  Rust's f32::min ignores a NaN distance
-// (default.rs:58), so a skipped triangle changes nothing even then.  The
-// planes are formed per tile: unit normal and offset, and the triangle's
-// slack (+inf where the bound does not apply).
-struct BfPlane {
-  float4 n;     // unit normal, n.w = n . a
-  float slack;  // 2^-11 of the triangle's largest coordinate magnitude, or +inf
-};
-__device__ __forceinline__ BfPlane bf_plane(const TriRec& r) {
-  // float arithmetic suffices: for the triangles kept (sin A >= 1/16) the
-  // normal's rounding is a few ulps, far inside the slack, and the shape test
-  // asks sin^2 A >= 1/200 so that its own rounding cannot admit sin A < 1/16
-  const float abx = r.b.x - r.a.x, aby = r.b.y - r.a.y, abz = r.b.z - r.a.z;
-  const float acx = r.c.x - r.a.x, acy = r.c.y - r.a.y, acz = r.c.z - r.a.z;
-  const float nx = aby * acz - abz * acy, ny = abz * acx - abx * acz, nz = abx * acy - aby * acx;
-  const float nn2 = nx * nx + ny * ny + nz * nz;
-  const float lab2 = abx * abx + aby * aby + abz * abz, lac2 = acx * acx + acy * acy + acz * acz;
-  const float vmax = fmaxf(fmaxf(fmaxf(fabsf(r.a.x), fabsf(r.a.y)), fmaxf(fabsf(r.a.z), fabsf(r.b.x))),
-                           fmaxf(fmaxf(fabsf(r.b.y), fabsf(r.b.z)), fmaxf(fmaxf(fabsf(r.c.x), fabsf(r.c.y)), fabsf(r.c.z))));
-  const bool ok = __float_as_int(r.a.w) == TRI_PROPER && vmax < 0x1p30f && nn2 > 0.0f && 200.0f * nn2 >= lab2 * lac2;
-  if (!ok) return {make_float4(0.f, 0.f, 0.f, 0.f), INFINITY};
-  const float inv = rsqrtf(nn2);
-  const float ux = nx * inv, uy = ny * inv, uz = nz * inv;
-  return {make_float4(ux, uy, uz, ux * r.a.x + uy * r.a.y + uz * r.a.z), 0x1p-11f * vmax};
-}
+// Raycast: a triangle whose plane bound (tri_plane in m2s_geo.cuh) exceeds
+// the query's best distance so far cannot lower the minimum, so its closest
+// point is not evaluated; its +X ray test always is (the parity counts every
+// triangle).  Rust's f32::min ignores a NaN distance (default.rs:58), so a
+// skipped triangle changes nothing even then.  The planes of a tile are
+// formed in shared memory as it lands.
 template <int SIGN>
 __global__ void __launch_bounds__(kBfThreads) k_brute(const TriRec* __restrict__ tris, uint32_t T,
                                                       const float* __restrict__ q, uint64_t nq,
                                                       float* __restrict__ out, uint32_t* status,
                                                       uint2* __restrict__ part, const uint32_t* __restrict__ order) {
   __shared__ __align__(128) TriRec tile[2][kBfTile];
-  __shared__ __align__(16) float4 plane_n[2][SIGN == 0 ? kBfTile : 1];  // BfPlane::n
-  __shared__ float plane_s[2][SIGN == 0 ? kBfTile : 1];                  // BfPlane::slack
+  __shared__ __align__(16) float4 plane_n[2][SIGN == 0 ? kBfTile : 1];  // TriPlane::n
+  __shared__ float plane_s[2][SIGN == 0 ? kBfTile : 1];                  // TriPlane::slack
   __shared__ __align__(8) uint64_t bar[2];
   const int tid = threadIdx.x;
   const uint64_t k = (uint64_t)blockIdx.x * kBfThreads + tid;
@@ -123,7 +91,7 @@ __global__ void __launch_bounds__(kBfThreads) k_brute(const TriRec* __restrict__
   // Raycast: a triangle's plane bound must exceed `above` to skip it;
   // `pslack` is the query's share of the bound's slack.
   float above = INFINITY;
-  const float pslack = 0x1p-11f * fmaxf(fabsf(p.x), fmaxf(fabsf(p.y), fabsf(p.z)));
+  const float pslack = plane_query_slack(p);
   uint32_t hits = 0;
   bool nan = false, lost = false;
   for (uint32_t i = 0; i < ntile; ++i) {
@@ -135,7 +103,7 @@ __global__ void __launch_bounds__(kBfThreads) k_brute(const TriRec* __restrict__
       lost = __syncthreads_or(lost);  // the planes are only formed from a tile every thread has
       if (!lost)
         for (uint32_t j = tid; j < cnt; j += kBfThreads) {
-          const BfPlane pl = bf_plane(tl[j]);
+          const TriPlane pl = tri_plane(p3(tl[j].a), p3(tl[j].b), p3(tl[j].c), __float_as_int(tl[j].a.w));
           plane_n[buf][j] = pl.n;
           plane_s[buf][j] = pl.slack;
         }
@@ -149,13 +117,11 @@ __global__ void __launch_bounds__(kBfThreads) k_brute(const TriRec* __restrict__
         const int kind = __float_as_int(ra.w);
         if (SIGN == 0) {
           // default.rs:45-49 then :59-62 — min of distances, count of +X hits.
-          const float4 pn = plane_n[buf][SIGN == 0 ? j : 0];
-          const float h = fabsf(fmaf(pn.x, p.x, fmaf(pn.y, p.y, fmaf(pn.z, p.z, -pn.w))));
-          if (!(fmaf(h, 1.0f - 0x1p-13f, -(plane_s[buf][SIGN == 0 ? j : 0] + pslack)) > above)) {
+          if (!(plane_bound(plane_n[buf][SIGN == 0 ? j : 0], plane_s[buf][SIGN == 0 ? j : 0], p, pslack) > above)) {
             const float d2 = point_triangle_distance2(p, a, b, c, kind);
             if (d2 < best) {  // fminf: a NaN distance is ignored
               best = d2;
-              above = sqrtf(best) * (1.0f + 0x1p-18f);
+              above = plane_above(best);
             }
           }
           float t;

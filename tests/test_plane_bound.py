@@ -5,7 +5,8 @@ closest-point evaluation when its plane bound
 
     |h| (1 - 2^-13) - 2^-11 (|p|max + |triangle|max),   h = p's distance to the plane,
 
-already exceeds the query's best distance, for proper triangles whose angle at
+already exceeds the query's best distance (so the triangle cannot be strictly
+nearer), for proper triangles whose angle at
 `a` has sin^2 >= 1/200 and whose coordinates stay below 2^30.  That is exact
 only if the reference's own f32 distance is never below the bound, whatever
 Voronoi region its rounding picks.  These tests check that claim against the
