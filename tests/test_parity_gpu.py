@@ -259,6 +259,49 @@ def test_brute_force_morton_order(orc):
         assert_bit_equal(m2s.generate_sdf(v, T.TriangleList(idx), q, am), orc_sdf(orc, v, idx, q, am), repr(am))
 
 
+def _plane_bound_soup(seed):
+    """Triangles that stress the Raycast brute force's plane bound: tiny
+    well-shaped ones (edges 1e-4 .. 1e-6) scattered far from the queries,
+    slivers on either side of the bound's shape threshold (sin^2 of the angle
+    at a near 1/200), and ordinary ones, around offsets 0, 1e3 and 1e5."""
+    rng = np.random.default_rng(seed)
+    tris = []
+    for off in (0.0, 1e3, 1e5):
+        for scale, sin_a, n in ((1e-4, 0.5, 300), (1e-6, 0.5, 300), (0.05, 0.069, 300), (0.05, 0.072, 300),
+                                (0.05, 0.6, 600)):
+            a = rng.normal(size=(n, 3)) * (0.5 + off * 1e-3) + off
+            e1 = rng.normal(size=(n, 3))
+            e1 /= np.linalg.norm(e1, axis=1, keepdims=True)
+            e2 = rng.normal(size=(n, 3))
+            e2 -= e1 * np.sum(e1 * e2, axis=1, keepdims=True)
+            e2 /= np.linalg.norm(e2, axis=1, keepdims=True)
+            ang = np.arcsin(sin_a)
+            b = a + scale * e1
+            c = a + scale * (np.cos(ang) * e1 + np.sin(ang) * e2)
+            tris.append(np.stack([a, b, c], 1))
+    v = np.concatenate(tris).reshape(-1, 3).astype(np.float32)
+    return v, np.arange(len(v), dtype=np.uint32)
+
+
+@pytest.mark.parametrize("seed", [21, 22])
+def test_none_raycast_plane_bound_adversarial(orc, seed):
+    # the brute force skips a triangle's closest point when its plane is
+    # already farther than the best distance; on a soup built to break that
+    # bound the results must still equal the reference's bit for bit, in the
+    # Morton-ordered chunked kernel and in the single-chunk one
+    v, idx = _plane_bound_soup(seed)
+    rng = np.random.default_rng(seed + 100)
+    q = np.concatenate([rng.normal(size=(20000, 3)) * 0.7,
+                        rng.normal(size=(10000, 3)) * 0.7 + 1e3,
+                        rng.normal(size=(10000, 3)) * 50.0 + 1e5,
+                        v[rng.integers(0, len(v), 10000)] + rng.normal(size=(10000, 3)) * 1e-5]).astype(np.float32)
+    assert len(q) * (len(idx) // 3) >= 1 << 28  # Morton order, triangle chunks
+    am = A.none(S.Raycast)
+    ref = orc_sdf(orc, v, idx, q, am)
+    assert_bit_equal(m2s.generate_sdf(v, T.TriangleList(idx), q, am), ref, "chunked")
+    assert_bit_equal(m2s.generate_sdf(v, T.TriangleList(idx), q[:1500], am), ref[:1500], "one chunk")
+
+
 def test_query_counting_changes_no_result():
     # profiling runs the counting kernel instantiations: same bits, sane counts
     v, idx = synth.star(4, seed=5)
