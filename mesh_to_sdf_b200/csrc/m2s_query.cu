@@ -796,8 +796,11 @@ __device__ __forceinline__ void audit_region(const MeshView& m, P3 p, uint32_t t
 // from f32::MAX with the rule of bvh.rs:125-127.
 constexpr int kBand = 32;
 
+// With a budget, the traversal gives up after `budget` node visits and clears
+// *finished (the caller then hands the query to the warp pass).
 template <bool STATS = false>
-__device__ float normal_band_fold(const MeshView& m, P3 p, float d2min, bool* nan, bool* overflow, QCount* qc = nullptr) {
+__device__ float normal_band_fold(const MeshView& m, P3 p, float d2min, bool* nan, bool* overflow, QCount* qc = nullptr,
+                                  uint32_t budget = 0xFFFFFFFFu, bool* finished = nullptr) {
   const double band = sqrt((double)d2min) * (1.0 + 1e-5) + 4e-6;
   const float reach = (float)((band + 2e-4) * (1.0 + 1e-6));
   const float reach2 = reach * reach;
@@ -823,7 +826,12 @@ __device__ float normal_band_fold(const MeshView& m, P3 p, float d2min, bool* na
     uint32_t stack[kStack];
     int sp = 0;
     uint32_t node = 0;
+    uint32_t visits = 0;
     while (true) {
+      if (++visits > budget) {
+        *finished = false;
+        return 0.0f;
+      }
       if constexpr (STATS) ++qc->sign_visits;
       BvhNode nd = load_node(m.nodes, node);
       uint32_t L = __float_as_uint(nd.l_lo.w), R = __float_as_uint(nd.l_hi.w);
@@ -882,6 +890,100 @@ __device__ float normal_band_fold(const MeshView& m, P3 p, float d2min, bool* na
   return best;
 }
 
+// normal_band_fold for one query on a whole warp: the same band and reach,
+// so the same candidates (every leaf within reach whose |d| lies in the band),
+// found by a traversal that takes up to 32 nodes a step from a shared stack;
+// lane 0 then sorts them by triangle index and folds them exactly as above.
+// The result is normal_band_fold's bit for bit.  Returns false (and leaves
+// *result alone) when the stack (CAP entries) or the candidate list
+// (kBandWarp) would overflow: the caller runs normal_band_fold instead.
+constexpr int kBandWarp = 64;
+template <bool STATS = false, int CAP = kWarpStack>
+__device__ bool normal_band_fold_warp(const MeshView& m, P3 p, float d2min, uint32_t* s_node, uint32_t* s_cidx,
+                                      float* s_cd, uint32_t* s_count, float* result, bool* nan, QCount* qc) {
+  const int lane = threadIdx.x & 31;
+  const double band = sqrt((double)d2min) * (1.0 + 1e-5) + 4e-6;
+  const float reach = (float)((band + 2e-4) * (1.0 + 1e-6));
+  const float reach2 = reach * reach;
+  if (lane == 0) *s_count = 0;
+  __syncwarp();
+  bool over = false;
+  auto consider = [&](uint32_t leaf) {
+    if constexpr (STATS) ++qc->sign_tests;
+    const TriRec r = load_tri(m.stris, leaf);
+    const float d = point_triangle_signed_distance(p, p3(r.a), p3(r.b), p3(r.c), __float_as_int(r.a.w));
+    if (!(fabs((double)d) <= band)) return;
+    const uint32_t pos = atomicAdd(s_count, 1u);
+    if (pos < (uint32_t)kBandWarp) {
+      s_cidx[pos] = __float_as_uint(r.b.w);
+      s_cd[pos] = d;
+    } else {
+      over = true;
+    }
+  };
+  if (m.root & LEAF_BIT) {
+    if (lane == 0) consider(m.root & ~LEAF_BIT);
+  } else {
+    if (lane == 0) s_node[0] = 0;
+    int sp = 1;
+    __syncwarp();
+    while (sp > 0) {
+      const int take = min(sp, 32), base = sp - take;
+      const uint32_t node = lane < take ? s_node[base + lane] : 0xFFFFFFFFu;
+      __syncwarp();
+      sp = base;
+      uint32_t push[2] = {0u, 0u};
+      int npush = 0;
+      if (node != 0xFFFFFFFFu) {
+        if constexpr (STATS) ++qc->sign_visits;
+        const BvhNode nd = load_node(m.nodes, node);
+        const uint32_t ch[2] = {__float_as_uint(nd.l_lo.w), __float_as_uint(nd.l_hi.w)};
+        const bool go[2] = {box_dist2(p, nd.l_lo, nd.l_hi) <= reach2, box_dist2(p, nd.r_lo, nd.r_hi) <= reach2};
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          if (!go[c]) continue;
+          if (ch[c] & LEAF_BIT) consider(ch[c] & ~LEAF_BIT);
+          else push[npush++] = ch[c];
+        }
+      }
+      int incl = npush;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      const int total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+      if (sp + total > CAP) return false;  // warp-uniform
+      int pos = sp + incl - npush;
+      for (int c = 0; c < npush; ++c) s_node[pos++] = push[c];
+      sp += total;
+      __syncwarp();
+    }
+  }
+  __syncwarp();
+  if (__any_sync(0xFFFFFFFFu, over)) return false;
+  if (lane == 0) {
+    const int n = (int)*s_count;
+    for (int i = 1; i < n; ++i) {  // insertion sort by triangle index
+      const uint32_t ki = s_cidx[i];
+      const float di = s_cd[i];
+      int j = i - 1;
+      while (j >= 0 && s_cidx[j] > ki) {
+        s_cidx[j + 1] = s_cidx[j];
+        s_cd[j + 1] = s_cd[j];
+        --j;
+      }
+      s_cidx[j + 1] = ki;
+      s_cd[j + 1] = di;
+    }
+    float best = F32_MAX;
+    for (int i = 0; i < n; ++i)
+      if (compare_distances(best, s_cd[i], nan) == 1) best = s_cd[i];
+    *result = best;
+  }
+  __syncwarp();
+  return true;
+}
+
 enum QueryMode { Q_BVH_RAYCAST = 0, Q_BVH_NORMAL = 1, Q_RTREE = 2, Q_VECTOR = 3 };
 
 // A query whose single-thread search ran over its node budget, with its
@@ -921,8 +1023,18 @@ __device__ __forceinline__ void finish_query(const MeshView& m, uint64_t i, P3 p
   }
 }
 
+// Bvh(Normal) with the band fold's result already formed.
+template <bool STATS = false>
+__device__ __forceinline__ void finish_normal(const MeshView& m, uint64_t i, P3 p, Nearest nn, float band_result,
+                                              float* out, QCount* qc) {
+  if (nn.tri == 0xFFFFFFFFu) nn = {INFINITY, 0u, 0u};  // every distance NaN
+  audit_region<STATS>(m, p, nn.tri, qc);
+  out[i] = band_result;
+}
+
 // Pass 1: one thread per query.  Searches that exceed `budget` node visits
-// are handed to pass 2 (k_query_hard) with their partial result.
+// are handed to pass 2 (k_query_hard) with their partial result; for
+// Bvh(Normal) so are the tie-band folds that exceed it.
 // Adds a thread's traversal counts to qstats[0..3] (one atomic per warp).
 __device__ __forceinline__ void add_counts(const QCount& c, unsigned long long* qstats) {
   const unsigned mask = __activemask();  // lanes past the last query have left
@@ -954,7 +1066,7 @@ __global__ void __launch_bounds__(128) k_query(MeshView m, const float* __restri
   bool inside = false;
   QCount qc;
   bool finished = true;
-  const uint32_t bud = (MODE == Q_BVH_NORMAL || !hard) ? 0xFFFFFFFFu : budget;
+  const uint32_t bud = !hard ? 0xFFFFFFFFu : budget;
   Nearest nn;
   if (packet) {
     nn = nearest_triangle_packet<STATS>(m, p, active, &overflow, bud, &finished, &qc);
@@ -963,8 +1075,12 @@ __global__ void __launch_bounds__(128) k_query(MeshView m, const float* __restri
     nn = nearest_triangle<STATS>(m, p, &overflow, Nearest{INFINITY, 0xFFFFFFFFu, 0}, bud, &finished, &qc);
   }
   if (MODE == Q_BVH_RAYCAST || MODE == Q_VECTOR) inside = vote_inside<STATS>(m, p, &overflow, &qc);
+  float band_result = 0.0f;
+  if (MODE == Q_BVH_NORMAL && hard && finished)
+    band_result = normal_band_fold<STATS>(m, p, nn.d2, &nan, &overflow, &qc, budget, &finished);
   if (finished) {
-    finish_query<MODE, STATS>(m, i, p, nn, inside, out, vec, inside_out, &nan, &overflow, &qc);
+    if (MODE == Q_BVH_NORMAL && hard) finish_normal<STATS>(m, i, p, nn, band_result, out, &qc);
+    else finish_query<MODE, STATS>(m, i, p, nn, inside, out, vec, inside_out, &nan, &overflow, &qc);
   } else {
     uint32_t pos = atomicAdd(hard_count, 1u);
     hard[pos] = HardQuery{(uint32_t)i, nn.d2, nn.tri, nn.leaf | (inside ? 0x80000000u : 0u)};
@@ -986,6 +1102,9 @@ __global__ void __launch_bounds__(32 * kHardWarps) k_query_hard(MeshView m, cons
   QCount qc;  // every lane's node fetches and tests of the warp searches
   __shared__ uint32_t s_node[kHardWarps][kWarpStack];
   __shared__ float s_dist[kHardWarps][kWarpStack];
+  __shared__ uint32_t s_cidx[MODE == Q_BVH_NORMAL ? kHardWarps : 1][kBandWarp];
+  __shared__ float s_cd[MODE == Q_BVH_NORMAL ? kHardWarps : 1][kBandWarp];
+  __shared__ uint32_t s_ccount[kHardWarps];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t n = *hard_count;
   bool overflow = false, nan = false;
@@ -995,7 +1114,19 @@ __global__ void __launch_bounds__(32 * kHardWarps) k_query_hard(MeshView m, cons
     Nearest nn{hq.d2, hq.tri, hq.leaf_inside & 0x7FFFFFFFu};
     const bool inside = (hq.leaf_inside >> 31) != 0;
     const bool ok = nearest_triangle_warp<STATS>(m, p, &nn, s_node[w], s_dist[w], &qc);
-    if (lane == 0) {
+    if (MODE == Q_BVH_NORMAL) {
+      if (lane == 0 && !ok) nn = nearest_triangle<STATS>(m, p, &overflow, nn, 0xFFFFFFFFu, nullptr, &qc);
+      nn.d2 = __shfl_sync(0xFFFFFFFFu, nn.d2, 0);
+      nn.tri = __shfl_sync(0xFFFFFFFFu, nn.tri, 0);
+      nn.leaf = __shfl_sync(0xFFFFFFFFu, nn.leaf, 0);
+      float r = 0.0f;
+      const bool wok = normal_band_fold_warp<STATS>(m, p, nn.d2, s_node[w], s_cidx[MODE == Q_BVH_NORMAL ? w : 0],
+                                                    s_cd[MODE == Q_BVH_NORMAL ? w : 0], &s_ccount[w], &r, &nan, &qc);
+      if (lane == 0) {
+        if (!wok) r = normal_band_fold<STATS>(m, p, nn.d2, &nan, &overflow, &qc);  // list or stack full: one lane
+        finish_normal<STATS>(m, hq.i, p, nn, r, out, &qc);
+      }
+    } else if (lane == 0) {
       if (!ok) nn = nearest_triangle<STATS>(m, p, &overflow, nn, 0xFFFFFFFFu, nullptr, &qc);  // stack full: finish on one lane
       finish_query<MODE, STATS>(m, hq.i, p, nn, inside, out, vec, inside_out, &nan, &overflow, &qc);
     }
@@ -1027,6 +1158,9 @@ __global__ void __launch_bounds__(32 * kSmallWarps) k_query_warpwise(MeshView m,
   QCount qc;
   __shared__ uint32_t s_node[kSmallWarps][kSmallStack];
   __shared__ float s_dist[kSmallWarps][kSmallStack];
+  __shared__ uint32_t s_cidx[MODE == Q_BVH_NORMAL ? kSmallWarps : 1][kBandWarp];
+  __shared__ float s_cd[MODE == Q_BVH_NORMAL ? kSmallWarps : 1][kBandWarp];
+  __shared__ uint32_t s_ccount[kSmallWarps];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   bool overflow = false, nan = false;
   for (uint64_t i = (uint64_t)blockIdx.x * kSmallWarps + w; i < nq; i += (uint64_t)gridDim.x * kSmallWarps) {
@@ -1035,6 +1169,23 @@ __global__ void __launch_bounds__(32 * kSmallWarps) k_query_warpwise(MeshView m,
     const bool ok = nearest_triangle_warp<STATS, kSmallStack>(m, p, &nn, s_node[w], s_dist[w], &qc);
     bool inside = false;
     if (MODE == Q_BVH_RAYCAST || MODE == Q_VECTOR) inside = vote_inside_warp<kSmallStack, STATS>(m, p, s_node[w], &overflow, &qc);
+    if (MODE == Q_BVH_NORMAL) {
+      if (lane == 0 && !ok) nn = nearest_triangle<STATS>(m, p, &overflow, nn, 0xFFFFFFFFu, nullptr, &qc);
+      nn.d2 = __shfl_sync(0xFFFFFFFFu, nn.d2, 0);
+      nn.tri = __shfl_sync(0xFFFFFFFFu, nn.tri, 0);
+      nn.leaf = __shfl_sync(0xFFFFFFFFu, nn.leaf, 0);
+      float r = 0.0f;
+      const bool wok = normal_band_fold_warp<STATS, kSmallStack>(m, p, nn.d2, s_node[w],
+                                                                 s_cidx[MODE == Q_BVH_NORMAL ? w : 0],
+                                                                 s_cd[MODE == Q_BVH_NORMAL ? w : 0], &s_ccount[w], &r,
+                                                                 &nan, &qc);
+      if (lane == 0) {
+        if (!wok) r = normal_band_fold<STATS>(m, p, nn.d2, &nan, &overflow, &qc);
+        finish_normal<STATS>(m, i, p, nn, r, out, &qc);
+      }
+      __syncwarp();
+      continue;
+    }
     if (lane == 0) {
       if (!ok) nn = nearest_triangle<STATS>(m, p, &overflow, nn, 0xFFFFFFFFu, nullptr, &qc);  // stack full: finish alone
       finish_query<MODE, STATS>(m, i, p, nn, inside, out, vec, inside_out, &nan, &overflow, &qc);
@@ -1209,8 +1360,11 @@ void launch_queries(int mode, const MeshView& m, const float* d_q, const uint32_
                                                                                   nullptr, d_status, qs);
       break;
     case Q_BVH_NORMAL:
-      k_query<Q_BVH_NORMAL, ST><<<blocks, 128, 0, s>>>(m, d_q, ord, nq, d_out, nullptr, nullptr, d_status, budget,
-                                                       nullptr, nullptr, packet, qs);
+      k_query<Q_BVH_NORMAL, ST><<<blocks, 128, 0, s>>>(m, d_q, ord, nq, d_out, nullptr, nullptr, d_status, budget, hp,
+                                                       hc, packet, qs);
+      if (two_pass)
+        k_query_hard<Q_BVH_NORMAL, ST><<<hard_blocks, 32 * kHardWarps, 0, s>>>(m, d_q, hp, hc, d_out, nullptr,
+                                                                                 nullptr, d_status, qs);
       break;
     case Q_RTREE:
       k_query<Q_RTREE, ST><<<blocks, 128, 0, s>>>(m, d_q, ord, nq, d_out, nullptr, nullptr, d_status, budget, hp, hc,
@@ -1239,9 +1393,8 @@ int query_points(const MeshView& m, int accel, int sign, const float* d_q, uint6
                          : (accel == M2S_ACCEL_RTREE
                                 ? Q_RTREE
                                 : ((accel == M2S_ACCEL_BVH && sign == M2S_SIGN_NORMAL) ? Q_BVH_NORMAL : Q_BVH_RAYCAST));
-  // Small batches (not Bvh(Normal), whose tie-band fold runs per thread;
-  // a mesh of more than one triangle): one warp per query.
-  if (mode != Q_BVH_NORMAL && nq <= kWarpwiseMaxQueries && !(m.root & LEAF_BIT)) {
+  // Small batches (a mesh of more than one triangle): one warp per query.
+  if (nq <= kWarpwiseMaxQueries && !(m.root & LEAF_BIT)) {
     const bool counting = profiling_enabled() || grid_tuning().fp64_audit;
     DevBuf<unsigned long long> qs;
     int st;
@@ -1259,6 +1412,9 @@ int query_points(const MeshView& m, int accel, int sign, const float* d_q, uint6
       else if (mode == Q_RTREE)
         k_query_warpwise<Q_RTREE, ST><<<wb, 32 * kSmallWarps, 0, s>>>(m, d_q, nq, d_out, nullptr, nullptr, d_status,
                                                                       qp);
+      else if (mode == Q_BVH_NORMAL)
+        k_query_warpwise<Q_BVH_NORMAL, ST><<<wb, 32 * kSmallWarps, 0, s>>>(m, d_q, nq, d_out, nullptr, nullptr,
+                                                                           d_status, qp);
       else
         k_query_warpwise<Q_VECTOR, ST><<<wb, 32 * kSmallWarps, 0, s>>>(m, d_q, nq, nullptr, d_vec, d_inside, d_status,
                                                                        qp);
@@ -1296,7 +1452,12 @@ int query_points(const MeshView& m, int accel, int sign, const float* d_q, uint6
   DevBuf<uint32_t> hard_count;
   const uint32_t base_budget =
       budget_override >= 0 ? (uint32_t)budget_override : g_query_budget.load(std::memory_order_relaxed);
-  const bool two_pass = mode != Q_BVH_NORMAL && base_budget > 0;
+  // Bvh(Normal) hands long searches and tie-band folds to the warp pass in
+  // batches below kPacketMinQueries (on star s6: 1,000 points 6.17 -> 0.59
+  // ms, 10,000 14.5 -> 1.26 ms, 100,000 22.5 -> 5.70 ms, whose single-thread
+  // band traversals set the time); from there on throughput wins and it
+  // stays in one pass (1M points 29.7 against 33.4 ms with the hand-off).
+  const bool two_pass = base_budget > 0 && (mode != Q_BVH_NORMAL || nq < kPacketMinQueries);
   if (two_pass) {
     if ((st = hard.alloc(nq, s)) || (st = hard_count.alloc(1, s))) return st;
     M2S_CUDA(cudaMemsetAsync(hard_count.p, 0, 4, s));
@@ -1315,9 +1476,8 @@ int query_points(const MeshView& m, int accel, int sign, const float* d_q, uint6
     M2S_CUDA(cudaMemsetAsync(qs.p, 0, 8 * kQueryCounters, s));
   }
   // Morton-ordered warps search together (nearest_triangle_packet): always
-  // for Bvh(Normal), whose searches have no budget, and for the others from
-  // kPacketMinQueries on, where throughput rather than the longest warp sets
-  // the time.
+  // for Bvh(Normal), and for the others from kPacketMinQueries on, where
+  // throughput rather than the longest warp sets the time.
   const bool packet = ord != nullptr && (mode == Q_BVH_NORMAL || nq >= kPacketMinQueries);
   if (counting)
     launch_queries<true>(mode, m, d_q, ord, nq, d_out, d_vec, d_inside, d_status, budget, hp, hc, two_pass, packet,

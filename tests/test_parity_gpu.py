@@ -346,6 +346,29 @@ def test_query_autotune_keeps_results():
         L.m2s_set_query_budget(saved)
 
 
+@pytest.mark.parametrize("n", [700, 9000, 150_000])
+def test_bvh_normal_band_fold_paths(orc, n):
+    # Bvh(Normal) folds the tie band of the nearest distance in triangle
+    # order: on one warp per query for small batches, on one thread per query
+    # otherwise, and, when a thread's search or fold exceeds the node budget,
+    # on one warp in the second pass.  Every path and every budget (budget 0:
+    # one pass, no hand-off) gives the oracle's bits.  The points include many
+    # deep inside the star, whose band traversals are long.
+    v, idx = synth.star(5, seed=31)
+    q = synth.mixed_points(v, idx, n, seed=32, frac_uniform=0.9)
+    ref = orc_sdf(orc, v, idx, q, A.bvh(S.Normal))
+    acc = m2s.build_sdf_acceleration(v, T.TriangleList(idx), A.bvh(S.Normal))
+    L = m2s._lib.lib()
+    saved = L.m2s_query_budget()
+    try:
+        for b in (0, 16, 256, 4096):
+            L.m2s_set_query_budget(b)
+            assert_bit_equal(m2s.query_sdf(acc, q), ref, f"n {n} budget {b}")
+    finally:
+        L.m2s_set_query_budget(saved)
+        acc.close()
+
+
 def test_fp64_error_report(orc):
     # error report: distance error against an FP64 brute force
     v, idx = synth.star(4, seed=9)
