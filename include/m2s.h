@@ -365,9 +365,10 @@ uint32_t m2s_last_grid_round_log(uint32_t* out, uint32_t capacity);
  * query that visits more than its node budget is continued by a whole warp
  * (points deep inside a closed mesh
  * see most triangles at nearly the same distance).  `node_visits` is the
- * budget of batches of 2^20 queries and more; a smaller batch of nq queries
- * uses node_visits * sqrt(nq / 2^20), at least 64, since its time is its
- * longest single-thread search.  0 keeps every query on one thread.
+ * budget of batches of 2^20 queries and more; a batch of nq queries from 2^18
+ * uses node_visits * sqrt(nq / 2^20), and a smaller one node_visits / 16,
+ * at least 64 either way, since a small batch's time is its longest
+ * single-thread search.  0 keeps every query on one thread.
  * Process-wide tuning knob; the autotuner sets it. */
 void m2s_set_query_budget(uint32_t node_visits);
 uint32_t m2s_query_budget(void);

@@ -130,11 +130,18 @@ int query_points(const MeshView& m, int accel, int sign, const float* d_q, uint6
 // Node visits a query may spend in the one-thread-per-query pass before it is
 // continued one warp per query (0 disables the second pass).
 extern std::atomic<uint32_t> g_query_budget;
-// The budget a batch of nq queries uses: `base` from 2^20 queries up, and
-// base * sqrt(nq / 2^20), at least 64, below (0 stays 0: no warp pass).
+// The budget a batch of nq queries uses: `base` from 2^20 queries up,
+// base * sqrt(nq / 2^20) from 2^18, and base / 16 below, at least 64 (0 stays
+// 0: no warp pass).  Below 2^18 queries every query has a thread from the
+// start and the batch waits for its longest searches, which the warp pass
+// finishes sooner (star s6 mixed points, Rtree, base 1024: 50,000 queries
+// 1.30 -> 1.08 ms, 100,000 1.68 -> 1.51 ms); from 2^18 on, the thread pass's
+// throughput counts (400,000: 3.32 ms at 632 against 3.83 at 316 and 3.99 at 158).
 inline uint32_t effective_query_budget(uint32_t base, uint64_t nq) {
   if (base == 0) return 0;
-  const double f = nq >= (1ull << 20) ? 1.0 : std::sqrt((double)nq / (double)(1ull << 20));
+  const double f = nq >= (1ull << 20) ? 1.0
+                   : nq >= (1ull << 18) ? std::sqrt((double)nq / (double)(1ull << 20))
+                                        : 1.0 / 16.0;
   const uint32_t b = (uint32_t)(base * f + 0.5);
   return b < 64 ? std::min<uint32_t>(64, base) : b;
 }
