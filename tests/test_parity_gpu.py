@@ -370,6 +370,25 @@ def test_bvh_normal_band_fold_paths(orc, n):
         acc.close()
 
 
+@pytest.mark.parametrize("n", [1000, 12_000])
+def test_equidistant_centre_points_warp_stack_fallback(orc, n):
+    # Points at and near the centre of a fine icosphere (20,480 triangles) are
+    # nearly equidistant from every triangle: an exact search tests most of
+    # them, its warp-wide frontier outgrows the warp kernels' 512-entry
+    # stacks, and lane 0 finishes the search (or band fold) alone.  1,000
+    # points run one warp per query from the start; 12,000 reach the warp
+    # pass after the thread pass's node budget.  Every method gives the
+    # oracle's bits (the exact centre's axis rays pass through shared edges:
+    # the reference's parity rule, followed bit for bit, calls it outside).
+    v, idx = synth.icosphere(5)
+    rng = np.random.default_rng(41)
+    q = np.vstack([np.zeros((1, 3)), rng.normal(0, 1e-3, (63, 3)),
+                   rng.uniform(-1.2, 1.2, (n - 64, 3))]).astype(np.float32)
+    for am in (A.rtree(), A.rtree_bvh(), A.bvh(S.Raycast), A.bvh(S.Normal)):
+        gpu = m2s.generate_sdf(v, T.TriangleList(idx), q, am)
+        assert_bit_equal(gpu, orc_sdf(orc, v, idx, q, am), f"n {n} {am!r}")
+
+
 def test_fp64_error_report(orc):
     # error report: distance error against an FP64 brute force
     v, idx = synth.star(4, seed=9)
