@@ -1460,14 +1460,15 @@ int query_points(const MeshView& m, int accel, int sign, const float* d_q, uint6
   const uint32_t base_budget =
       budget_override >= 0 ? (uint32_t)budget_override : g_query_budget.load(std::memory_order_relaxed);
   // Bvh(Normal) hands long searches and tie-band folds to the warp pass in
-  // batches below 2^17 queries, whose single-thread band traversals set the
-  // time (star s6: 1,000 points 6.17 -> 0.59 ms, 10,000 15.5 -> 1.4 ms,
-  // 100,000 19.9 -> 5.2 ms; the terrain strip: 20,000 3.69 -> 1.39 ms, 50,000
-  // 2.91 -> 2.52 ms); from there on the one-pass packet search keeps its
-  // coherence and wins on the terrain (200,000 points 3.2 against 6.1 ms
-  // with the hand-off, 4M 18.1 against 18.3) though not on the star (300,000
-  // 25.7 against 12.4 ms).
-  const bool two_pass = base_budget > 0 && (mode != Q_BVH_NORMAL || nq < (1u << 17));
+  // batches below 2^18 queries (where the budget is base / 16), whose
+  // single-thread band traversals set the time (star s6: 1,000 points 6.17
+  // -> 0.59 ms, 10,000 15.5 -> 1.4 ms, 131,072 21.9 -> 3.4 ms, 262,143 23.9
+  // -> 5.2 ms; star s4 200,000 4.1 -> 1.9 ms; the terrain strip: 20,000 3.69
+  // -> 1.39 ms, 131,072 2.85 -> 2.38 ms, though 262,143 3.36 -> 4.31 ms);
+  // from there on the one-pass packet search keeps its coherence and wins on
+  // the terrain (400,000 points 4.1 against 9.0 ms with the hand-off, 1M 6.7
+  // against 20.0) and ties on the star (1M 30.2 against 30.7 ms).
+  const bool two_pass = base_budget > 0 && (mode != Q_BVH_NORMAL || nq < (1u << 18));
   if (two_pass) {
     if ((st = hard.alloc(nq, s)) || (st = hard_count.alloc(1, s))) return st;
     M2S_CUDA(cudaMemsetAsync(hard_count.p, 0, 4, s));

@@ -346,13 +346,13 @@ def test_query_autotune_keeps_results():
         L.m2s_set_query_budget(saved)
 
 
-@pytest.mark.parametrize("n", [700, 9000, 100_000, 150_000])
+@pytest.mark.parametrize("n", [700, 9000, 100_000, 150_000, 300_000])
 def test_bvh_normal_band_fold_paths(orc, n):
     # Bvh(Normal) folds the tie band of the nearest distance in triangle
     # order: on one warp per query for small batches (700), on one thread per
-    # query otherwise, and, below 2^17 queries (9,000; 100,000 with the packet
-    # search), when a thread's search or fold exceeds the node budget, on one
-    # warp in the second pass; from 2^17 (150,000) in one pass.  Every path and every budget (budget 0:
+    # query otherwise, and, below 2^18 queries (9,000; 100,000 and 150,000
+    # with the packet search), when a thread's search or fold exceeds the node
+    # budget, on one warp in the second pass; from 2^18 (300,000) in one pass.  Every path and every budget (budget 0:
     # one pass, no hand-off) gives the oracle's bits.  The points include many
     # deep inside the star, whose band traversals are long.
     v, idx = synth.star(5, seed=31)
