@@ -369,13 +369,17 @@ uint32_t m2s_last_grid_round_log(uint32_t* out, uint32_t capacity);
  * uses node_visits * sqrt(nq / 2^20), and a smaller one node_visits / 16,
  * at least 64 either way, since a small batch's time is its longest
  * single-thread search.  0 keeps every query on one thread.
+ * Bvh(Normal) hands searches and band folds over the budget to the warp pass
+ * in batches under 2^18 queries, and at every size when node_visits is 64 or
+ * less (a win on closed meshes with many deep-interior points, a loss on open
+ * surfaces; the autotuner tries it).
  * Process-wide tuning knob; the autotuner sets it. */
 void m2s_set_query_budget(uint32_t node_visits);
 uint32_t m2s_query_budget(void);
 
 /* The query autotuner (no counterpart in the reference): times the resident
  * mesh's LBVH query on the caller's device queries d_q[0..nq) with each
- * base budget of {0, 256, 512, 768, 1024, 1536, 2048, 4096} (see
+ * base budget of {0, 64, 256, 512, 1024, 1536, 2048, 4096} (see
  * m2s_set_query_budget: where a query moves from one thread to one warp,
  * scaled down for batches under 2^20 queries) and sets the fastest.  Results
  * do not depend on the budget.  Candidates are timed on this call alone:

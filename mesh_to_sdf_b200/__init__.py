@@ -406,7 +406,7 @@ class SdfAccelerationMesh:
                                              None if stream is None else ctypes.c_void_p(stream))
         _check(st, "query_sdf_device")
 
-    QUERY_BUDGETS = (0, 256, 512, 768, 1024, 1536, 2048, 4096)
+    QUERY_BUDGETS = (0, 64, 256, 512, 1024, 1536, 2048, 4096)
 
     def autotune_queries(self, q, stream=None):
         """The query autotuner: times this mesh's query on the device tensor q

@@ -145,9 +145,14 @@ inline uint32_t effective_query_budget(uint32_t base, uint64_t nq) {
   const uint32_t b = (uint32_t)(base * f + 0.5);
   return b < 64 ? std::min<uint32_t>(64, base) : b;
 }
-// Node budgets the query autotuner tries.
+// Node budgets the query autotuner tries (64 also moves Bvh(Normal) batches
+// of 2^18 queries and more to the warp hand-off: see query_points).
 constexpr int kQueryBudgetCandidates = 8;
-constexpr uint32_t kQueryBudgets[kQueryBudgetCandidates] = {0, 256, 512, 768, 1024, 1536, 2048, 4096};
+constexpr uint32_t kQueryBudgets[kQueryBudgetCandidates] = {0, 64, 256, 512, 1024, 1536, 2048, 4096};
+// Base budgets at or below this hand Bvh(Normal) searches and band folds to
+// the warp pass at every batch size; larger ones keep batches of 2^18
+// queries and more in one pass.
+constexpr uint32_t kNormalHandoffMaxBudget = 64;
 
 // Profiling (m2s_set_profiling, per host thread): whether it is on, and the
 // traversal counts of the last point query made with it on:

@@ -1466,9 +1466,15 @@ int query_points(const MeshView& m, int accel, int sign, const float* d_q, uint6
   // -> 5.2 ms; star s4 200,000 4.1 -> 1.9 ms; the terrain strip: 20,000 3.69
   // -> 1.39 ms, 131,072 2.85 -> 2.38 ms, though 262,143 3.36 -> 4.31 ms);
   // from there on the one-pass packet search keeps its coherence and wins on
-  // the terrain (400,000 points 4.1 against 9.0 ms with the hand-off, 1M 6.7
-  // against 20.0) and ties on the star (1M 30.2 against 30.7 ms).
-  const bool two_pass = base_budget > 0 && (mode != Q_BVH_NORMAL || nq < (1u << 18));
+  // the terrain (400,000 points 4.1 against 9.0 ms with the hand-off at the
+  // default budget, 1M 6.7 against 20.0) and ties on the star (1M 30.2
+  // against 30.7 ms).  A base budget of at most kNormalHandoffMaxBudget keeps
+  // the hand-off at every size, which suits closed meshes whose deep-interior
+  // points make long searches (star s6 at budget 64: 400,000 points 27.5 ->
+  // 7.7 ms, 1M 29.8 -> 17.0 ms) but not open ones (the terrain: 4.1 -> 6.3
+  // and 6.6 -> 14.7 ms); the autotuner tries it.
+  const bool two_pass =
+      base_budget > 0 && (mode != Q_BVH_NORMAL || nq < (1u << 18) || base_budget <= kNormalHandoffMaxBudget);
   if (two_pass) {
     if ((st = hard.alloc(nq, s)) || (st = hard_count.alloc(1, s))) return st;
     M2S_CUDA(cudaMemsetAsync(hard_count.p, 0, 4, s));
