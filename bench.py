@@ -611,7 +611,10 @@ def main():
         q = torch.from_numpy(q_host).to(dev)
         qo = torch.empty(N_POINTS, dtype=torch.float32, device=dev)
         # the library's query autotuner picks the node budget (one thread per
-        # query, then one warp) on the Bvh+Raycast batch
+        # query, then one warp) on the Bvh+Raycast batch; the process-wide
+        # budget it sets is put back after these lines, so later entries
+        # start from the library default
+        saved_budget = m2s._lib.lib().m2s_query_budget()
         acc = m2s.build_sdf_acceleration(v, m2s.Topology.TriangleList(idx), A.bvh(S.Raycast))
         best_budget, tune = acc.autotune_queries(q, stream)
         acc.close()
@@ -650,6 +653,7 @@ def main():
                 points[name]["per_query"] = {k[:-len("_per_query")]: round(v_, 2) for k, v_ in qs.items()
                                              if k.endswith("_per_query")}
             acc.close()
+        m2s._lib.lib().m2s_set_query_budget(saved_budget)
         assert int(status.item()) == 0
 
     # ---- result-side rows on this grid and mesh: the viewer's distance-ordered
@@ -783,7 +787,10 @@ def small_or_terrain_entry(which, steps=5, warmup=3, accuracy=True, peaks=None):
         roof.pop(k)  # the ncu traffic figure belongs to the bench grid
     qd = torch.from_numpy(q).cuda()
     qo = torch.empty(npts, dtype=torch.float32, device="cuda")
-    budget, _ = mesh.autotune_queries(qd)  # the library's query autotuner, on these points
+    # the library's query autotuner, on these points; the process-wide budget
+    # it sets is put back below, so it does not carry over to other entries
+    saved_budget = m2s._lib.lib().m2s_query_budget()
+    budget, _ = mesh.autotune_queries(qd)
     for _ in range(2):
         mesh.query_device(qd, qo, status)
     torch.cuda.synchronize()
@@ -798,6 +805,7 @@ def small_or_terrain_entry(which, steps=5, warmup=3, accuracy=True, peaks=None):
     torch.cuda.synchronize()
     m2s.set_fp64_audit(False)
     points_audit = m2s.last_query_audit()
+    m2s._lib.lib().m2s_set_query_budget(saved_budget)
     assert int(status.item()) == 0, int(status.item())
     line = {"workload": which, "triangles": mesh.triangle_count, "grid": [int(c) for c in grid.cell_count],
             "sign": sign.name, "grid_ms": gms, "cells_per_s": N / (gms / 1e3), "grid_phase_ms": phases,
@@ -979,8 +987,10 @@ def serving_entry(rates=(50.0, 100.0, 200.0, 400.0), n_req=200, plain=True):
     same arrivals also go through the plain path — one library call per
     request (query_sdf, a resident-mesh grid call with its copies, or
     build_sdf_acceleration), served in arrival order by one host thread — and
-    both arms report p50 / p99 and aggregate cells/s and points/s.  Returns
-    one dict."""
+    both arms report p50 / p99 and aggregate cells/s and points/s.  Point
+    requests use the process-wide node budget as found (the library default
+    unless a caller set one; the entries above restore theirs).  Returns one
+    dict."""
     import torch
 
     import mesh_to_sdf_b200 as m2s
